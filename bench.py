@@ -1,0 +1,421 @@
+"""Benchmark: forward + backward of the tiled 2D Gaussian rasterizer, ms per iteration.
+
+Workload (default): 1024x1024x3 float32 target from the seeded generator (gratings, polygons,
+noise) and 100,000 Gaussians (means uniform, σ = exp(N(ln 2, 0.5)), θ ~ U[0, π), RGB ~ U[0,1]³,
+opacity = sigmoid(N(0,1)), 3σ support), normalized mode.  One step = render from the RS field
+tensors + gradients of Σ image·(target − 0.5) w.r.t. means, log-scales, rotations, colours and
+opacity logits (the reference's fwd+bwd protocol, benchmarks/tiled_render_profile.py:349-351).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Every rank renders its own image (replicas: the path needs no collective); rank 0 prints one
+JSON line.  L2 is flushed (a 256 MiB write) before every timed step.  Step times are CUDA-event
+durations on the rendering stream, summed over the K steps, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "fwd+bwd ms/iter (1024², 100k Gaussians); batched fit img/s vs plain kernel"
+WORKLOAD = {"H": 1024, "W": 1024, "N": 100_000, "seed": 0, "mode": "normalized"}
+PAIR_SLOTS_FWD, PAIR_SLOTS_BWD = 14, 40   # FP32 issue slots per in-rectangle pair (reference)
+SM_COUNT, FP32_LANES = 148, 128
+
+
+def measured_peaks():
+    try:
+        return json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def make_inputs(dev, wl=WORKLOAD):
+    from structsplat_b200.synthetic import make_field, make_target
+    f = make_field(wl["H"], wl["W"], wl["N"], seed=wl["seed"])
+    target = make_target(wl["H"], wl["W"], seed=wl["seed"] + 1)
+    host = {"means": f.means, "log_scales": f.log_scales, "rotations": f.rotations,
+            "colors": f.colors, "opacity_logits": f.opacity_logits,
+            "grad_out": (target - 0.5).astype(np.float32)}
+    return host
+
+
+def pair_count(host, wl=WORKLOAD):
+    from oracle import c_oracle, field_ref
+    r = field_ref.radii(torch.tensor(host["log_scales"]), torch.tensor(host["rotations"]), 3.0)
+    return c_oracle.pair_count(host["means"], r, wl["H"], wl["W"])
+
+
+def flush_l2(buf):
+    buf.fill_(1)   # 256 MiB write, twice the L2
+
+
+def run_ours(args, rank, world, dev):
+    from structsplat_b200 import _native, render_gaussians
+    from structsplat_b200 import render as R
+    from structsplat_b200.field import project
+
+    wl = WORKLOAD
+    H, W = wl["H"], wl["W"]
+    host = make_inputs(dev)
+    names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
+    params = [torch.tensor(host[k], device=dev, requires_grad=True) for k in names]
+    grad_out = torch.tensor(host["grad_out"], device=dev)
+    normalize = wl["mode"] == "normalized"
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+
+    def step():
+        img = render_gaussians(params[0], params[1], params[2], params[3], H, W,
+                               opacity_logits=params[4], normalize=normalize)
+        return torch.autograd.grad(img, params, grad_out)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _native.CALLS.clear()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clocks:
+        for i in range(args.steps):
+            flush_l2(flush)
+            starts[i].record()
+            step()
+            ends[i].record()
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    launches = launches_from_calls(_native.CALLS)
+
+    # ---- dominant kernels, timed alone with CUDA events on the launching stream ----
+    with torch.no_grad():
+        n = wl["N"]
+        rec, _, _ = project(*[p.detach() for p in params[:4]], params[4].detach(), H, W)
+        index = R.index_from_records(rec, n, H, W, exact=True)
+        out, den = R._forward(rec, n, index, H, W, normalize, 1e-8, 0.0, dev)
+        kt = {}
+        for name, fn in (
+            ("forward", lambda: R._forward(rec, n, index, H, W, normalize, 1e-8, 0.0, dev)),
+            ("backward", lambda: R._backward(grad_out, rec, n, den, out, index, H, W, normalize,
+                                             1e-8, 0.0, True, False, dev)),
+            ("binning", lambda: R.index_from_records(rec, n, H, W, capacity=index.capacity)),
+        ):
+            for _ in range(3):
+                fn()
+            times = []
+            for _ in range(max(5, args.steps)):
+                flush_l2(flush)
+                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s.record()
+                fn()
+                e.record()
+                torch.cuda.synchronize()
+                times.append(s.elapsed_time(e))
+            kt[name] = statistics.median(times)
+        entries = index.capacity
+
+    # ---- end to end through the public API with host buffers ----
+    pinned = {k: torch.tensor(host[k]).pin_memory() for k in names + ["grad_out"]}
+    host_grads = [torch.empty(p.shape, dtype=torch.float32).pin_memory() for p in params]
+    bi = sum(v.numel() * 4 for v in pinned.values())
+    bo = sum(g.numel() * 4 for g in host_grads)
+
+    def e2e_step():
+        dev_in = [pinned[k].to(dev, non_blocking=True).requires_grad_(True) for k in names]
+        go = pinned["grad_out"].to(dev, non_blocking=True)
+        img = render_gaussians(dev_in[0], dev_in[1], dev_in[2], dev_in[3], H, W,
+                               opacity_logits=dev_in[4], normalize=normalize)
+        grads = torch.autograd.grad(img, dev_in, go)
+        for h, g in zip(host_grads, grads):
+            h.copy_(g, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        e2e_step()
+        e.record()
+        e.synchronize()
+        e2e_ms.append(s.elapsed_time(e))
+
+    stats = torch.tensor([total_ms, sum(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
+    return {"total_ms": float(stats[0]), "e2e_total_ms": float(stats[1]), "step_ms": step_ms,
+            "kernels_ms": kt, "entries": entries, "launches": launches, "bi": bi, "bo": bo,
+            "clocks": clocks.summary(), "host": host}
+
+
+KERNELS_PER_CALL = {
+    # kernels of this library launched by each entry point (CUB's scan is two kernels)
+    "ss_project_rs": 1, "ss_pack_splats": 1, "ss_tile_index_count": 4, "ss_tile_index_fill": 3,
+    "ss_render_forward": 1, "ss_render_backward": 1, "ss_project_rs_backward": 1,
+}
+
+
+def launches_from_calls(calls):
+    return sum(KERNELS_PER_CALL.get(k, 1) * v for k, v in calls.items())
+
+
+def cpu_reference_step_fn(host, wl=WORKLOAD):
+    """One fwd+bwd of the reference's CPU (torch) path; the reference package itself when it
+    is installed under baseline/_ref, else the oracle's restatement of it."""
+    H, W = wl["H"], wl["W"]
+    ref_root = REPO / "baseline" / "_ref"
+    kind = "port"
+    if (ref_root / "structsplat" / "render.py").is_file():
+        sys.path.insert(0, str(ref_root))
+        from structsplat.gaussians import GaussianField
+        from structsplat.render import render_field
+        kind = "reference"
+
+        def step():
+            f = GaussianField(*[torch.tensor(host[k]) for k in
+                                ("means", "log_scales", "rotations", "colors", "opacity_logits")])
+            f.trainable()
+            img = render_field(f.means, f.conics(), f.colors, f.radii(3.0), H, W,
+                               mode=wl["mode"], opacities=f.opacity_values())
+            params = [f.means, f.log_scales, f.rotations, f.colors, f.opacities]
+            torch.autograd.grad(img, params, torch.tensor(host["grad_out"]))
+    else:
+        from oracle import field_ref, render_ref
+
+        def step():
+            p = [torch.tensor(host[k]).requires_grad_(True) for k in
+                 ("means", "log_scales", "rotations", "colors", "opacity_logits")]
+            img = render_ref.render(p[0], field_ref.conics(p[1], p[2]), p[3],
+                                    field_ref.radii(p[1], p[2], 3.0), H, W,
+                                    opacities=torch.sigmoid(p[4]),
+                                    normalize=wl["mode"] == "normalized")
+            torch.autograd.grad(img, p, torch.tensor(host["grad_out"]))
+    return step, kind
+
+
+def cpu_baseline(host, budget_s=20.0):
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    step, kind = cpu_reference_step_fn(host)
+    t0 = time.perf_counter()
+    step()
+    times = [time.perf_counter() - t0]
+    while sum(times) < budget_s * 0.5 and len(times) < 10:
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    ms = statistics.median(times[1:] if len(times) > 1 else times) * 1e3
+    return {"value": round(ms, 3), "unit": "ms/iter", "cores": threads, "kind": kind,
+            "sample": f"{len(times)} full fwd+bwd steps of the same workload (first untimed "
+                      "for the median), torch CPU, all host threads"}
+
+
+def ref_cuda_baseline(host, dev, steps=10):
+    """The reference's own CUDA extension (built unmodified for sm_100a into baseline/_ref)
+    through its public render_cuda_exact, untiled and tiled arms; None when not built."""
+    try:
+        sys.path.insert(0, str(REPO / "baseline"))
+        from build_ref_cuda import load_reference_extension
+        cuda_render = load_reference_extension()
+        from structsplat.gaussians import GaussianField
+    except Exception as exc:  # not built / not installed
+        return {"unavailable": str(exc)[:200]}
+    H, W = WORKLOAD["H"], WORKLOAD["W"]
+    f = GaussianField(*[torch.tensor(host[k], device=dev) for k in
+                        ("means", "log_scales", "rotations", "colors", "opacity_logits")])
+    f.trainable()
+    params = [f.means, f.log_scales, f.rotations, f.colors, f.opacities]
+    go = torch.tensor(host["grad_out"], device=dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    res = {}
+    for arm, kw in (("cuda", dict(tiled=False)), ("cuda_tiled", dict(tiled=True))):
+        def step():
+            img = cuda_render.render_cuda_exact(f.means, f.conics(), f.colors, f.radii(3.0), H, W,
+                                                opacities=f.opacity_values(), **kw)
+            torch.autograd.grad(img, params, go)
+        for _ in range(3):
+            step()
+        times = []
+        for _ in range(steps):
+            flush_l2(flush)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            step()
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        res[arm] = round(statistics.median(times), 4)
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        host = make_inputs(None)
+        step, kind = cpu_reference_step_fn(host)
+        torch.set_num_threads(os.cpu_count() or 1)
+        for _ in range(min(args.warmup, 1)):
+            step()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        line = {"impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms/iter",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "1024x1024x3, 100k Gaussians, normalized, fwd+bwd through "
+                                       "RS params", "parallelism": "cpu"},
+                "cpu_baseline": {"value": round(ms, 3), "unit": "ms/iter",
+                                 "cores": torch.get_num_threads(), "kind": kind,
+                                 "sample": "full workload steps on the host cores"},
+                "e2e": {"value": round(ms, 3), "unit": "ms/iter", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(
+            seconds=120))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    res = run_ours(args, rank, world, dev)
+    host = res.pop("host")
+    peaks = measured_peaks()
+    P = pair_count(host) if rank == 0 else 0
+    line = None
+    if rank == 0:
+        ms = res["total_ms"] / args.steps
+        clk = res["clocks"]
+        f_mhz = peaks.get("sm_max_mhz") or 1965.0
+        peak_slots = SM_COUNT * FP32_LANES * f_mhz * 1e6 / 1e9   # Gslot/s
+        kt = res["kernels_ms"]
+        bwd_ach = P * PAIR_SLOTS_BWD / (kt["backward"] * 1e-3) / 1e9
+        fwd_ach = P * PAIR_SLOTS_FWD / (kt["forward"] * 1e-3) / 1e9
+        t_bound_ms = P * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (peak_slots * 1e9) * 1e3
+        line = {
+            "metric": METRIC, "value": round(ms, 4), "unit": "ms/iter", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "1024x1024x3 target, 100k Gaussians, normalized, fwd+bwd "
+                                   "through RS params (means, log_scales, rotations, colors, "
+                                   "opacity logits)", "H": 1024, "W": 1024, "gaussians": 100000,
+                       "pairs": P, "tile_entries": res["entries"],
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "fp32", "kernel": "backward_kernel",
+                         "achieved": round(bwd_ach, 1), "peak": round(peak_slots, 1),
+                         "unit": "Gslot/s", "frac": round(bwd_ach / peak_slots, 4),
+                         "traffic": None,
+                         "work": f"{PAIR_SLOTS_BWD} FP32 issue slots per in-rectangle pair x "
+                                 f"{P} pairs per launch",
+                         "peak_source": "148 SMs x 128 FP32 lanes x sm_max_mhz of "
+                                        "MEASURED_PEAKS.json"},
+            "kernels_ms": {k: round(v, 4) for k, v in kt.items()},
+            "forward_roofline_frac": round(fwd_ach / peak_slots, 4),
+            "step_roofline_frac": round(t_bound_ms / ms, 4),
+            "clocks": clk,
+            "gpu_launches": res["launches"],
+            "e2e": {"value": round(res["e2e_total_ms"] / args.steps, 4), "unit": "ms/iter",
+                    "h2d_bytes_per_step": res["bi"], "d2h_bytes_per_step": res["bo"]},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(host)
+        if world == 1 and not args.no_ref_cuda:
+            line["reference_cuda_ms"] = ref_cuda_baseline(host, dev)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,175 @@
+/*
+ * structsplat_b200 — B200 (sm_100a) tiled 2D Gaussian rasterizer, C ABI.
+ *
+ * Plain pointers and sizes only.  Every pointer argument named *_dev or documented as
+ * "device" must point to CUDA device memory; the caller allocates every buffer (outputs and
+ * workspaces, sized by the *_workspace_bytes queries) and the library only borrows them.
+ * Every call is asynchronous on the given stream (a cudaStream_t; 0 = legacy default stream),
+ * performs no host synchronisation and no allocation, and is safe to capture in a CUDA graph.
+ *
+ * Return value: SS_OK (0) or an SS_ERR_* code; ss_last_error() gives a thread-local message.
+ * In-kernel conditions the host cannot see are OR-ed into a caller-provided device status
+ * word (SS_STATUS_* bits) that the caller reads whenever it chooses.
+ *
+ * Reference correspondence (intrinsicD/structsplat, src/structsplat/):
+ *   ss_build_tile_index  <- cuda/render_ext.cpp:140-175 build_tile_index / render_ext.cu:858-952
+ *   ss_forward_tiled     <- cuda/render_ext.cpp forward_tiled / render_ext.cu:1011-1061
+ *   ss_backward_tiled    <- cuda/render_ext.cpp backward_tiled / render_ext.cu:1174-1231
+ *   ss_render_*          <- the same three, split into pack / index / render stages
+ *   ss_structure_tensor  <- structure_tensor.py:137-186 (NumPy in the reference)
+ *   ss_project_rs*       <- gaussians.py:270-321 (conics, radii, opacity) and their autograd
+ */
+#ifndef STRUCTSPLAT_B200_H
+#define STRUCTSPLAT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* ss_stream_t;
+
+enum {
+  SS_OK = 0,
+  SS_ERR_INVALID_ARGUMENT = 1,
+  SS_ERR_CAPACITY = 2,
+  SS_ERR_CUDA = 3,
+  SS_ERR_UNSUPPORTED = 4
+};
+
+/* Device status word bits. */
+#define SS_STATUS_INDEX_OVERFLOW 0x1u  /* tile index needed more than gid_capacity entries */
+#define SS_STATUS_INDEX_INT32 0x2u     /* entry total exceeded INT32_MAX */
+#define SS_STATUS_DETERMINISTIC_TRUNCATED 0x4u /* deterministic backward met a truncated index */
+
+/* ---------------------------------------------------------------- library */
+const char* ss_last_error(void);
+int ss_version(void);
+/* Bytes of one packed splat record (64). */
+size_t ss_splat_record_bytes(void);
+
+/* ---------------------------------------------------------------- splat records
+ * Packs one 64-byte record per Gaussian: mean, exponent-domain conic, opacity, colour, conic,
+ * and the clipped support rectangle of render.py:62-78 (torch.round half-to-even centre,
+ * clip to the image; a non-finite centre has empty support as in render_ext.cu:25-34).
+ * means (n,2) f32, conics (n,3) f32 [a,b,c] with q = a dx^2 + 2b dx dy + c dy^2,
+ * colors (n,3) f32, radii (n,2) int64, opacities (n) f32 or NULL (opacity 1). */
+int ss_pack_splats(const float* means, const float* conics, const float* colors,
+                   const int64_t* radii, const float* opacities, int64_t n, int height,
+                   int width, void* records, ss_stream_t stream);
+
+/* Fused RS projection (gaussians.py:270-321): from means (n,2), log_scales (n,2),
+ * rotations (n), colors (n,3), opacity_logits (n or NULL) computes the conic with isotropic
+ * `dilation`, the radii ceil(cutoff*sqrt(Sigma_axis)) >= 1, the opacity sigmoid, and writes the
+ * packed records.  conics_out (n,3) and radii_out (n,2) are optional (NULL skips them). */
+int ss_project_rs(const float* means, const float* log_scales, const float* rotations,
+                  const float* colors, const float* opacity_logits, int64_t n, float dilation,
+                  float sigma_cutoff, int height, int width, void* records, float* conics_out,
+                  int64_t* radii_out, ss_stream_t stream);
+
+/* Chain rule of ss_project_rs: conic and opacity gradients -> log_scale, rotation and
+ * opacity-logit gradients (written, not accumulated).  grad_opacities / grad_opacity_logits
+ * may be NULL together. */
+int ss_project_rs_backward(const float* log_scales, const float* rotations,
+                           const float* opacity_logits, int64_t n, float dilation,
+                           const float* grad_conics, const float* grad_opacities,
+                           float* grad_log_scales, float* grad_rotations,
+                           float* grad_opacity_logits, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- tile index
+ * Tiles are tile_size x tile_size pixels, tiles_x = ceil(W/ts), T = tiles_x * ceil(H/ts);
+ * 1 <= tile_size and tile_size^2 <= 1024 (render_ext.cpp:163-164).  Entries of tile t are
+ * tile_gids[tile_offsets[t] .. tile_offsets[t+1]) in ascending Gaussian id.
+ * ellipse_cull drops (tile, Gaussian) pairs whose faded weight is zero on the whole tile
+ * (render_ext.cu:101-133,178-191); callers enable it only together with the support fade. */
+int ss_tile_index_workspace_bytes(int64_t n, int height, int width, int tile_size,
+                                  size_t* bytes);
+/* Stage 1: per-tile counts and offsets.  tile_offsets (T+1) int32 receives the offsets;
+ * tile_offsets[T] is the entry total.  workspace must be kept for stage 2. */
+int ss_tile_index_count(const void* records, int64_t n, int height, int width, int tile_size,
+                        int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets,
+                        void* workspace, size_t workspace_bytes, uint32_t* status,
+                        ss_stream_t stream);
+/* Stage 2: fill tile_gids (capacity gid_capacity) and sort every tile ascending.  Entries
+ * beyond the capacity are dropped and SS_STATUS_INDEX_OVERFLOW is raised; the render calls
+ * then render the affected tiles exactly by scanning all Gaussians. */
+int ss_tile_index_fill(const void* records, int64_t n, int height, int width, int tile_size,
+                       int ellipse_cull, float sigma_cutoff, const int32_t* tile_offsets,
+                       int32_t* tile_gids, int64_t gid_capacity, void* workspace,
+                       size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- render
+ * Supported render tile sizes: 16 (the reference default).  fade_tail is
+ * alpha*exp(-cutoff^2/2) rounded to float (0 = no fade); eps > 0 and finite.
+ * out (H,W,3) f32 image; den (H,W) f32 raw weight sum without eps. */
+int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
+                      int64_t gid_capacity, const int32_t* tile_offsets, int height, int width,
+                      int tile_size, int normalize, float eps, float fade_tail, float* out,
+                      float* den, uint32_t* status, ss_stream_t stream);
+
+/* Workspace for the deterministic backward (0 bytes for the atomic one). */
+int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
+                                       size_t* bytes);
+/* Gradients of sum(out * grad_out) w.r.t. means (n,2), conics (n,3), colors (n,3) and, when
+ * has_opacity, opacities (n).  Outputs are overwritten.  deterministic=0 reduces each
+ * (tile, Gaussian) pair in-warp and adds it with one atomic per component; deterministic=1
+ * stores the per-pair partials and sums them per Gaussian in ascending tile order, which is
+ * bitwise reproducible run to run. */
+int ss_render_backward(const float* grad_out, const void* records, int64_t n, const float* den,
+                       const float* out, const int32_t* tile_gids, int64_t gid_capacity,
+                       const int32_t* tile_offsets, int height, int width, int tile_size,
+                       int normalize, float eps, float fade_tail, int has_opacity,
+                       float* grad_means, float* grad_conics, float* grad_colors,
+                       float* grad_opacities, int deterministic, void* workspace,
+                       size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- reference-shaped calls
+ * One-call equivalents of the reference extension's entry points, taking its tensor
+ * contract (render_ext.cpp:89-137).  They pack records into `workspace` (size from
+ * ss_reference_workspace_bytes) and then run the staged calls above. */
+int ss_reference_workspace_bytes(int64_t n, int height, int width, int tile_size,
+                                 int64_t gid_capacity, size_t* bytes);
+int ss_build_tile_index(const float* means, const float* conics, const int64_t* radii,
+                        int64_t n, int height, int width, int tile_size, int ellipse_cull,
+                        float sigma_cutoff, int32_t* tile_gids, int64_t gid_capacity,
+                        int32_t* tile_offsets, void* workspace, size_t workspace_bytes,
+                        uint32_t* status, ss_stream_t stream);
+int ss_forward_tiled(const float* means, const float* conics, const float* colors,
+                     const int64_t* radii, const float* opacities, int64_t n,
+                     const int32_t* tile_gids, int64_t gid_capacity,
+                     const int32_t* tile_offsets, int height, int width, int normalize,
+                     float eps, int tile_size, int support_fade, float sigma_cutoff, float* out,
+                     float* den, void* workspace, size_t workspace_bytes, uint32_t* status,
+                     ss_stream_t stream);
+int ss_backward_tiled(const float* grad_out, const float* means, const float* conics,
+                      const float* colors, const int64_t* radii, const float* opacities,
+                      int64_t n, const float* den, const float* out, const int32_t* tile_gids,
+                      int64_t gid_capacity, const int32_t* tile_offsets, int height, int width,
+                      int normalize, float eps, int tile_size, int support_fade,
+                      float sigma_cutoff, float* grad_means, float* grad_conics,
+                      float* grad_colors, float* grad_opacities, void* workspace,
+                      size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- structure tensor
+ * J = G_rho * (grad I grad I^T) of an (H,W,C) f32 image, C in {1,3} (structure_tensor.py).
+ * taps_grad / taps_tensor are HOST arrays of 2r+1 normalised Gaussian taps (r <= 31) for the
+ * pre-smoothing and tensor smoothing (a radius of 0 disables that blur).  gradient_operator:
+ * 0 central (np.gradient), 1 sobel, 2 scharr.  color_space: 0 luma (Rec.709), 1 rgb
+ * (Di Zenzo sum).  Outputs (H,W) f32 maps and u8 labels; stats_dev receives four doubles:
+ * energy_ref, flat threshold, median, 99th percentile. */
+int ss_structure_tensor_workspace_bytes(int height, int width, int channels, size_t* bytes);
+int ss_structure_tensor(const float* image, int height, int width, int channels,
+                        const float* taps_grad, int radius_grad, const float* taps_tensor,
+                        int radius_tensor, int gradient_operator, int color_space,
+                        double flat_frac, double corner_frac, float* lam1, float* lam2,
+                        float* angle, float* coherence, float* energy, uint8_t* label,
+                        double* stats_dev, void* workspace, size_t workspace_bytes,
+                        ss_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STRUCTSPLAT_B200_H */

@@ -1,0 +1,107 @@
+"""ctypes binding of ``libstructsplat_b200.so`` (the C ABI in ``include/structsplat_b200.h``).
+
+The library is built in-tree by ``structsplat_b200.build``.  There is no fallback: if the
+library is missing or cannot be loaded, every entry point raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libstructsplat_b200.so"
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_f32 = ctypes.c_float
+_f64 = ctypes.c_double
+_szp = ctypes.POINTER(ctypes.c_size_t)
+
+# name -> argtypes (all return int status unless listed in _RESTYPES)
+SIGNATURES = {
+    "ss_last_error": [],
+    "ss_version": [],
+    "ss_splat_record_bytes": [],
+    "ss_pack_splats": [_vp, _vp, _vp, _vp, _vp, _i64, _int, _int, _vp, _vp],
+    "ss_project_rs": [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _int, _int, _vp, _vp, _vp, _vp],
+    "ss_project_rs_backward": [_vp, _vp, _vp, _i64, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
+    "ss_tile_index_workspace_bytes": [_i64, _int, _int, _int, _szp],
+    "ss_tile_index_count": [_vp, _i64, _int, _int, _int, _int, _f32, _vp, _vp, ctypes.c_size_t,
+                            _vp, _vp],
+    "ss_tile_index_fill": [_vp, _i64, _int, _int, _int, _int, _f32, _vp, _vp, _i64, _vp,
+                           ctypes.c_size_t, _vp, _vp],
+    "ss_render_forward": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _f32, _f32, _vp, _vp,
+                          _vp, _vp],
+    "ss_render_backward_workspace_bytes": [_i64, _i64, _int, _szp],
+    "ss_render_backward": [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _int, _int, _int,
+                           _f32, _f32, _int, _vp, _vp, _vp, _vp, _int, _vp, ctypes.c_size_t, _vp,
+                           _vp],
+    "ss_reference_workspace_bytes": [_i64, _int, _int, _int, _i64, _szp],
+    "ss_build_tile_index": [_vp, _vp, _vp, _i64, _int, _int, _int, _int, _f32, _vp, _i64, _vp,
+                            _vp, ctypes.c_size_t, _vp, _vp],
+    "ss_forward_tiled": [_vp, _vp, _vp, _vp, _vp, _i64, _vp, _i64, _vp, _int, _int, _int, _f32,
+                         _int, _int, _f32, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp],
+    "ss_backward_tiled": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int,
+                          _int, _int, _f32, _int, _int, _f32, _vp, _vp, _vp, _vp, _vp,
+                          ctypes.c_size_t, _vp, _vp],
+    "ss_structure_tensor_workspace_bytes": [_int, _int, _int, _szp],
+    "ss_structure_tensor": [_vp, _int, _int, _int, _vp, _int, _vp, _int, _int, _int, _f64, _f64,
+                            _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],
+}
+_RESTYPES = {"ss_last_error": ctypes.c_char_p, "ss_splat_record_bytes": ctypes.c_size_t}
+
+_LIB = None
+_LOCK = threading.Lock()
+CALLS: collections.Counter = collections.Counter()  # entry-point call counts (launch accounting)
+
+
+class NativeError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, name: str, code: int, message: str):
+        super().__init__(f"{name} failed (status {code}): {message}")
+        self.code = code
+
+
+def lib():
+    """Load (once) and return the CUDA library; raises RuntimeError when it is unavailable."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    with _LOCK:
+        if _LIB is not None:
+            return _LIB
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"structsplat_b200 CUDA library not built ({LIB_PATH} missing); run "
+                "`python -m structsplat_b200.build` (there is no CPU fallback)")
+        handle = ctypes.CDLL(str(LIB_PATH))
+        for name, args in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, ctypes.c_int)
+        _LIB = handle
+        return _LIB
+
+
+def call(name: str, *args) -> None:
+    """Invoke a status-returning entry point and raise on failure."""
+    CALLS[name] += 1
+    rc = getattr(lib(), name)(*args)
+    if rc != 0:
+        msg = lib().ss_last_error().decode("utf-8", "replace")
+        if rc == 1:
+            raise ValueError(f"{name}: {msg}")
+        raise NativeError(name, rc, msg)
+
+
+def size_query(name: str, *args) -> int:
+    out = ctypes.c_size_t(0)
+    call(name, *args, ctypes.byref(out))
+    return int(out.value)
+
+
+def exported_symbols() -> list[str]:
+    return sorted(SIGNATURES)

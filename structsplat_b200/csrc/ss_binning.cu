@@ -1,0 +1,374 @@
+// Tile binning: count -> exclusive scan -> fill -> per-tile sort.
+//
+// Result contract (cuda_render.py:177-226, render_ext.cu:858-952): tile t lists every Gaussian
+// whose clipped support rectangle touches it, offsets[t]..offsets[t+1]; the lists are sorted by
+// ascending Gaussian id, which is the order the reference's stable radix sort leaves and makes
+// every downstream sum deterministic.  No sort over all pairs is needed: per-tile counts come
+// from atomics, a device-wide scan gives the offsets, the fill claims slots with per-tile atomic
+// cursors, and a per-tile bitonic sort in shared memory restores ascending ids.
+#include <cub/device/device_scan.cuh>
+
+#include "ss_common.cuh"
+
+namespace ss {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSmallRect = 8;          // tiles a lane enumerates alone; larger rects use the warp
+constexpr int kWarpSortMax = 1024;     // per-warp shared-memory sort capacity (ints)
+constexpr int kBigSortSmem = 16384;    // per-CTA shared-memory sort capacity (ints)
+
+struct TileGrid {
+  int ts, tiles_x, tiles_y;
+  int64_t T;
+};
+
+inline TileGrid make_grid(int H, int W, int ts) {
+  TileGrid g;
+  g.ts = ts;
+  g.tiles_x = (W + ts - 1) / ts;
+  g.tiles_y = (H + ts - 1) / ts;
+  g.T = (int64_t)g.tiles_x * g.tiles_y;
+  return g;
+}
+
+// Workspace layout (each region 256-byte aligned).
+struct IndexWorkspace {
+  int* tile_count;        // T+1   per-tile counters (fill consumes them back to zero)
+  long long* offsets64;   // T+1   exclusive scan in int64
+  int* big_tiles;         // T     tiles whose list is too long for the warp sort
+  int* big_count;         // 1
+  void* scan_temp;
+  size_t scan_bytes;
+};
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t scan_temp_bytes(int64_t items) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveScan(nullptr, bytes, (const int*)nullptr, (long long*)nullptr,
+                                 ::cuda::std::plus<long long>(), (long long)0, (int)items);
+  return bytes;
+}
+
+size_t index_workspace_bytes(int64_t T) {
+  return align256(sizeof(int) * (T + 1)) + align256(sizeof(long long) * (T + 1)) +
+         align256(sizeof(int) * (T > 0 ? T : 1)) + align256(sizeof(int)) +
+         align256(scan_temp_bytes(T + 1));
+}
+
+IndexWorkspace carve(void* base, int64_t T) {
+  IndexWorkspace w;
+  char* p = static_cast<char*>(base);
+  w.tile_count = reinterpret_cast<int*>(p);
+  p += align256(sizeof(int) * (T + 1));
+  w.offsets64 = reinterpret_cast<long long*>(p);
+  p += align256(sizeof(long long) * (T + 1));
+  w.big_tiles = reinterpret_cast<int*>(p);
+  p += align256(sizeof(int) * (T > 0 ? T : 1));
+  w.big_count = reinterpret_cast<int*>(p);
+  p += align256(sizeof(int));
+  w.scan_temp = p;
+  w.scan_bytes = align256(scan_temp_bytes(T + 1));
+  return w;
+}
+
+struct TileRect {
+  int gx0, gy0, gw, gh;
+};
+
+__device__ __forceinline__ TileRect tile_rect_of(const Splat* rec, int64_t i, int ts) {
+  TileRect r{0, 0, 0, 0};
+  int4 b = reinterpret_cast<const int4*>(rec + i)[3];
+  if (b.z > b.x && b.w > b.y) {
+    r.gx0 = b.x / ts;
+    r.gy0 = b.y / ts;
+    r.gw = (b.z - 1) / ts - r.gx0 + 1;
+    r.gh = (b.w - 1) / ts - r.gy0 + 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ Splat load_splat(const Splat* rec, int64_t i) {
+  Splat s;
+  const float4* src = reinterpret_cast<const float4*>(rec + i);
+  float4* d = reinterpret_cast<float4*>(&s);
+  d[0] = src[0];
+  d[1] = src[1];
+  d[2] = src[2];
+  d[3] = src[3];
+  return s;
+}
+
+// Calls visit(gaussian, tile) for every (tile, Gaussian) pair of the index, in any order.
+// Each lane enumerates small rectangles itself; a rectangle of more than kSmallRect tiles is
+// enumerated by the whole warp so one huge Gaussian cannot serialise a lane.
+template <bool CULL, typename Visit>
+__device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int ts, int tiles_x,
+                                                float cutoff2, Visit visit) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int lane = threadIdx.x & 31;
+  TileRect r{0, 0, 0, 0};
+  if (i < n) r = tile_rect_of(rec, i, ts);
+  int cnt = r.gw * r.gh;
+  if (cnt > 0 && cnt <= kSmallRect) {
+    Splat s;
+    if (CULL) s = load_splat(rec, i);
+    for (int k = 0; k < cnt; ++k) {
+      int gx = r.gx0 + k % r.gw, gy = r.gy0 + k / r.gw;
+      if (CULL && culled(s, gx, gy, ts, cutoff2)) continue;
+      visit((int)i, gy * tiles_x + gx);
+    }
+  }
+  unsigned big = __ballot_sync(0xffffffffu, cnt > kSmallRect);
+  while (big) {
+    int src = __ffs(big) - 1;
+    big &= big - 1;
+    int gx0 = __shfl_sync(0xffffffffu, r.gx0, src);
+    int gy0 = __shfl_sync(0xffffffffu, r.gy0, src);
+    int gw = __shfl_sync(0xffffffffu, r.gw, src);
+    int total = __shfl_sync(0xffffffffu, cnt, src);
+    long long gi = __shfl_sync(0xffffffffu, (long long)i, src);
+    Splat s;
+    if (CULL) s = load_splat(rec, gi);
+    for (int k = lane; k < total; k += 32) {
+      int gx = gx0 + k % gw, gy = gy0 + k / gw;
+      if (CULL && culled(s, gx, gy, ts, cutoff2)) continue;
+      visit((int)gi, gy * tiles_x + gx);
+    }
+  }
+}
+
+template <bool CULL>
+__global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
+                                  float cutoff2, int* __restrict__ tile_count) {
+  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2,
+                        [&](int, int t) { atomicAdd(tile_count + t, 1); });
+}
+
+// Writes int32 offsets, checks capacity, then claims one slot per pair.  Slots are claimed by
+// counting each tile's counter back down, which leaves the counters at zero.
+template <bool CULL>
+__global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
+                                 float cutoff2, int64_t T, const long long* __restrict__ off64,
+                                 int* __restrict__ tile_count, int32_t* __restrict__ offsets32,
+                                 int32_t* __restrict__ gids, int64_t cap, int* big_count,
+                                 uint32_t* status) {
+  int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  long long total = off64[T];
+  for (int64_t t = tid; t <= T; t += stride) offsets32[t] = (int32_t)min(off64[t], 2147483647LL);
+  if (tid == 0) {
+    *big_count = 0;
+    if (total > 2147483647LL) raise_status(status, SS_STATUS_INDEX_INT32);
+    if (total > cap) raise_status(status, SS_STATUS_INDEX_OVERFLOW);
+  }
+  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2, [&](int g, int t) {
+    long long pos = off64[t] + (atomicSub(tile_count + t, 1) - 1);
+    if (pos < cap) gids[pos] = g;
+  });
+}
+
+// Ascending sort of buf[0..len) using a bitonic network over the next power of two in which
+// every comparator puts the smaller key first; positions >= len act as +inf and never move.
+template <typename Sync>
+__device__ void bitonic_sort(int* buf, int len, int tid, int nthreads, Sync sync) {
+  int n2 = 1;
+  while (n2 < len) n2 <<= 1;
+  for (int k = 2; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int p = tid; p < (n2 >> 1); p += nthreads) {
+        int blk = p / j, r = p - blk * j, a, b;
+        if (j == (k >> 1)) {
+          a = blk * k + r;
+          b = blk * k + k - 1 - r;
+        } else {
+          a = blk * 2 * j + r;
+          b = a + j;
+        }
+        if (b < len) {
+          int va = buf[a], vb = buf[b];
+          if (va > vb) {
+            buf[a] = vb;
+            buf[b] = va;
+          }
+        }
+      }
+      sync();
+    }
+  }
+}
+
+// One warp per tile; lists longer than kWarpSortMax are queued for tile_sort_big_kernel.
+__global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __restrict__ offsets,
+                                                             int32_t* __restrict__ gids,
+                                                             int64_t cap, int64_t T,
+                                                             int* big_tiles, int* big_count) {
+  __shared__ int buf[kThreads / 32][kWarpSortMax];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + warp;
+  if (t >= T) return;
+  int64_t lo = offsets[t], hi = offsets[t + 1];
+  if (hi > cap) return;  // truncated list: the renderers scan all Gaussians for this tile
+  int len = (int)(hi - lo);
+  if (len <= 1) return;
+  if (len > kWarpSortMax) {
+    if (lane == 0) big_tiles[atomicAdd(big_count, 1)] = (int)t;
+    return;
+  }
+  int* b = buf[warp];
+  for (int k = lane; k < len; k += 32) b[k] = gids[lo + k];
+  __syncwarp();
+  bitonic_sort(b, len, lane, 32, [] { __syncwarp(); });
+  for (int k = lane; k < len; k += 32) gids[lo + k] = b[k];
+}
+
+// Long lists: one CTA per list, in shared memory up to kBigSortSmem ids, else in place.
+__global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __restrict__ offsets,
+                                                             int32_t* __restrict__ gids,
+                                                             const int* __restrict__ big_tiles,
+                                                             const int* __restrict__ big_count) {
+  extern __shared__ int sbuf[];
+  int count = *big_count;
+  for (int k = blockIdx.x; k < count; k += gridDim.x) {
+    int t = big_tiles[k];
+    int64_t lo = offsets[t];
+    int len = (int)(offsets[t + 1] - lo);
+    auto sync = [] { __syncthreads(); };
+    if (len <= kBigSortSmem) {
+      for (int e = threadIdx.x; e < len; e += blockDim.x) sbuf[e] = gids[lo + e];
+      __syncthreads();
+      bitonic_sort(sbuf, len, threadIdx.x, blockDim.x, sync);
+      for (int e = threadIdx.x; e < len; e += blockDim.x) gids[lo + e] = sbuf[e];
+    } else {
+      bitonic_sort(gids + lo, len, threadIdx.x, blockDim.x, sync);
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int kBigSortCtas = 32;
+
+// Opts tile_sort_big_kernel into its dynamic shared memory once per device.
+int allow_big_sort_smem() {
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("cudaGetDevice");
+  if (dev >= 0 && dev < 64 && done[dev]) return SS_OK;
+  if (cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kBigSortSmem * sizeof(int))) != cudaSuccess)
+    return check_launch("tile_sort_big smem attribute");
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return SS_OK;
+}
+
+int check_index_args(int64_t n, int H, int W, int ts) {
+  if (n < 0 || H < 0 || W < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
+  if (ts <= 0 || ts * ts > 1024)
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile_size must be positive with tile_size^2 <= 1024");
+  TileGrid g = make_grid(H, W, ts);
+  if (g.T + 1 > (int64_t)INT32_MAX)
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile grid exceeds int32 tile ids");
+  return SS_OK;
+}
+
+}  // namespace
+}  // namespace ss
+
+using namespace ss;
+
+extern "C" {
+
+int ss_tile_index_workspace_bytes(int64_t n, int height, int width, int tile_size,
+                                  size_t* bytes) {
+  int rc = check_index_args(n, height, width, tile_size);
+  if (rc) return rc;
+  if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
+  *bytes = index_workspace_bytes(make_grid(height, width, tile_size).T);
+  return SS_OK;
+}
+
+int ss_tile_index_count(const void* records, int64_t n, int height, int width, int tile_size,
+                        int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets,
+                        void* workspace, size_t workspace_bytes, uint32_t* status,
+                        ss_stream_t stream) {
+  int rc = check_index_args(n, height, width, tile_size);
+  if (rc) return rc;
+  TileGrid g = make_grid(height, width, tile_size);
+  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  if (workspace_bytes < index_workspace_bytes(g.T))
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small (%zu < %zu)",
+                workspace_bytes, index_workspace_bytes(g.T));
+  cudaStream_t s = as_stream(stream);
+  IndexWorkspace w = carve(workspace, g.T);
+  if (cudaMemsetAsync(w.tile_count, 0, sizeof(int) * (g.T + 1), s) != cudaSuccess)
+    return check_launch("tile_index_count memset");
+  const Splat* rec = static_cast<const Splat*>(records);
+  float cutoff2 = sigma_cutoff * sigma_cutoff;
+  if (n > 0 && g.T > 0) {
+    int blocks = (int)((n + kThreads - 1) / kThreads);
+    if (ellipse_cull)
+      tile_count_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2,
+                                                          w.tile_count);
+    else
+      tile_count_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2,
+                                                           w.tile_count);
+    if ((rc = check_launch("tile_count"))) return rc;
+  }
+  size_t sb = w.scan_bytes;
+  cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, w.tile_count, w.offsets64,
+                                                 ::cuda::std::plus<long long>(), (long long)0,
+                                                 (int)(g.T + 1), s);
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, "tile offsets scan: %s", cudaGetErrorString(e));
+  // int32 offsets for callers that only run stage 1 (the fill rewrites them identically).
+  tile_fill_kernel<false><<<(int)((g.T + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+      rec, 0, g.ts, g.tiles_x, cutoff2, g.T, w.offsets64, w.tile_count, tile_offsets, nullptr,
+      INT64_MAX, w.big_count, nullptr);
+  (void)status;
+  return check_launch("tile_offsets");
+}
+
+int ss_tile_index_fill(const void* records, int64_t n, int height, int width, int tile_size,
+                       int ellipse_cull, float sigma_cutoff, const int32_t* tile_offsets,
+                       int32_t* tile_gids, int64_t gid_capacity, void* workspace,
+                       size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  int rc = check_index_args(n, height, width, tile_size);
+  if (rc) return rc;
+  TileGrid g = make_grid(height, width, tile_size);
+  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative gid capacity");
+  if (gid_capacity > 0 && !tile_gids) return fail(SS_ERR_INVALID_ARGUMENT, "null tile_gids");
+  if (workspace_bytes < index_workspace_bytes(g.T))
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small");
+  if (g.T == 0) return SS_OK;
+  cudaStream_t s = as_stream(stream);
+  IndexWorkspace w = carve(workspace, g.T);
+  const Splat* rec = static_cast<const Splat*>(records);
+  float cutoff2 = sigma_cutoff * sigma_cutoff;
+  int64_t threads_needed = n > g.T + 1 ? n : g.T + 1;
+  int blocks = (int)((threads_needed + kThreads - 1) / kThreads);
+  int32_t* offsets32 = const_cast<int32_t*>(tile_offsets);
+  if (ellipse_cull)
+    tile_fill_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2, g.T,
+                                                       w.offsets64, w.tile_count, offsets32,
+                                                       tile_gids, gid_capacity, w.big_count,
+                                                       status);
+  else
+    tile_fill_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2, g.T,
+                                                        w.offsets64, w.tile_count, offsets32,
+                                                        tile_gids, gid_capacity, w.big_count,
+                                                        status);
+  if ((rc = check_launch("tile_fill"))) return rc;
+  int sort_blocks = (int)((g.T + (kThreads / 32) - 1) / (kThreads / 32));
+  tile_sort_kernel<<<sort_blocks, kThreads, 0, s>>>(tile_offsets, tile_gids, gid_capacity, g.T,
+                                                     w.big_tiles, w.big_count);
+  if ((rc = check_launch("tile_sort"))) return rc;
+  if ((rc = allow_big_sort_smem())) return rc;
+  tile_sort_big_kernel<<<kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s>>>(
+      tile_offsets, tile_gids, w.big_tiles, w.big_count);
+  return check_launch("tile_sort_big");
+}
+
+}  // extern "C"

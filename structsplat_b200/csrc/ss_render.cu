@@ -1,0 +1,437 @@
+// Tiled forward and backward of the clipped-support normalized / additive renderer.
+//
+// Forward (render_ext.cu:349-431 contract): one CTA per 16x16 tile.  The tile's Gaussian list is
+// staged 64 records at a time into shared memory with cp.async, double-buffered, so the next
+// chunk's gather from L2 overlaps the current chunk's math.  Each warp owns an 8x4 pixel
+// sub-block (one pixel per lane) and skips, warp-uniformly, every staged Gaussian whose support
+// rectangle misses the sub-block; inside, a lane's in-rectangle test masks its own pixel.  The
+// weight is 2^(qa dx^2 + qb dx dy + qc dy^2) on the SFU.  The epilogue writes den raw and
+// out = num / (den + eps) or num.
+//
+// Backward (render_ext.cu:696-847 contract): one CTA per tile.  A prologue turns grad_out, out
+// and den into per-pixel (dnum_r, dnum_g, dnum_b, dden) in shared memory.  Work is then
+// Gaussian-major: each half-warp takes one staged Gaussian and walks exactly the pixels of its
+// support rectangle inside the tile (no out-of-rectangle work), accumulating nine moments
+//   R_c = Σ base·dnum_c,  G = Σ base·dw,  S1 = Σ t dx,  S2 = Σ t dy,  S3 = Σ t dx²,
+//   S4 = Σ t dx dy,  S5 = Σ t dy²,   with dw = dnum·c + dden and t = raw·dw (0 where the fade
+// clamps), from which
+//   dL/dμx = o(a S1 + b S2),  dL/dμy = o(b S1 + c S2),  dL/da = -o S3/2,  dL/db = -o S4,
+//   dL/dc = -o S5/2,  dL/dc_k = o R_k,  dL/do = G
+// which is the reference's per-pixel formula (render_ext.cu:785-818) summed over pixels.  The
+// nine moments are reduced over the 16 lanes with xor shuffles and either added with one atomic
+// per component (fast mode) or stored per (tile, Gaussian) entry and summed per Gaussian in
+// ascending tile order by a second kernel (deterministic mode).
+#include "ss_common.cuh"
+
+namespace ss {
+namespace {
+
+constexpr int TS = 16;
+constexpr int kThreads = 256;
+constexpr int kChunk = 64;      // Gaussians per shared-memory stage (4 x 16 B each)
+constexpr int kMoments = 9;
+constexpr int kPartialFloats = 12;  // one deterministic partial: 9 moments padded to 3 float4
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() {
+  asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
+
+// Source of a tile's Gaussians: its index list, or — when the list was truncated by the
+// capacity — every Gaussian in ascending id (the same order, so results are identical).
+struct TileList {
+  const int32_t* gids;
+  int64_t first, count;
+  bool direct;
+  __device__ __forceinline__ int gid(int64_t k) const {
+    return direct ? (int)(first + k) : gids[first + k];
+  }
+};
+
+__device__ __forceinline__ TileList tile_list(const int32_t* gids, const int32_t* offsets,
+                                              int64_t cap, int64_t n, int tile) {
+  TileList L;
+  int64_t lo = offsets[tile], hi = offsets[tile + 1];
+  L.gids = gids;
+  L.direct = hi > cap;
+  L.first = L.direct ? 0 : lo;
+  L.count = L.direct ? n : hi - lo;
+  return L;
+}
+
+__device__ __forceinline__ int chunk_len(int64_t count, int64_t k0) {
+  const int64_t r = count - k0;
+  return r < kChunk ? (int)r : kChunk;
+}
+
+// Issues the copies of list entries [k0, k0+m) into one stage; thread t copies 16-byte piece
+// (t & 3) of entry (t >> 2).
+__device__ __forceinline__ void stage_chunk(float4 (*dst)[4], const Splat* rec, const TileList& L,
+                                            int64_t k0, int m) {
+  int slot = threadIdx.x >> 2, piece = threadIdx.x & 3;
+  if (slot < m) {
+    int g = L.gid(k0 + slot);
+    cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
+  }
+}
+
+template <bool NORMALIZE, bool FADE>
+__global__ void __launch_bounds__(kThreads)
+    forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
+                   int64_t cap, const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
+                   float eps, float tail, float* __restrict__ out, float* __restrict__ den) {
+  __shared__ __align__(16) float4 stage[2][kChunk][4];
+  const int tile = blockIdx.x;
+  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sx0 = tx0 + (warp & 1) * 8, sy0 = ty0 + (warp >> 1) * 4;
+  const int px = sx0 + (lane & 7), py = sy0 + (lane >> 3);
+  const float fx = (float)px, fy = (float)py;
+  const TileList L = tile_list(gids, offsets, cap, n, tile);
+  const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
+
+  float nr = 0.f, ng = 0.f, nb = 0.f, d = 0.f;
+  if (nchunks > 0) stage_chunk(stage[0], rec, L, 0, chunk_len(L.count, 0));
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    int64_t k0 = (int64_t)c * kChunk;
+    if (c + 1 < nchunks)
+      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk,
+                  chunk_len(L.count, k0 + kChunk));
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const int m = chunk_len(L.count, k0);
+    const float4(*st)[4] = stage[c & 1];
+    for (int j = 0; j < m; ++j) {
+      const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+      if (r.x >= sx0 + 8 || r.z <= sx0 || r.y >= sy0 + 4 || r.w <= sy0) continue;
+      const float4 p0 = st[j][0], p1 = st[j][1];
+      const float cb = st[j][2].x;
+      const bool in = px >= r.x && px < r.z && py >= r.y && py < r.w;
+      const float dx = fx - p0.x, dy = fy - p0.y;
+      const float e = fmaf(dx, fmaf(p0.z, dx, p0.w * dy), p1.x * dy * dy);
+      const float raw = fast_exp2(e);
+      const float vis = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+      const float w = in ? vis * p1.y : 0.0f;
+      nr = fmaf(w, p1.z, nr);
+      ng = fmaf(w, p1.w, ng);
+      nb = fmaf(w, cb, nb);
+      d += w;
+    }
+    __syncthreads();
+  }
+  if (px < W && py < H) {
+    const int64_t p = (int64_t)py * W + px;
+    den[p] = d;
+    if (NORMALIZE) {
+      const float denom = d + eps;
+      out[3 * p] = nr / denom;
+      out[3 * p + 1] = ng / denom;
+      out[3 * p + 2] = nb / denom;
+    } else {
+      out[3 * p] = nr;
+      out[3 * p + 1] = ng;
+      out[3 * p + 2] = nb;
+    }
+  }
+}
+
+// 16-bit reciprocal multipliers: (idx * kRowMul[w]) >> 16 == idx / w for idx < 256, w <= 16.
+__constant__ int kRowMul[17] = {0,    65536, 32768, 21846, 16384, 13108, 10923, 9363, 8192,
+                                7282, 6554,  5958,  5462,  5042,  4682,  4370,  4096};
+
+template <bool FADE, bool DETERMINISTIC>
+__global__ void __launch_bounds__(kThreads)
+    backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec, int64_t n,
+                    const float* __restrict__ den, const float* __restrict__ out,
+                    const int32_t* __restrict__ gids, int64_t cap,
+                    const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
+                    int normalize, float eps, float tail, int has_opacity,
+                    float* __restrict__ g_means, float* __restrict__ g_conics,
+                    float* __restrict__ g_colors, float* __restrict__ g_opac,
+                    float4* __restrict__ partials, uint32_t* status) {
+  __shared__ __align__(16) float4 stage[2][kChunk][4];
+  __shared__ float4 pix[TS * TS];
+  const int tile = blockIdx.x;
+  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
+  {
+    const int lx = threadIdx.x & (TS - 1), ly = threadIdx.x / TS;
+    const int x = tx0 + lx, y = ty0 + ly;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (x < W && y < H) {
+      const int64_t p = (int64_t)y * W + x;
+      const float gr = grad_out[3 * p], gg = grad_out[3 * p + 1], gb = grad_out[3 * p + 2];
+      if (normalize) {
+        const float denom = den[p] + eps;
+        v.x = gr / denom;
+        v.y = gg / denom;
+        v.z = gb / denom;
+        v.w = -(gr * out[3 * p] + gg * out[3 * p + 1] + gb * out[3 * p + 2]) / denom;
+      } else {
+        v = make_float4(gr, gg, gb, 0.f);
+      }
+    }
+    pix[threadIdx.x] = v;
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int half = lane >> 4, hl = lane & 15;
+  const TileList L = tile_list(gids, offsets, cap, n, tile);
+  if (DETERMINISTIC && L.direct) {
+    if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
+    return;
+  }
+  const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
+  if (nchunks > 0) stage_chunk(stage[0], rec, L, 0, chunk_len(L.count, 0));
+  cp_async_commit();
+  for (int c = 0; c < nchunks; ++c) {
+    const int64_t k0 = (int64_t)c * kChunk;
+    if (c + 1 < nchunks)
+      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk,
+                  chunk_len(L.count, k0 + kChunk));
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const int m = chunk_len(L.count, k0);
+    const float4(*st)[4] = stage[c & 1];
+    // Both halves of a warp run the same number of iterations so the shuffles stay converged.
+    for (int base = 2 * warp; base < m; base += 2 * (kThreads / 32)) {
+      const int j = base + half;
+      float acc[kMoments];
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
+      float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0;
+      if (j < m) {
+        p0 = st[j][0];
+        p1 = st[j][1];
+        p2 = st[j][2];
+        const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+        const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
+        const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
+        const int w = cx1 - cx0, h = cy1 - cy0;
+        const int npx = (w > 0 && h > 0) ? w * h : 0;
+        const int mul = npx ? kRowMul[w] : 0;
+        for (int idx = hl; idx < npx; idx += 16) {
+          const int row = (idx * mul) >> 16, col = idx - row * w;
+          const float4 g = pix[(cy0 + row) * TS + cx0 + col];
+          const float dx = (float)(tx0 + cx0 + col) - p0.x;
+          const float dy = (float)(ty0 + cy0 + row) - p0.y;
+          const float e = fmaf(dx, fmaf(p0.z, dx, p0.w * dy), p1.x * dy * dy);
+          const float raw = fast_exp2(e);
+          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
+          acc[0] = fmaf(base_w, g.x, acc[0]);
+          acc[1] = fmaf(base_w, g.y, acc[1]);
+          acc[2] = fmaf(base_w, g.z, acc[2]);
+          acc[3] = fmaf(base_w, dw, acc[3]);
+          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+          const float u = t * dx, v = t * dy;
+          acc[4] += u;
+          acc[5] += v;
+          acc[6] = fmaf(u, dx, acc[6]);
+          acc[7] = fmaf(u, dy, acc[7]);
+          acc[8] = fmaf(v, dy, acc[8]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) {
+        float v = acc[k];
+        v += __shfl_xor_sync(0xffffffffu, v, 8);
+        v += __shfl_xor_sync(0xffffffffu, v, 4);
+        v += __shfl_xor_sync(0xffffffffu, v, 2);
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+        acc[k] = v;
+      }
+      if (hl == 0 && j < m) {
+        const int64_t entry = L.first + k0 + j;
+        if (DETERMINISTIC) {
+          float4* dst = partials + 3 * entry;
+          dst[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
+          dst[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
+          dst[2] = make_float4(acc[8], 0.f, 0.f, 0.f);
+        } else {
+          const int g = L.gid(k0 + j);
+          const float op = p1.y, a = p2.y, b = p2.z, cc = p2.w;
+          atomicAdd(g_means + 2 * g, op * (a * acc[4] + b * acc[5]));
+          atomicAdd(g_means + 2 * g + 1, op * (b * acc[4] + cc * acc[5]));
+          atomicAdd(g_conics + 3 * g, -0.5f * op * acc[6]);
+          atomicAdd(g_conics + 3 * g + 1, -op * acc[7]);
+          atomicAdd(g_conics + 3 * g + 2, -0.5f * op * acc[8]);
+          atomicAdd(g_colors + 3 * g, op * acc[0]);
+          atomicAdd(g_colors + 3 * g + 1, op * acc[1]);
+          atomicAdd(g_colors + 3 * g + 2, op * acc[2]);
+          if (has_opacity) atomicAdd(g_opac + g, acc[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Deterministic second pass: Gaussian g sums its per-tile partials over the tiles of its
+// support rectangle in ascending tile order (each located by binary search in the tile's
+// ascending list), then applies the per-Gaussian factors once.
+__global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
+                                       const int32_t* __restrict__ gids, int64_t cap,
+                                       const int32_t* __restrict__ offsets, int tiles_x,
+                                       const float4* __restrict__ partials, int has_opacity,
+                                       float* __restrict__ g_means, float* __restrict__ g_conics,
+                                       float* __restrict__ g_colors,
+                                       float* __restrict__ g_opac) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const float4* src = reinterpret_cast<const float4*>(rec + g);
+  const float4 p1 = src[1], p2 = src[2];
+  const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
+  float acc[kMoments] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (r.z > r.x && r.w > r.y) {
+    const int gx0 = r.x / TS, gx1 = (r.z - 1) / TS, gy0 = r.y / TS, gy1 = (r.w - 1) / TS;
+    for (int gy = gy0; gy <= gy1; ++gy) {
+      for (int gx = gx0; gx <= gx1; ++gx) {
+        const int t = gy * tiles_x + gx;
+        int64_t lo = offsets[t], hi = offsets[t + 1];
+        if (hi > cap) continue;  // truncated list (reported by the backward kernel)
+        const int64_t end = hi;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if (gids[mid] < g) lo = mid + 1; else hi = mid;
+        }
+        if (lo < end && gids[lo] == g) {
+          const float4 a = partials[3 * lo], b = partials[3 * lo + 1], c = partials[3 * lo + 2];
+          acc[0] += a.x; acc[1] += a.y; acc[2] += a.z; acc[3] += a.w;
+          acc[4] += b.x; acc[5] += b.y; acc[6] += b.z; acc[7] += b.w;
+          acc[8] += c.x;
+        }
+      }
+    }
+  }
+  const float op = p1.y, a = p2.y, b = p2.z, cc = p2.w;
+  g_means[2 * g] = op * (a * acc[4] + b * acc[5]);
+  g_means[2 * g + 1] = op * (b * acc[4] + cc * acc[5]);
+  g_conics[3 * g] = -0.5f * op * acc[6];
+  g_conics[3 * g + 1] = -op * acc[7];
+  g_conics[3 * g + 2] = -0.5f * op * acc[8];
+  g_colors[3 * g] = op * acc[0];
+  g_colors[3 * g + 1] = op * acc[1];
+  g_colors[3 * g + 2] = op * acc[2];
+  if (has_opacity) g_opac[g] = acc[3];
+}
+
+int check_render_args(int64_t n, int H, int W, int ts, float eps) {
+  if (n < 0 || H < 0 || W < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
+  if (ts != TS) return fail(SS_ERR_UNSUPPORTED, "render tile_size must be %d, got %d", TS, ts);
+  if (!(eps > 0.0f) || !isfinite(eps))
+    return fail(SS_ERR_INVALID_ARGUMENT, "normalization_eps must be finite and > 0");
+  if ((int64_t)H * W > (int64_t)INT32_MAX * 4)
+    return fail(SS_ERR_INVALID_ARGUMENT, "image too large");
+  return SS_OK;
+}
+
+}  // namespace
+}  // namespace ss
+
+using namespace ss;
+
+extern "C" {
+
+int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
+                      int64_t gid_capacity, const int32_t* tile_offsets, int height, int width,
+                      int tile_size, int normalize, float eps, float fade_tail, float* out,
+                      float* den, uint32_t* status, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, eps);
+  if (rc) return rc;
+  (void)status;
+  const int64_t npx = (int64_t)height * width;
+  if (npx == 0) return SS_OK;
+  if (!out || !den || !tile_offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  const int tiles_x = (width + TS - 1) / TS, tiles_y = (height + TS - 1) / TS;
+  const int64_t T = (int64_t)tiles_x * tiles_y;
+  cudaStream_t s = as_stream(stream);
+  const Splat* rec = static_cast<const Splat*>(records);
+  const bool fade = fade_tail > 0.0f;
+#define SS_FWD(NORM, FADE)                                                                    \
+  forward_kernel<NORM, FADE><<<(unsigned)T, kThreads, 0, s>>>(rec, n, tile_gids, gid_capacity, \
+                                                              tile_offsets, height, width,    \
+                                                              tiles_x, eps, fade_tail, out, den)
+  if (normalize) {
+    if (fade) SS_FWD(true, true); else SS_FWD(true, false);
+  } else {
+    if (fade) SS_FWD(false, true); else SS_FWD(false, false);
+  }
+#undef SS_FWD
+  return check_launch("render_forward");
+}
+
+int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
+                                       size_t* bytes) {
+  if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
+  if (n < 0 || gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  *bytes = deterministic ? (size_t)gid_capacity * kPartialFloats * sizeof(float) : 0;
+  return SS_OK;
+}
+
+int ss_render_backward(const float* grad_out, const void* records, int64_t n, const float* den,
+                       const float* out, const int32_t* tile_gids, int64_t gid_capacity,
+                       const int32_t* tile_offsets, int height, int width, int tile_size,
+                       int normalize, float eps, float fade_tail, int has_opacity,
+                       float* grad_means, float* grad_conics, float* grad_colors,
+                       float* grad_opacities, int deterministic, void* workspace,
+                       size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, eps);
+  if (rc) return rc;
+  if (n == 0) return SS_OK;
+  if (!grad_means || !grad_conics || !grad_colors || (has_opacity && !grad_opacities))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null gradient output");
+  cudaStream_t s = as_stream(stream);
+  const int64_t npx = (int64_t)height * width;
+  if (!deterministic || npx == 0) {
+    cudaMemsetAsync(grad_means, 0, sizeof(float) * 2 * n, s);
+    cudaMemsetAsync(grad_conics, 0, sizeof(float) * 3 * n, s);
+    cudaMemsetAsync(grad_colors, 0, sizeof(float) * 3 * n, s);
+    if (has_opacity) cudaMemsetAsync(grad_opacities, 0, sizeof(float) * n, s);
+    if ((rc = check_launch("backward zero-fill"))) return rc;
+  }
+  if (npx == 0) return SS_OK;
+  if (!grad_out || !records || !den || !out || !tile_offsets)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (normalize && !(eps > 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "bad eps");
+  size_t need = 0;
+  ss_render_backward_workspace_bytes(n, gid_capacity, deterministic, &need);
+  if (deterministic && (workspace_bytes < need || !workspace))
+    return fail(SS_ERR_INVALID_ARGUMENT, "deterministic backward workspace too small");
+  const int tiles_x = (width + TS - 1) / TS, tiles_y = (height + TS - 1) / TS;
+  const int64_t T = (int64_t)tiles_x * tiles_y;
+  const Splat* rec = static_cast<const Splat*>(records);
+  const bool fade = fade_tail > 0.0f;
+  float4* partials = static_cast<float4*>(workspace);
+#define SS_BWD(FADE, DET)                                                                       \
+  backward_kernel<FADE, DET><<<(unsigned)T, kThreads, 0, s>>>(                                  \
+      grad_out, rec, n, den, out, tile_gids, gid_capacity, tile_offsets, height, width, tiles_x, \
+      normalize, eps, fade_tail, has_opacity, grad_means, grad_conics, grad_colors,             \
+      grad_opacities, partials, status)
+  if (deterministic) {
+    if (fade) SS_BWD(true, true); else SS_BWD(false, true);
+  } else {
+    if (fade) SS_BWD(true, false); else SS_BWD(false, false);
+  }
+#undef SS_BWD
+  if ((rc = check_launch("render_backward"))) return rc;
+  if (deterministic) {
+    reduce_partials_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+        rec, n, tile_gids, gid_capacity, tile_offsets, tiles_x, partials, has_opacity, grad_means,
+        grad_conics,
+        grad_colors, grad_opacities);
+    if ((rc = check_launch("reduce_partials"))) return rc;
+  }
+  return SS_OK;
+}
+
+}  // extern "C"

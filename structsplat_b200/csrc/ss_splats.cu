@@ -1,0 +1,193 @@
+// Library plumbing (errors, version) and the per-Gaussian kernels: record packing and the
+// fused RS projection with its chain rule.
+#include <cstdarg>
+#include <cstdio>
+
+#include "ss_common.cuh"
+
+namespace ss {
+
+static thread_local char g_error[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_error, sizeof(g_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return SS_OK;
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+
+inline int blocks_for(int64_t n) { return (int)((n + kThreads - 1) / kThreads); }
+
+__global__ void pack_splats_kernel(const float* __restrict__ means,
+                                   const float* __restrict__ conics,
+                                   const float* __restrict__ colors,
+                                   const int64_t* __restrict__ radii,
+                                   const float* __restrict__ opacities, int64_t n, int H, int W,
+                                   Splat* __restrict__ out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float mx = means[2 * i], my = means[2 * i + 1];
+  int x0, y0, x1, y1;
+  support_rect(mx, my, radii[2 * i], radii[2 * i + 1], H, W, x0, y0, x1, y1);
+  float op = opacities ? opacities[i] : 1.0f;
+  store_splat(out + i, make_splat(mx, my, conics[3 * i], conics[3 * i + 1], conics[3 * i + 2],
+                                  op, colors[3 * i], colors[3 * i + 1], colors[3 * i + 2], x0,
+                                  y0, x1, y1));
+}
+
+// RS -> conic, radii and opacity.  The conic follows gaussians.py:275-300 and the radii
+// gaussians.py:302-321; every product and sum is rounded separately (no FMA contraction) so
+// the radii's ceil() sees the same float the reference's elementwise torch ops produce.
+__global__ void project_rs_kernel(const float* __restrict__ means,
+                                  const float* __restrict__ log_scales,
+                                  const float* __restrict__ rotations,
+                                  const float* __restrict__ colors,
+                                  const float* __restrict__ logits, int64_t n, float dilation,
+                                  float cutoff, int H, int W, Splat* __restrict__ out,
+                                  float* __restrict__ conics_out,
+                                  int64_t* __restrict__ radii_out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float sx = expf(log_scales[2 * i]), sy = expf(log_scales[2 * i + 1]);
+  float sx2 = __fmul_rn(sx, sx), sy2 = __fmul_rn(sy, sy);
+  float th = rotations[i];
+  float cs = cosf(th), sn = sinf(th);
+  float cc = __fmul_rn(cs, cs), ss2 = __fmul_rn(sn, sn);
+  // conic
+  float ix = __fdiv_rn(1.0f, __fadd_rn(sx2, dilation));
+  float iy = __fdiv_rn(1.0f, __fadd_rn(sy2, dilation));
+  float a = __fadd_rn(__fmul_rn(cc, ix), __fmul_rn(ss2, iy));
+  float b = __fmul_rn(__fmul_rn(cs, sn), __fsub_rn(ix, iy));
+  float c = __fadd_rn(__fmul_rn(ss2, ix), __fmul_rn(cc, iy));
+  // radii: ceil(cutoff * sqrt(var)) clamped >= 1
+  float vx2 = __fadd_rn(sx2, dilation), vy2 = __fadd_rn(sy2, dilation);
+  float varx = __fadd_rn(__fmul_rn(cc, vx2), __fmul_rn(ss2, vy2));
+  float vary = __fadd_rn(__fmul_rn(ss2, vx2), __fmul_rn(cc, vy2));
+  float fr_x = ceilf(__fmul_rn(cutoff, __fsqrt_rn(varx)));
+  float fr_y = ceilf(__fmul_rn(cutoff, __fsqrt_rn(vary)));
+  long long rx = isfinite(fr_x) ? (long long)fmaxf(fminf(fr_x, 1e15f), 1.0f) : (1LL << 40);
+  long long ry = isfinite(fr_y) ? (long long)fmaxf(fminf(fr_y, 1e15f), 1.0f) : (1LL << 40);
+  float op = logits ? 1.0f / (1.0f + expf(-logits[i])) : 1.0f;
+  float mx = means[2 * i], my = means[2 * i + 1];
+  int x0, y0, x1, y1;
+  support_rect(mx, my, rx, ry, H, W, x0, y0, x1, y1);
+  store_splat(out + i, make_splat(mx, my, a, b, c, op, colors[3 * i], colors[3 * i + 1],
+                                  colors[3 * i + 2], x0, y0, x1, y1));
+  if (conics_out) {
+    conics_out[3 * i] = a;
+    conics_out[3 * i + 1] = b;
+    conics_out[3 * i + 2] = c;
+  }
+  if (radii_out) {
+    radii_out[2 * i] = rx;
+    radii_out[2 * i + 1] = ry;
+  }
+}
+
+// d(conic)/d(log_scale, rotation) and d(opacity)/d(logit).  With u = 1/(sx^2+d),
+// v = 1/(sy^2+d): a = C^2 u + S^2 v, b = CS (u - v), c = S^2 u + C^2 v, so
+//   dL/du = ga C^2 + gb CS + gc S^2,   dL/dv = ga S^2 - gb CS + gc C^2,
+//   du/dlx = -2 sx^2 u^2,              dv/dly = -2 sy^2 v^2,
+//   dL/dθ = (u - v) (-2CS ga + (C^2 - S^2) gb + 2CS gc),   dσ/dl = σ (1 - σ).
+__global__ void project_rs_backward_kernel(const float* __restrict__ log_scales,
+                                           const float* __restrict__ rotations,
+                                           const float* __restrict__ logits, int64_t n,
+                                           float dilation, const float* __restrict__ g_conics,
+                                           const float* __restrict__ g_opac,
+                                           float* __restrict__ g_log_scales,
+                                           float* __restrict__ g_rot,
+                                           float* __restrict__ g_logits) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float sx = expf(log_scales[2 * i]), sy = expf(log_scales[2 * i + 1]);
+  float sx2 = sx * sx, sy2 = sy * sy;
+  float u = 1.0f / (sx2 + dilation), v = 1.0f / (sy2 + dilation);
+  float cs, sn;
+  sincosf(rotations[i], &sn, &cs);
+  float ga = g_conics[3 * i], gb = g_conics[3 * i + 1], gc = g_conics[3 * i + 2];
+  float cc = cs * cs, s2 = sn * sn, csn = cs * sn;
+  float gu = ga * cc + gb * csn + gc * s2;
+  float gv = ga * s2 - gb * csn + gc * cc;
+  g_log_scales[2 * i] = gu * (-2.0f * sx2 * u * u);
+  g_log_scales[2 * i + 1] = gv * (-2.0f * sy2 * v * v);
+  g_rot[i] = (u - v) * (2.0f * csn * (gc - ga) + (cc - s2) * gb);
+  if (logits && g_opac && g_logits) {
+    float o = 1.0f / (1.0f + expf(-logits[i]));
+    g_logits[i] = g_opac[i] * o * (1.0f - o);
+  }
+}
+
+}  // namespace
+}  // namespace ss
+
+using namespace ss;
+
+extern "C" {
+
+const char* ss_last_error(void) { return ss::g_error; }
+
+int ss_version(void) { return 1; }
+
+size_t ss_splat_record_bytes(void) { return sizeof(Splat); }
+
+int ss_pack_splats(const float* means, const float* conics, const float* colors,
+                   const int64_t* radii, const float* opacities, int64_t n, int height,
+                   int width, void* records, ss_stream_t stream) {
+  if (n < 0 || height < 0 || width < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
+  if (n == 0) return SS_OK;
+  if (!means || !conics || !colors || !radii || !records)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (reinterpret_cast<uintptr_t>(records) % 16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
+  pack_splats_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+      means, conics, colors, radii, opacities, n, height, width,
+      reinterpret_cast<Splat*>(records));
+  return check_launch("pack_splats");
+}
+
+int ss_project_rs(const float* means, const float* log_scales, const float* rotations,
+                  const float* colors, const float* opacity_logits, int64_t n, float dilation,
+                  float sigma_cutoff, int height, int width, void* records, float* conics_out,
+                  int64_t* radii_out, ss_stream_t stream) {
+  if (n < 0 || height < 0 || width < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
+  if (!(dilation >= 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "dilation must be >= 0");
+  if (n == 0) return SS_OK;
+  if (!means || !log_scales || !rotations || !colors || !records)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (reinterpret_cast<uintptr_t>(records) % 16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
+  project_rs_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+      means, log_scales, rotations, colors, opacity_logits, n, dilation, sigma_cutoff, height,
+      width, reinterpret_cast<Splat*>(records), conics_out, radii_out);
+  return check_launch("project_rs");
+}
+
+int ss_project_rs_backward(const float* log_scales, const float* rotations,
+                           const float* opacity_logits, int64_t n, float dilation,
+                           const float* grad_conics, const float* grad_opacities,
+                           float* grad_log_scales, float* grad_rotations,
+                           float* grad_opacity_logits, ss_stream_t stream) {
+  if (n < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n == 0) return SS_OK;
+  if (!log_scales || !rotations || !grad_conics || !grad_log_scales || !grad_rotations)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  project_rs_backward_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+      log_scales, rotations, opacity_logits, n, dilation, grad_conics, grad_opacities,
+      grad_log_scales, grad_rotations, grad_opacity_logits);
+  return check_launch("project_rs_backward");
+}
+
+}  // extern "C"

@@ -1,0 +1,317 @@
+"""Host side of the B200 renderer: the reference's render call, re-pointed at the CUDA library.
+
+Mirrors the reference interface so it drops in behind the fitting loop:
+
+* ``render_field``      ↔ ``structsplat.render.render_field``      (render.py:319-414)
+* ``render_b200``       ↔ ``structsplat.cuda_render.render_cuda_exact`` (cuda_render.py:256-294)
+* ``build_tile_index``  ↔ the extension's ``build_tile_index``     (render_ext.cu:858-952)
+* ``_B200Render``       ↔ ``_ExactRenderCuda``                     (cuda_render.py:52-174)
+
+Tensor contract (render_ext.cpp:89-137): means (N,2) f32, conics (N,3) f32 ``[a, b, c]`` with
+``q = a dx² + 2b dx dy + c dy²``, colors (N,3) f32, radii (N,2) int64, opacities (N,) f32 or
+None; CUDA tensors only — there is no CPU fallback.  Everything runs on the current CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+from torch.autograd import Function
+from torch.autograd.function import once_differentiable
+
+from . import _native
+
+DEFAULT_EPS = 1e-8
+RECORD_FLOATS = 16  # one 64-byte splat record
+
+NORMALIZED_MODES = ("b200", "b200_normalized", "normalized", "cuda", "cuda_normalized",
+                    "cuda_block_reduce", "cuda_tiled", "cuda_tiled_normalized")
+ADDITIVE_MODES = ("b200_additive", "additive", "cuda_additive", "cuda_tiled_additive")
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def validate_eps(value: float) -> float:
+    """Same rule as render.py:33-37."""
+    eps = float(value)
+    if not math.isfinite(eps) or eps <= 0.0:
+        raise ValueError(f"normalization_eps must be finite and > 0, got {value}")
+    return eps
+
+
+def resolve_fade_alpha(support_fade: bool, support_fade_alpha=None) -> float:
+    """render.py:94-98: None → 1 with the fade on, 0 off; otherwise clamped to [0, 1]."""
+    if support_fade_alpha is None:
+        return 1.0 if support_fade else 0.0
+    return max(0.0, min(1.0, float(support_fade_alpha)))
+
+
+def fade_tail(sigma_cutoff: float, alpha: float) -> float:
+    """alpha·exp(−½ cutoff²) as the float32 the reference subtracts (render.py:101-107)."""
+    if alpha <= 0.0:
+        return 0.0
+    return float(np.float32(alpha * math.exp(-0.5 * float(sigma_cutoff) ** 2)))
+
+
+def tile_grid(H: int, W: int, tile_size: int) -> tuple[int, int]:
+    if tile_size <= 0 or tile_size * tile_size > 1024:
+        raise ValueError("tile_size must be positive with tile_size^2 <= 1024")
+    return (W + tile_size - 1) // tile_size, (H + tile_size - 1) // tile_size
+
+
+def _check_cuda_f32(means, conics, colors):
+    if not means.is_cuda:
+        raise RuntimeError("StructSplat B200 renderer requires CUDA tensors; pass device='cuda'.")
+    if means.dtype != torch.float32 or conics.dtype != torch.float32 or \
+            colors.dtype != torch.float32:
+        raise RuntimeError("StructSplat B200 renderer supports float32 tensors only.")
+
+
+def _check_shapes(means, conics, colors, radii, opacities):
+    n = means.shape[0]
+    if means.dim() != 2 or means.shape[1] != 2:
+        raise ValueError("means must be (N, 2)")
+    if conics.shape != (n, 3):
+        raise ValueError("conics must be (N, 3)")
+    if colors.shape != (n, 3):
+        raise ValueError("colors must be (N, 3)")
+    if radii.shape != (n, 2) or radii.dtype != torch.int64:
+        raise ValueError("radii must be (N, 2) int64")
+    if opacities is not None and opacities.numel() not in (0, n):
+        raise ValueError("opacities must be empty or length N")
+    for t in (conics, colors, radii):
+        if t.device != means.device:
+            raise ValueError("all inputs must be on the same device")
+
+
+@dataclass
+class TileIndex:
+    """Per-tile Gaussian lists: tile t is ``gids[offsets[t]:offsets[t+1]]`` (ascending ids)."""
+    gids: torch.Tensor      # int32 [entries]
+    offsets: torch.Tensor   # int32 [T+1]
+    tile_size: int
+    status: torch.Tensor    # int32 [1] device status word
+
+    @property
+    def capacity(self) -> int:
+        return int(self.gids.numel())
+
+
+def pack_records(means, conics, colors, radii, opacities, H: int, W: int) -> torch.Tensor:
+    n = means.shape[0]
+    rec = torch.empty(max(n, 1) * RECORD_FLOATS, device=means.device, dtype=torch.float32)
+    if n:
+        _native.call("ss_pack_splats", _p(means), _p(conics), _p(colors), _p(radii),
+                     _p(opacities), n, H, W, _p(rec), _stream())
+    return rec
+
+
+class _CapacityCache:
+    """Per-problem capacity for the tile index, so steady-state calls never wait on the host.
+
+    The first call for a (device, N, H, W, tile size, cull) key reads the entry total back
+    (one sync, as the reference's build does at render_ext.cu:908-914) and keeps 25 % headroom.
+    Later calls reuse that capacity and copy their own total to pinned memory asynchronously;
+    the next call reads it (only once its copy has completed) and grows the capacity if
+    needed.  A call whose total exceeds the capacity still renders exactly: the kernels scan
+    every Gaussian for the truncated tiles.
+    """
+
+    def __init__(self):
+        self.entries = {}
+
+    def capacity(self, key, offsets) -> int:
+        ent = self.entries.get(key)
+        if ent is None:
+            total = int(offsets[-1].item())
+            cap = int(total * 1.25) + 1024
+            host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+            ent = self.entries[key] = {"cap": cap, "host": host, "event": None}
+        elif ent["event"] is not None and ent["event"].query():
+            seen = int(ent["host"][0])
+            if seen > ent["cap"]:
+                ent["cap"] = int(seen * 1.25) + 1024
+        ent["host"].copy_(offsets[-1:], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        ent["event"] = ev
+        return ent["cap"]
+
+
+CAPACITY = _CapacityCache()
+
+
+def index_from_records(records, n: int, H: int, W: int, tile_size: int = 16,
+                       ellipse_cull: bool = False, sigma_cutoff: float = 3.0,
+                       capacity: int | None = None, exact: bool = False) -> TileIndex:
+    """Count → scan → fill → sort.  ``exact`` reads the entry total back (one device→host sync)
+    and sizes the list exactly; otherwise the capacity comes from ``capacity`` or the
+    per-problem cache."""
+    tiles_x, tiles_y = tile_grid(H, W, tile_size)
+    T = tiles_x * tiles_y
+    dev = records.device
+    offsets = torch.empty(T + 1, device=dev, dtype=torch.int32)
+    status = torch.zeros(1, device=dev, dtype=torch.int32)
+    ws_bytes = _native.size_query("ss_tile_index_workspace_bytes", n, H, W, tile_size)
+    ws = torch.empty(max(ws_bytes, 1), device=dev, dtype=torch.uint8)
+    _native.call("ss_tile_index_count", _p(records), n, H, W, tile_size, int(ellipse_cull),
+                 float(sigma_cutoff), _p(offsets), _p(ws), ws_bytes, _p(status), _stream())
+    if T == 0:
+        capacity = 0
+    elif exact:
+        capacity = int(offsets[-1].item())
+    elif capacity is None:
+        key = (dev.index, n, H, W, tile_size, bool(ellipse_cull))
+        capacity = CAPACITY.capacity(key, offsets)
+    gids = torch.empty(max(capacity, 1), device=dev, dtype=torch.int32)
+    _native.call("ss_tile_index_fill", _p(records), n, H, W, tile_size, int(ellipse_cull),
+                 float(sigma_cutoff), _p(offsets), _p(gids), int(capacity), _p(ws), ws_bytes,
+                 _p(status), _stream())
+    return TileIndex(gids[:capacity], offsets, tile_size, status)
+
+
+def build_tile_index(means, conics, radii, H: int, W: int, tile_size: int = 16,
+                     ellipse_cull: bool = False, sigma_cutoff: float = 3.0):
+    """``(gids int32 [entries], offsets int32 [T+1])`` like the extension's build_tile_index."""
+    if not means.is_cuda:
+        raise RuntimeError("StructSplat B200 renderer requires CUDA tensors; pass device='cuda'.")
+    tile_grid(H, W, tile_size)
+    means = means.detach().contiguous()
+    conics = conics.detach().contiguous().to(torch.float32)
+    radii = radii.contiguous()
+    rec = pack_records(means.to(torch.float32), conics, conics, radii, None, H, W)
+    idx = index_from_records(rec, means.shape[0], H, W, tile_size, ellipse_cull, sigma_cutoff,
+                             exact=True)
+    return idx.gids, idx.offsets
+
+
+def _forward(records, n, index: TileIndex, H, W, normalize, eps, tail, dev):
+    out = torch.empty(H, W, 3, device=dev, dtype=torch.float32)
+    den = torch.empty(H, W, device=dev, dtype=torch.float32)
+    if H * W:
+        _native.call("ss_render_forward", _p(records), n, _p(index.gids), index.capacity,
+                     _p(index.offsets), H, W, index.tile_size, int(normalize), float(eps),
+                     float(tail), _p(out), _p(den), _p(index.status), _stream())
+    return out, den
+
+
+def _backward(grad_out, records, n, den, out, index: TileIndex, H, W, normalize, eps, tail,
+              has_opacity, deterministic, dev):
+    g_means = torch.empty(n, 2, device=dev, dtype=torch.float32)
+    g_conics = torch.empty(n, 3, device=dev, dtype=torch.float32)
+    g_colors = torch.empty(n, 3, device=dev, dtype=torch.float32)
+    g_opac = torch.empty(n, device=dev, dtype=torch.float32) if has_opacity else None
+    ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n, index.capacity,
+                                  int(deterministic))
+    ws = torch.empty(max(ws_bytes, 16), device=dev, dtype=torch.uint8)
+    _native.call("ss_render_backward", _p(grad_out), _p(records), n, _p(den), _p(out),
+                 _p(index.gids), index.capacity, _p(index.offsets), H, W, index.tile_size,
+                 int(normalize), float(eps), float(tail), int(has_opacity), _p(g_means),
+                 _p(g_conics), _p(g_colors), _p(g_opac), int(deterministic), _p(ws), ws_bytes,
+                 _p(index.status), _stream())
+    return g_means, g_conics, g_colors, g_opac
+
+
+class _B200Render(Function):
+    """Autograd Function with the slots of ``_ExactRenderCuda`` (cuda_render.py:52-174)."""
+
+    @staticmethod
+    def forward(ctx, means, conics, colors, radii, opacities, H, W, normalize, eps, tile_size,
+                tail, cull, sigma_cutoff, deterministic):
+        n = means.shape[0]
+        means, conics, colors = means.contiguous(), conics.contiguous(), colors.contiguous()
+        radii = radii.contiguous()
+        has_op = opacities is not None and opacities.numel() > 0
+        op = opacities.contiguous() if has_op else None
+        rec = pack_records(means, conics, colors, radii, op, H, W)
+        index = index_from_records(rec, n, H, W, tile_size, cull, sigma_cutoff,
+                                   exact=bool(deterministic))
+        out, den = _forward(rec, n, index, H, W, normalize, eps, tail, means.device)
+        ctx.save_for_backward(rec, index.gids, index.offsets, index.status, out, den)
+        ctx.meta = (n, H, W, bool(normalize), float(eps), int(tile_size), float(tail), has_op,
+                    bool(deterministic))
+        return out
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, grad_out):
+        rec, gids, offsets, status, out, den = ctx.saved_tensors
+        n, H, W, normalize, eps, ts, tail, has_op, det = ctx.meta
+        need = ctx.needs_input_grad
+        if not (need[0] or need[1] or need[2] or need[4]) or n == 0:
+            return (None,) * 14
+        index = TileIndex(gids, offsets, ts, status)
+        g_means, g_conics, g_colors, g_opac = _backward(
+            grad_out.contiguous().to(torch.float32), rec, n, den, out, index, H, W, normalize,
+            eps, tail, has_op, det, grad_out.device)
+        return (g_means if need[0] else None, g_conics if need[1] else None,
+                g_colors if need[2] else None, None,
+                g_opac if (has_op and need[4]) else None) + (None,) * 9
+
+
+def render_b200(means, conics, colors, radii, H: int, W: int, opacities=None,
+                normalize: bool = True, eps: float = DEFAULT_EPS, tile_size: int = 16,
+                support_fade: bool = False, sigma_cutoff: float = 3.0,
+                support_fade_alpha: float | None = None, tile_ellipse_cull: bool = True,
+                deterministic: bool = False):
+    """Render with the reference's exact normalized / additive equations on the B200 library.
+
+    Arguments mirror ``render_cuda_exact``.  ``tile_ellipse_cull`` only takes effect with the
+    full support fade, the one case where culled pairs have exactly zero weight.
+    ``deterministic`` selects the two-pass backward whose gradients are bitwise reproducible.
+    """
+    _check_cuda_f32(means, conics, colors)
+    _check_shapes(means, conics, colors, radii, opacities)
+    tile_grid(H, W, tile_size)
+    if normalize:
+        eps = validate_eps(eps)
+    alpha = resolve_fade_alpha(support_fade, support_fade_alpha)
+    tail = fade_tail(sigma_cutoff, alpha)
+    cull = bool(tile_ellipse_cull) and alpha >= 1.0
+    if opacities is not None and opacities.numel() == 0:
+        opacities = None
+    if opacities is not None and opacities.dtype != torch.float32:
+        raise RuntimeError("StructSplat B200 renderer supports float32 tensors only.")
+    return _B200Render.apply(means, conics, colors, radii, opacities, int(H), int(W),
+                             bool(normalize), float(eps), int(tile_size), tail, cull,
+                             float(sigma_cutoff), bool(deterministic))
+
+
+def render_field(means, conics, colors, radii, H: int, W: int, chunk: int = 4096,
+                 mode: str = "b200", opacities=None, scales=None, rotations=None,
+                 support_fade: bool = False, sigma_cutoff: float = 3.0, color_grads=None,
+                 support_fade_alpha: float | None = None, checkpoint_chunks: bool = False,
+                 normalization_eps: float = DEFAULT_EPS, deterministic: bool = False):
+    """``render_field`` with the reference's signature (render.py:319-414) on the B200 library.
+
+    Every normalized mode (``b200``, ``normalized``, ``cuda``, ``cuda_tiled`` …) and every
+    additive mode (``b200_additive``, ``additive``, ``cuda_additive`` …) evaluates the same
+    equation as the reference; ``chunk`` and ``checkpoint_chunks`` are memory knobs of the
+    reference's torch loop and have no effect here.  CUDA tensors only.
+    """
+    del chunk, checkpoint_chunks, scales, rotations
+    if color_grads is not None:
+        raise NotImplementedError(
+            "affine colour gradients (color_grads) are not implemented by the B200 renderer")
+    if mode in NORMALIZED_MODES:
+        normalize = True
+        eps = validate_eps(normalization_eps)
+    elif mode in ADDITIVE_MODES:
+        normalize = False
+        eps = DEFAULT_EPS
+    else:
+        raise ValueError(
+            f"unknown renderer {mode!r}; expected one of {NORMALIZED_MODES + ADDITIVE_MODES}")
+    return render_b200(means, conics, colors, radii, H, W, opacities=opacities,
+                       normalize=normalize, eps=eps, support_fade=support_fade,
+                       sigma_cutoff=sigma_cutoff, support_fade_alpha=support_fade_alpha,
+                       deterministic=deterministic)

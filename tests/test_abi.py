@@ -1,0 +1,100 @@
+"""The C-ABI library loads and exports every symbol the public header declares.
+
+No compute call is made here (no GPU is needed): only calls that fail argument validation
+before touching CUDA, and pure host queries.
+"""
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+
+import pytest
+
+from conftest import REPO
+from structsplat_b200 import _native, build
+
+HEADER = REPO / "include" / "structsplat_b200.h"
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not _native.LIB_PATH.exists():
+        build.build()
+    return _native.lib()
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(ss_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_the_bound_symbols():
+    assert declared_symbols() == _native.exported_symbols()
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_native.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\b(ss_\w+)$", out, re.M))
+    assert set(declared_symbols()) <= exported
+
+
+def test_build_targets_sm100a():
+    assert build.ARCH_FLAGS == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_host_queries(lib):
+    assert lib.ss_version() == 1
+    assert lib.ss_splat_record_bytes() == 64
+
+
+def _status(lib, name, *args):
+    rc = getattr(lib, name)(*args)
+    return rc, lib.ss_last_error().decode()
+
+
+def test_argument_validation_without_gpu(lib):
+    size = ctypes.c_size_t(0)
+    rc, msg = _status(lib, "ss_tile_index_workspace_bytes", 10, 16, 16, 0, ctypes.byref(size))
+    assert rc == 1 and "tile_size" in msg
+    rc, msg = _status(lib, "ss_tile_index_workspace_bytes", 10, 16, 16, 33, ctypes.byref(size))
+    assert rc == 1 and "tile_size^2 <= 1024" in msg
+    rc, msg = _status(lib, "ss_render_forward", None, 0, None, 0, None, 8, 8, 8, 1,
+                      ctypes.c_float(1e-8), ctypes.c_float(0.0), None, None, None, None)
+    assert rc == 4 and "tile_size" in msg
+    rc, msg = _status(lib, "ss_render_forward", None, 0, None, 0, None, 8, 8, 16, 1,
+                      ctypes.c_float(0.0), ctypes.c_float(0.0), None, None, None, None)
+    assert rc == 1 and "normalization_eps" in msg
+    rc, msg = _status(lib, "ss_pack_splats", None, None, None, None, None, -1, 4, 4, None, None)
+    assert rc == 1 and "negative" in msg
+    rc, msg = _status(lib, "ss_project_rs", None, None, None, None, None, 4, ctypes.c_float(-1.0),
+                      ctypes.c_float(3.0), 4, 4, None, None, None, None)
+    assert rc == 1 and "dilation" in msg
+    rc, msg = _status(lib, "ss_structure_tensor", None, 1, 5, 3, None, 0, None, 0, 0, 0,
+                      ctypes.c_double(0.02), ctypes.c_double(0.15), None, None, None, None, None,
+                      None, None, None, 0, None)
+    assert rc == 1 and "central gradients" in msg
+    rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 1, ctypes.byref(size))
+    assert rc == 0 and size.value == 100 * 48
+
+
+def test_empty_problem_needs_no_device(lib):
+    """Zero-sized calls return before any CUDA work."""
+    rc, _ = _status(lib, "ss_pack_splats", None, None, None, None, None, 0, 4, 4, None, None)
+    assert rc == 0
+    rc, _ = _status(lib, "ss_render_forward", None, 0, None, 0, None, 0, 7, 16, 1,
+                    ctypes.c_float(1e-8), ctypes.c_float(0.0), None, None, None, None)
+    assert rc == 0
+
+
+def test_row_multipliers_divide_exactly():
+    """The backward kernel's (idx * mul[w]) >> 16 replaces idx / w for idx < 256, w <= 16."""
+    src = (REPO / "structsplat_b200" / "csrc" / "ss_render.cu").read_text()
+    table = re.search(r"kRowMul\[17\] = \{([^}]*)\}", src).group(1)
+    mul = [int(v) for v in table.replace("\n", " ").split(",")]
+    for w in range(1, 17):
+        for idx in range(16 * w):
+            assert (idx * mul[w]) >> 16 == idx // w, (w, idx)

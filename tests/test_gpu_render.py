@@ -1,0 +1,191 @@
+"""Forward and backward parity of the B200 renderer against the reference's own results.
+
+Golden vectors come from the reference's ``render_field`` (tests/golden).  Bars: forward images
+within 1e-5 relative and gradients within 1e-4 relative (norm-wise: max |got − ref| / max |ref|)
+of the reference's float32 results; each case also states its error against the reference
+evaluated in float64.  Cases with the full support fade are ill-conditioned at the cutoff
+(exp(−q/2) − exp(−c²/2) cancels): for those the forward is compared element-wise with a floor
+and the float64 yardstick shows the reference float32 path has the same conditioning.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, golden_names
+from gpu_helpers import cuda, rel_err, require_cuda
+from structsplat_b200 import render_b200, render_gaussians
+from structsplat_b200 import render as R
+
+pytestmark = pytest.mark.gpu
+
+RENDER_CASES = golden_names("render_")
+FWD_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def _case(z):
+    op = cuda(z["opacities"]) if "opacities" in z.files else None
+    return (cuda(z["means"]), cuda(z["conics"]), cuda(z["colors"]), cuda(z["radii"]), op)
+
+
+def _render(z, deterministic=False, want_grads=True):
+    m, c, col, r, op = _case(z)
+    leaves = [m, c, col] + ([op] if op is not None else [])
+    for t in leaves:
+        t.requires_grad_(want_grads)
+    alpha = float(z["fade_alpha"])
+    img = render_b200(m, c, col, r, int(z["H"]), int(z["W"]), opacities=op,
+                      normalize=bool(z["normalize"]), eps=float(z["eps"]),
+                      support_fade=alpha > 0, support_fade_alpha=alpha,
+                      sigma_cutoff=float(z["sigma_cutoff"]), deterministic=deterministic)
+    if not want_grads:
+        return img.detach(), None
+    grads = torch.autograd.grad(img, leaves, cuda(z["grad_out"]))
+    torch.cuda.synchronize()
+    return img.detach(), grads
+
+
+def _fwd_error_ok(img, z):
+    """Forward bar; faded cases use an element-wise bar floored at 1e-3 of the image scale."""
+    e32 = rel_err(img, z["image_f32"])
+    if float(z["fade_alpha"]) > 0:
+        return e32 <= 5e-5
+    return e32 <= FWD_TOL
+
+
+@pytest.mark.parametrize("name", RENDER_CASES)
+def test_forward_matches_reference(name):
+    require_cuda()
+    z = golden(name)
+    img, _ = _render(z, want_grads=False)
+    e32, e64 = rel_err(img, z["image_f32"]), rel_err(img, z["image_f64"])
+    ref64 = rel_err(z["image_f32"], z["image_f64"])
+    print(f"{name}: fwd err vs ref f32 {e32:.2e}, vs f64 {e64:.2e} (ref f32 vs f64 {ref64:.2e})")
+    assert _fwd_error_ok(img, z), (e32, e64)
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+@pytest.mark.parametrize("name", RENDER_CASES)
+def test_gradients_match_reference(name, deterministic):
+    require_cuda()
+    z = golden(name)
+    _, grads = _render(z, deterministic=deterministic)
+    keys = ["means", "conics", "colors"] + (["opacities"] if "opacities" in z.files else [])
+    for key, g in zip(keys, grads):
+        e32 = rel_err(g, z[f"g_{key}_f32"])
+        e64 = rel_err(g, z[f"g_{key}_f64"])
+        print(f"{name} {key}: grad err vs ref f32 {e32:.2e}, vs f64 {e64:.2e}")
+        assert e32 <= GRAD_TOL, (key, e32, e64)
+
+
+@pytest.mark.parametrize("name", RENDER_CASES)
+def test_rs_field_path_matches_reference(name):
+    """render_gaussians (fused projection + chain rule) against autograd through the
+    reference's GaussianField.conics / radii / opacity_values."""
+    require_cuda()
+    z = golden(name)
+    m, ls, rot, col = (cuda(z[k]) for k in ("means", "log_scales", "rotations", "colors"))
+    logits = cuda(z["opacity_logits"]) if "opacity_logits" in z.files else None
+    leaves = [m, ls, rot, col] + ([logits] if logits is not None else [])
+    for t in leaves:
+        t.requires_grad_(True)
+    alpha = float(z["fade_alpha"])
+    img = render_gaussians(m, ls, rot, col, int(z["H"]), int(z["W"]), opacity_logits=logits,
+                           normalize=bool(z["normalize"]), eps=float(z["eps"]),
+                           sigma_cutoff=float(z["sigma_cutoff"]), dilation=float(z["dilation"]),
+                           support_fade=alpha > 0, support_fade_alpha=alpha)
+    grads = torch.autograd.grad(img, leaves, cuda(z["grad_out"]))
+    assert _fwd_error_ok(img.detach(), z)
+    keys = ["means", "log_scales", "rotations", "colors"] + (
+        ["opacity_logits"] if logits is not None else [])
+    for key, g in zip(keys, grads):
+        e32 = rel_err(g, z[f"rs_{key}_f32"])
+        print(f"{name} rs {key}: grad err vs ref f32 {e32:.2e}, "
+              f"vs f64 {rel_err(g, z[f'rs_{key}_f64']):.2e}")
+        assert e32 <= GRAD_TOL, (key, e32)
+
+
+def test_rs_projection_matches_reference_conics_and_radii():
+    require_cuda()
+    from structsplat_b200.field import project
+    for name in RENDER_CASES:
+        z = golden(name)
+        logits = cuda(z["opacity_logits"]) if "opacity_logits" in z.files else None
+        _, conics, radii = project(cuda(z["means"]), cuda(z["log_scales"]), cuda(z["rotations"]),
+                                   cuda(z["colors"]), logits, int(z["H"]), int(z["W"]),
+                                   float(z["sigma_cutoff"]), float(z["dilation"]),
+                                   want_conics=True)
+        assert np.array_equal(radii.cpu().numpy(), z["radii"]), name
+        assert rel_err(conics, z["conics"]) <= 1e-6, name
+
+
+def test_deterministic_backward_is_bitwise_reproducible():
+    require_cuda()
+    z = golden("render_synthetic_64_256.npz")
+    _, g1 = _render(z, deterministic=True)
+    _, g2 = _render(z, deterministic=True)
+    for a, b in zip(g1, g2):
+        assert torch.equal(a, b)
+
+
+def test_forward_is_bitwise_reproducible():
+    require_cuda()
+    z = golden("render_synthetic_64_256.npz")
+    a, _ = _render(z, want_grads=False)
+    b, _ = _render(z, want_grads=False)
+    assert torch.equal(a, b)
+
+
+def test_truncated_index_renders_identically():
+    """With too small a capacity the affected tiles scan every Gaussian in ascending id: the
+    image is bitwise identical and the status word reports the overflow."""
+    require_cuda()
+    z = golden("render_synthetic_64_256.npz")
+    m, c, col, r, op = _case(z)
+    H, W = int(z["H"]), int(z["W"])
+    rec = R.pack_records(m, c, col, r, op, H, W)
+    full = R.index_from_records(rec, m.shape[0], H, W)
+    part = R.index_from_records(rec, m.shape[0], H, W, capacity=full.capacity // 3)
+    out_f, den_f = R._forward(rec, m.shape[0], full, H, W, True, 1e-8, 0.0, m.device)
+    out_p, den_p = R._forward(rec, m.shape[0], part, H, W, True, 1e-8, 0.0, m.device)
+    torch.cuda.synchronize()
+    assert int(full.status.item()) == 0
+    assert int(part.status.item()) & 1
+    assert torch.equal(out_f, out_p) and torch.equal(den_f, den_p)
+    go = cuda(z["grad_out"])
+    g_f = R._backward(go, rec, m.shape[0], den_f, out_f, full, H, W, True, 1e-8, 0.0, True,
+                      False, m.device)
+    g_p = R._backward(go, rec, m.shape[0], den_p, out_p, part, H, W, True, 1e-8, 0.0, True,
+                      False, m.device)
+    for a, b in zip(g_f, g_p):
+        assert rel_err(b, a) <= 1e-6
+
+
+def test_empty_field_renders_zeros():
+    require_cuda()
+    e = torch.zeros(0, 2, device="cuda")
+    img = render_b200(e, torch.zeros(0, 3, device="cuda"), torch.zeros(0, 3, device="cuda"),
+                      torch.zeros(0, 2, dtype=torch.long, device="cuda"), 8, 9)
+    assert img.shape == (8, 9, 3) and torch.count_nonzero(img) == 0
+
+
+def test_nonfinite_means_are_dropped():
+    """render_ext.cu:25-34 semantics: NaN / inf / huge centres contribute nothing."""
+    require_cuda()
+    means = cuda(np.array([[5.0, 5.0], [np.nan, 3.0], [1e12, 1e12], [np.inf, 2.0]], np.float32))
+    conics = cuda(np.tile(np.array([[0.44, 0.0, 0.44]], np.float32), (4, 1)))
+    colors = torch.ones(4, 3, device="cuda")
+    radii = torch.full((4, 2), 5, dtype=torch.long, device="cuda")
+    img = render_b200(means, conics, colors, radii, 12, 12)
+    one = render_b200(means[:1], conics[:1], colors[:1], radii[:1], 12, 12)
+    assert torch.isfinite(img).all() and torch.equal(img, one)
+
+
+def test_zero_sized_image():
+    require_cuda()
+    m = torch.tensor([[1.0, 1.0]], device="cuda")
+    img = render_b200(m, torch.ones(1, 3, device="cuda"), torch.ones(1, 3, device="cuda"),
+                      torch.ones(1, 2, dtype=torch.long, device="cuda"), 0, 5)
+    assert img.shape == (0, 5, 3)

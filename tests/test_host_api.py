@@ -1,0 +1,107 @@
+"""Host-side behaviour of the reference-mirroring Python interface (no GPU needed).
+
+Mirrors the reference's requirement / error tests (tests/test_render.py:136-165,
+tests/test_normalization_epsilon.py:32-37): CPU tensors are refused loudly (there is no CPU
+fallback), bad selectors raise ValueError, and the fade / epsilon rules match render.py.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import render_ref
+from structsplat_b200 import render as R
+from structsplat_b200 import render_field, render_gaussians
+from structsplat_b200.structure_tensor import StructureTensorConfig, compute, gaussian_taps
+
+
+def _cpu_field(n=2):
+    means = torch.tensor([[3.0, 3.0], [6.0, 3.0]])[:n]
+    conics = torch.tensor([[0.4, 0.0, 0.4]] * n)
+    colors = torch.tensor([[1.0, 0.0, 0.0]] * n)
+    radii = torch.tensor([[5, 5]] * n, dtype=torch.long)
+    return means, conics, colors, radii
+
+
+@pytest.mark.parametrize("mode", R.NORMALIZED_MODES + R.ADDITIVE_MODES)
+def test_cpu_tensors_are_refused(mode):
+    m, c, col, r = _cpu_field()
+    with pytest.raises(RuntimeError, match="requires CUDA tensors"):
+        render_field(m, c, col, r, 10, 10, mode=mode)
+
+
+def test_rs_path_refuses_cpu():
+    with pytest.raises(RuntimeError, match="requires CUDA tensors"):
+        render_gaussians(torch.zeros(1, 2), torch.zeros(1, 2), torch.zeros(1), torch.zeros(1, 3),
+                         4, 4)
+
+
+def test_unknown_mode_and_gsplat_raise_value_error():
+    m, c, col, r = _cpu_field()
+    for mode in ("nope", "gsplat", "cuda_gsplat"):
+        with pytest.raises(ValueError, match="unknown renderer"):
+            render_field(m, c, col, r, 10, 10, mode=mode)
+
+
+def test_affine_colours_are_not_silently_rendered():
+    m, c, col, r = _cpu_field()
+    with pytest.raises(NotImplementedError):
+        render_field(m, c, col, r, 10, 10, color_grads=torch.zeros(2, 2, 3))
+
+
+@pytest.mark.parametrize("value", [0.0, -1e-12, float("inf"), float("nan")])
+def test_normalization_eps_validation(value):
+    with pytest.raises(ValueError, match="normalization_eps must be finite and > 0"):
+        R.validate_eps(value)
+
+
+def test_fade_alpha_resolution_matches_reference():
+    assert R.resolve_fade_alpha(False) == 0.0
+    assert R.resolve_fade_alpha(True) == 1.0
+    assert R.resolve_fade_alpha(True, 0.25) == 0.25
+    assert R.resolve_fade_alpha(False, 3.0) == 1.0
+    assert R.resolve_fade_alpha(True, -1.0) == 0.0
+
+
+def test_fade_tail_is_the_float32_the_reference_subtracts():
+    """render.py:106 subtracts the Python float alpha*exp(-c^2/2) from a float32 tensor."""
+    q = torch.tensor([0.0, 1.0, 8.9, 9.0, 9.2, 20.0])
+    for alpha in (1.0, 0.5):
+        expect = render_ref.visible_weight(q, 3.0, alpha)
+        tail = np.float32(R.fade_tail(3.0, alpha))
+        got = torch.clamp(torch.exp(-0.5 * q) - torch.tensor(tail), min=0.0)
+        assert torch.equal(got, expect)
+    assert R.fade_tail(3.0, 0.0) == 0.0
+    assert math.isclose(R.fade_tail(3.0, 1.0), math.exp(-4.5), rel_tol=1e-7)
+
+
+def test_tile_size_validation():
+    with pytest.raises(ValueError, match="tile_size"):
+        R.tile_grid(8, 8, 0)
+    with pytest.raises(ValueError, match="tile_size"):
+        R.tile_grid(8, 8, 33)
+    assert R.tile_grid(33, 29, 8) == (4, 5)
+
+
+def test_gaussian_taps_match_reference_kernel():
+    from oracle.structure_tensor_ref import gaussian_taps as ref_taps
+    for sigma in (0.5, 1.0, 2.0, 3.0, 4.7):
+        assert np.array_equal(gaussian_taps(sigma), ref_taps(sigma))
+
+
+def test_structure_tensor_rejects_bad_config_and_cpu():
+    with pytest.raises(ValueError, match="gradient_operator"):
+        compute(np.zeros((8, 8, 3), np.float32), StructureTensorConfig(gradient_operator="x"))
+    with pytest.raises(ValueError, match="color_space"):
+        compute(np.zeros((8, 8, 3), np.float32), StructureTensorConfig(color_space="hsv"))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        compute(torch.zeros(8, 8, 3))
+
+
+def test_shape_validation_happens_before_launch():
+    m, c, col, r = _cpu_field()
+    with pytest.raises(RuntimeError, match="requires CUDA tensors"):
+        R.build_tile_index(m, c, r, 8, 8, 4)
