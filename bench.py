@@ -117,107 +117,105 @@ def flush_l2(buf):
     buf.fill_(1)   # 256 MiB write, twice the L2
 
 
+def timed_loop(fn, steps, flush):
+    """Per-step CUDA-event times of ``fn`` with an L2 flush before each step."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        flush_l2(flush)
+        starts[i].record()
+        fn()
+        ends[i].record()
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in zip(starts, ends)]
+
+
 def run_ours(args, rank, world, dev):
     from structsplat_b200 import _native, render_gaussians
     from structsplat_b200 import render as R
-    from structsplat_b200.field import project
+    from structsplat_b200.fit import CapturedStep, RenderPlan
 
     wl = WORKLOAD
     H, W = wl["H"], wl["W"]
     host = make_inputs(dev)
     names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
-    params = [torch.tensor(host[k], device=dev, requires_grad=True) for k in names]
+    params = {k: torch.tensor(host[k], device=dev) for k in names}
     grad_out = torch.tensor(host["grad_out"], device=dev)
     normalize = wl["mode"] == "normalized"
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
 
-    def step():
-        img = render_gaussians(params[0], params[1], params[2], params[3], H, W,
-                               opacity_logits=params[4], normalize=normalize)
-        return torch.autograd.grad(img, params, grad_out)
+    # ---- the measured step: forward + backward as one captured CUDA graph ----
+    plan = RenderPlan.for_field(params, H, W, normalize=normalize)
+    _native.CALLS.clear()
+    plan.forward_backward(params, grad_out)
+    torch.cuda.synchronize()
+    launches_per_step = launches_from_calls(_native.CALLS)
+    step = CapturedStep(lambda: plan.forward_backward(params, grad_out), warmup=args.warmup)
+    if args.profile:
+        for _ in range(args.steps):
+            step.replay()
+        torch.cuda.synchronize()
+        return None
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clocks:
+        step_ms = timed_loop(step.replay, args.steps, flush)
+    if world > 1:
+        torch.distributed.barrier()
+    total_ms = sum(step_ms)
+    if plan.overflowed():
+        raise RuntimeError("tile index capacity exceeded during the timed steps")
+
+    # ---- the same step through the eager autograd API (render_gaussians + autograd.grad) ----
+    leaves = [params[k].clone().requires_grad_(True) for k in names]
+
+    def eager():
+        img = render_gaussians(leaves[0], leaves[1], leaves[2], leaves[3], H, W,
+                               opacity_logits=leaves[4], normalize=normalize)
+        return torch.autograd.grad(img, leaves, grad_out)
 
     for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    _native.CALLS.clear()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with ClockSampler(dev.index) as clocks:
-        for i in range(args.steps):
-            flush_l2(flush)
-            starts[i].record()
-            step()
-            ends[i].record()
-        torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(step_ms)
-    launches = launches_from_calls(_native.CALLS)
+        eager()
+    eager_ms = timed_loop(eager, args.steps, flush)
 
-    # ---- dominant kernels, timed alone with CUDA events on the launching stream ----
-    with torch.no_grad():
-        n = wl["N"]
-        rec, _, _ = project(*[p.detach() for p in params[:4]], params[4].detach(), H, W)
-        index = R.index_from_records(rec, n, H, W, exact=True)
-        out, den = R._forward(rec, n, index, H, W, normalize, 1e-8, 0.0, dev)
-        kt = {}
-        for name, fn in (
-            ("forward", lambda: R._forward(rec, n, index, H, W, normalize, 1e-8, 0.0, dev)),
-            ("backward", lambda: R._backward(grad_out, rec, n, den, out, index, H, W, normalize,
-                                             1e-8, 0.0, True, False, dev)),
-            ("binning", lambda: R.index_from_records(rec, n, H, W, capacity=index.capacity)),
-        ):
-            for _ in range(3):
-                fn()
-            times = []
-            for _ in range(max(5, args.steps)):
-                flush_l2(flush)
-                s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s.record()
-                fn()
-                e.record()
-                torch.cuda.synchronize()
-                times.append(s.elapsed_time(e))
-            kt[name] = statistics.median(times)
-        entries = index.capacity
+    # ---- dominant kernels alone, CUDA events on the launching stream ----
+    kt = {}
+    for name, fn in (("forward", plan.render), ("backward", lambda: plan.backward(grad_out, params)),
+                     ("binning", lambda: (plan.count(), plan.fill())),
+                     ("project", lambda: plan.project(params))):
+        for _ in range(3):
+            fn()
+        kt[name] = statistics.median(timed_loop(fn, max(5, args.steps), flush))
+    plan.forward(params)
+    torch.cuda.synchronize()
+    entries = int(plan.offsets[-1].item())
 
-    # ---- end to end through the public API with host buffers ----
+    # ---- end to end with host buffers: H2D inputs, the captured step, D2H gradients ----
     pinned = {k: torch.tensor(host[k]).pin_memory() for k in names + ["grad_out"]}
-    host_grads = [torch.empty(p.shape, dtype=torch.float32).pin_memory() for p in params]
+    grads = plan.grads()
+    host_grads = {k: torch.empty(grads[k].shape, dtype=torch.float32).pin_memory() for k in names}
     bi = sum(v.numel() * 4 for v in pinned.values())
-    bo = sum(g.numel() * 4 for g in host_grads)
+    bo = sum(g.numel() * 4 for g in host_grads.values())
 
     def e2e_step():
-        dev_in = [pinned[k].to(dev, non_blocking=True).requires_grad_(True) for k in names]
-        go = pinned["grad_out"].to(dev, non_blocking=True)
-        img = render_gaussians(dev_in[0], dev_in[1], dev_in[2], dev_in[3], H, W,
-                               opacity_logits=dev_in[4], normalize=normalize)
-        grads = torch.autograd.grad(img, dev_in, go)
-        for h, g in zip(host_grads, grads):
-            h.copy_(g, non_blocking=True)
+        for k in names:
+            params[k].copy_(pinned[k], non_blocking=True)
+        grad_out.copy_(pinned["grad_out"], non_blocking=True)
+        step.replay()
+        for k in names:
+            host_grads[k].copy_(grads[k], non_blocking=True)
 
     for _ in range(args.warmup):
         e2e_step()
-    torch.cuda.synchronize()
-    e2e_ms = []
-    for _ in range(args.steps):
-        flush_l2(flush)
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        e2e_step()
-        e.record()
-        e.synchronize()
-        e2e_ms.append(s.elapsed_time(e))
+    e2e_ms = timed_loop(e2e_step, args.steps, flush)
 
     stats = torch.tensor([total_ms, sum(e2e_ms)], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
     return {"total_ms": float(stats[0]), "e2e_total_ms": float(stats[1]), "step_ms": step_ms,
-            "kernels_ms": kt, "entries": entries, "launches": launches, "bi": bi, "bo": bo,
+            "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
+            "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
             "clocks": clocks.summary(), "host": host}
 
 
@@ -329,6 +327,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only replay the captured step (for ncu launch lists)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -367,6 +367,8 @@ def main():
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     res = run_ours(args, rank, world, dev)
+    if res is None:
+        return
     host = res.pop("host")
     peaks = measured_peaks()
     P = pair_count(host) if rank == 0 else 0
@@ -390,7 +392,9 @@ def main():
                                    "opacity logits)", "H": 1024, "W": 1024, "gaussians": 100000,
                        "pairs": P, "tile_entries": res["entries"],
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}",
+                       "step": "one captured CUDA graph: RS projection, tile binning, forward, "
+                               "backward, RS chain rule"},
             "roofline": {"bound": "fp32", "kernel": "backward_kernel",
                          "achieved": round(bwd_ach, 1), "peak": round(peak_slots, 1),
                          "unit": "Gslot/s", "frac": round(bwd_ach / peak_slots, 4),
@@ -400,6 +404,7 @@ def main():
                          "peak_source": "148 SMs x 128 FP32 lanes x sm_max_mhz of "
                                         "MEASURED_PEAKS.json"},
             "kernels_ms": {k: round(v, 4) for k, v in kt.items()},
+            "eager_autograd_ms_per_step": round(res["eager_ms"], 4),
             "forward_roofline_frac": round(fwd_ach / peak_slots, 4),
             "step_roofline_frac": round(t_bound_ms / ms, 4),
             "clocks": clk,

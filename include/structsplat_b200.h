@@ -12,9 +12,9 @@
  * word (SS_STATUS_* bits) that the caller reads whenever it chooses.
  *
  * Reference correspondence (intrinsicD/structsplat, src/structsplat/):
- *   ss_build_tile_index  <- cuda/render_ext.cpp:140-175 build_tile_index / render_ext.cu:858-952
- *   ss_forward_tiled     <- cuda/render_ext.cpp forward_tiled / render_ext.cu:1011-1061
- *   ss_backward_tiled    <- cuda/render_ext.cpp backward_tiled / render_ext.cu:1174-1231
+ *   ss_build_tile_index  <- cuda/render_ext.cpp:139-167 build_tile_index / render_ext.cu:858-952
+ *   ss_forward_tiled     <- cuda/render_ext.cpp:188-211 forward_tiled / render_ext.cu:1011-1063
+ *   ss_backward_tiled    <- cuda/render_ext.cpp:269-301 backward_tiled / render_ext.cu:1169-1231
  *   ss_render_*          <- the same three, split into pack / index / render stages
  *   ss_structure_tensor  <- structure_tensor.py:137-186 (NumPy in the reference)
  *   ss_project_rs*       <- gaussians.py:270-321 (conics, radii, opacity) and their autograd

@@ -47,8 +47,8 @@ __global__ void source_maps_kernel(const float* __restrict__ img, int H, int W, 
   } else if (rgb) {
     for (int c = 0; c < 3; ++c) maps[c * HW + p] = px[c];
   } else {
-    maps[p] = __fadd_rn(__fadd_rn(__fmul_rn(px[0], 0.2126f), __fmul_rn(px[1], 0.7152f)),
-                        __fmul_rn(px[2], 0.0722f));
+    // `img[..., :3] @ luma` evaluates as a fused multiply-add chain in NumPy's float32 dot.
+    maps[p] = __fmaf_rn(px[2], 0.0722f, __fmaf_rn(px[1], 0.7152f, __fmul_rn(px[0], 0.2126f)));
   }
 }
 

@@ -1,0 +1,241 @@
+"""Graph-capturable rendering plans and the CUDA-graph-captured Adam fit.
+
+``RenderPlan`` owns every buffer one forward + backward of an RS field needs (splat records,
+tile offsets, a capacity-bounded tile list, workspaces, image, denominator, gradients), sized
+once, so a step is a fixed sequence of library launches with no allocation and no host
+synchronisation — exactly what a CUDA graph needs.  A step whose tile list would exceed the
+capacity still renders exactly (truncated tiles scan every Gaussian) and raises
+``SS_STATUS_INDEX_OVERFLOW`` in the plan's status word, which the host may read between replays
+to re-plan with a larger capacity.
+
+``fit`` runs the reference's plain fitting iteration (render → pixel MSE → backward → Adam,
+``fit.py:3182-3351`` of the reference) with the whole iteration captured in one CUDA graph.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _native
+from .render import DEFAULT_EPS, RECORD_FLOATS, _p, _stream, fade_tail, tile_grid, validate_eps
+
+PARAM_NAMES = ("means", "log_scales", "rotations", "colors", "opacity_logits")
+
+
+@dataclass
+class RenderPlan:
+    """Preallocated forward + backward of one RS field of ``n`` Gaussians on an H×W image."""
+    n: int
+    H: int
+    W: int
+    normalize: bool = True
+    eps: float = DEFAULT_EPS
+    sigma_cutoff: float = 3.0
+    dilation: float = 0.0
+    fade_alpha: float = 0.0
+    has_opacity: bool = True
+    capacity: int = 0
+    deterministic: bool = False
+    tile_size: int = 16
+    device: torch.device = field(default_factory=lambda: torch.device("cuda"))
+
+    def __post_init__(self):
+        if self.normalize:
+            self.eps = validate_eps(self.eps)
+        tiles_x, tiles_y = tile_grid(self.H, self.W, self.tile_size)
+        self.T = tiles_x * tiles_y
+        self.tail = fade_tail(self.sigma_cutoff, self.fade_alpha)
+        self.cull = self.fade_alpha >= 1.0
+        d, n = self.device, self.n
+        f32 = dict(device=d, dtype=torch.float32)
+        self.records = torch.empty(max(n, 1) * RECORD_FLOATS, **f32)
+        self.offsets = torch.zeros(self.T + 1, device=d, dtype=torch.int32)
+        self.status = torch.zeros(1, device=d, dtype=torch.int32)
+        self.idx_ws_bytes = _native.size_query("ss_tile_index_workspace_bytes", n, self.H, self.W,
+                                               self.tile_size)
+        self.idx_ws = torch.empty(max(self.idx_ws_bytes, 1), device=d, dtype=torch.uint8)
+        if self.capacity <= 0:
+            self.capacity = 1
+        self.gids = torch.empty(self.capacity, device=d, dtype=torch.int32)
+        self.bwd_ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n,
+                                               self.capacity, int(self.deterministic))
+        self.bwd_ws = torch.empty(max(self.bwd_ws_bytes, 16), device=d, dtype=torch.uint8)
+        self.image = torch.zeros(self.H, self.W, 3, **f32)
+        self.den = torch.zeros(self.H, self.W, **f32)
+        self.g_means = torch.zeros(n, 2, **f32)
+        self.g_conics = torch.zeros(n, 3, **f32)
+        self.g_colors = torch.zeros(n, 3, **f32)
+        self.g_opac = torch.zeros(n, **f32)
+        self.g_log_scales = torch.zeros(n, 2, **f32)
+        self.g_rotations = torch.zeros(n, **f32)
+        self.g_logits = torch.zeros(n, **f32)
+
+    @classmethod
+    def for_field(cls, params, H, W, headroom: float = 1.5, **kw):
+        """Plan sized from the field's current tile-list total (one sync, at planning time)."""
+        n = params["means"].shape[0]
+        plan = cls(n=n, H=H, W=W, capacity=1, has_opacity=params.get("opacity_logits") is not None,
+                   device=params["means"].device, **kw)
+        plan.project(params)
+        plan.count()
+        total = int(plan.offsets[-1].item())
+        return cls(n=n, H=H, W=W, capacity=int(total * headroom) + 4096,
+                   has_opacity=plan.has_opacity, device=plan.device, **kw)
+
+    # -- stages --------------------------------------------------------------------------
+    def project(self, params):
+        if self.n:
+            _native.call("ss_project_rs", _p(params["means"]), _p(params["log_scales"]),
+                         _p(params["rotations"]), _p(params["colors"]),
+                         _p(params.get("opacity_logits") if self.has_opacity else None), self.n,
+                         float(self.dilation), float(self.sigma_cutoff), self.H, self.W,
+                         _p(self.records), None, None, _stream())
+
+    def count(self):
+        _native.call("ss_tile_index_count", _p(self.records), self.n, self.H, self.W,
+                     self.tile_size, int(self.cull), float(self.sigma_cutoff), _p(self.offsets),
+                     _p(self.idx_ws), self.idx_ws_bytes, _p(self.status), _stream())
+
+    def fill(self):
+        _native.call("ss_tile_index_fill", _p(self.records), self.n, self.H, self.W,
+                     self.tile_size, int(self.cull), float(self.sigma_cutoff), _p(self.offsets),
+                     _p(self.gids), self.capacity, _p(self.idx_ws), self.idx_ws_bytes,
+                     _p(self.status), _stream())
+
+    def render(self):
+        if self.H * self.W:
+            _native.call("ss_render_forward", _p(self.records), self.n, _p(self.gids),
+                         self.capacity, _p(self.offsets), self.H, self.W, self.tile_size,
+                         int(self.normalize), float(self.eps), float(self.tail), _p(self.image),
+                         _p(self.den), _p(self.status), _stream())
+
+    def backward(self, grad_out, params):
+        if not self.n:
+            return
+        _native.call("ss_render_backward", _p(grad_out), _p(self.records), self.n, _p(self.den),
+                     _p(self.image), _p(self.gids), self.capacity, _p(self.offsets), self.H,
+                     self.W, self.tile_size, int(self.normalize), float(self.eps),
+                     float(self.tail), int(self.has_opacity), _p(self.g_means),
+                     _p(self.g_conics), _p(self.g_colors), _p(self.g_opac),
+                     int(self.deterministic), _p(self.bwd_ws), self.bwd_ws_bytes,
+                     _p(self.status), _stream())
+        _native.call("ss_project_rs_backward", _p(params["log_scales"]), _p(params["rotations"]),
+                     _p(params.get("opacity_logits") if self.has_opacity else None), self.n,
+                     float(self.dilation), _p(self.g_conics),
+                     _p(self.g_opac if self.has_opacity else None), _p(self.g_log_scales),
+                     _p(self.g_rotations), _p(self.g_logits if self.has_opacity else None),
+                     _stream())
+
+    def forward(self, params):
+        self.status.zero_()
+        self.project(params)
+        self.count()
+        self.fill()
+        self.render()
+        return self.image
+
+    def forward_backward(self, params, grad_out):
+        self.forward(params)
+        self.backward(grad_out, params)
+        return self.grads()
+
+    def grads(self):
+        g = {"means": self.g_means, "log_scales": self.g_log_scales,
+             "rotations": self.g_rotations, "colors": self.g_colors}
+        if self.has_opacity:
+            g["opacity_logits"] = self.g_logits
+        return g
+
+    def overflowed(self) -> bool:
+        return bool(int(self.status.item()) & 1)
+
+
+class CapturedStep:
+    """A CUDA graph of ``fn()``; ``fn`` must only launch work on the current stream."""
+
+    def __init__(self, fn, warmup: int = 2):
+        self.fn = fn
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                fn()
+        torch.cuda.current_stream().wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            fn()
+
+    def replay(self):
+        self.graph.replay()
+
+
+def fit(params: dict, target: torch.Tensor, iters: int = 100, lr: float = 1e-2,
+        normalize: bool = True, sigma_cutoff: float = 3.0, log_every: int = 0,
+        graph: bool = True, capacity_headroom: float = 1.5):
+    """Adam fit of an RS field to ``target`` (H,W,3) with the pixel MSE loss.
+
+    ``params`` maps the five field names to CUDA float32 tensors (updated in place).  Returns a
+    history dict with the PSNR at every ``log_every`` iterations (and at the end).  With
+    ``graph=True`` one CUDA graph holds render, loss gradient, backward and the Adam update.
+    """
+    H, W, _ = target.shape
+    names = [k for k in PARAM_NAMES if params.get(k) is not None]
+    plan = RenderPlan.for_field(params, H, W, headroom=capacity_headroom, normalize=normalize,
+                                sigma_cutoff=sigma_cutoff)
+    grads = plan.grads()
+    tensors = [params[k] for k in names]
+    state = [(torch.zeros_like(t), torch.zeros_like(t)) for t in tensors]
+    step_t = torch.zeros(1, device=target.device, dtype=torch.float32)
+    grad_out = torch.empty_like(target)
+    scale = 2.0 / target.numel()
+    b1, b2, eps_adam = 0.9, 0.999, 1e-8
+
+    def iteration():
+        plan.forward(params)
+        torch.sub(plan.image, target, out=grad_out)
+        grad_out.mul_(scale)
+        plan.backward(grad_out, params)
+        step_t.add_(1.0)
+        bc1 = 1.0 - torch.pow(b1, step_t)
+        bc2 = 1.0 - torch.pow(b2, step_t)
+        for t, (m, v), k in zip(tensors, state, names):
+            g = grads[k]
+            m.mul_(b1).add_(g, alpha=1.0 - b1)
+            v.mul_(b2).addcmul_(g, g, value=1.0 - b2)
+            denom = (v / bc2).sqrt_().add_(eps_adam)
+            t.sub_(lr * (m / bc1) / denom)
+
+    history = {"iter": [], "psnr": []}
+
+    def log(it):
+        mse = torch.mean((plan.image - target) ** 2).item()
+        history["iter"].append(it)
+        history["psnr"].append(10.0 * math.log10(1.0 / max(mse, 1e-20)))
+
+    if graph:
+        # warm up (every lazily initialised resource must exist before capture), capture, then
+        # restore the field and the optimizer state the warm-up iterations advanced
+        snapshot = [t.detach().clone() for t in tensors]
+        iteration()
+        cap = CapturedStep(iteration, warmup=1)
+        with torch.no_grad():
+            for t, s in zip(tensors, snapshot):
+                t.copy_(s)
+        step_t.zero_()
+        for (m, v) in state:
+            m.zero_()
+            v.zero_()
+        run = cap.replay
+    else:
+        run = iteration
+    for it in range(1, iters + 1):
+        run()
+        if log_every and it % log_every == 0:
+            log(it)
+    if not history["iter"] or history["iter"][-1] != iters:
+        plan.forward(params)
+        log(iters)
+    history["overflowed"] = plan.overflowed()
+    return history

@@ -3,7 +3,10 @@
 Golden vectors come from the reference's ``render_field`` (tests/golden).  Bars: forward images
 within 1e-5 relative and gradients within 1e-4 relative (norm-wise: max |got − ref| / max |ref|)
 of the reference's float32 results; each case also states its error against the reference
-evaluated in float64.  Cases with the full support fade are ill-conditioned at the cutoff
+evaluated in float64.  Where the reference's own float32 gradient is itself far from float64
+(a gradient made of cancelling terms, e.g. a lone or single-colour splat whose
+dw = dnum·c + dden is rounding noise), matching it is meaningless; there the bar is to be no
+less accurate than it: error vs float64 ≤ max(1e-4, 2 × the reference's own float32 error).  Cases with the full support fade are ill-conditioned at the cutoff
 (exp(−q/2) − exp(−c²/2) cancels): for those the forward is compared element-wise with a floor
 and the float64 yardstick shows the reference float32 path has the same conditioning.
 """
@@ -47,6 +50,15 @@ def _render(z, deterministic=False, want_grads=True):
     return img.detach(), grads
 
 
+def _grad_ok(got, z, key, prefix="g"):
+    e32 = rel_err(got, z[f"{prefix}_{key}_f32"])
+    e64 = rel_err(got, z[f"{prefix}_{key}_f64"])
+    ref_err = rel_err(z[f"{prefix}_{key}_f32"], z[f"{prefix}_{key}_f64"])
+    if ref_err <= GRAD_TOL / 10:
+        return e32 <= GRAD_TOL, (e32, e64, ref_err)
+    return e64 <= max(GRAD_TOL, 2 * ref_err), (e32, e64, ref_err)
+
+
 def _fwd_error_ok(img, z):
     """Forward bar; faded cases use an element-wise bar floored at 1e-3 of the image scale."""
     e32 = rel_err(img, z["image_f32"])
@@ -74,10 +86,10 @@ def test_gradients_match_reference(name, deterministic):
     _, grads = _render(z, deterministic=deterministic)
     keys = ["means", "conics", "colors"] + (["opacities"] if "opacities" in z.files else [])
     for key, g in zip(keys, grads):
-        e32 = rel_err(g, z[f"g_{key}_f32"])
-        e64 = rel_err(g, z[f"g_{key}_f64"])
-        print(f"{name} {key}: grad err vs ref f32 {e32:.2e}, vs f64 {e64:.2e}")
-        assert e32 <= GRAD_TOL, (key, e32, e64)
+        ok, (e32, e64, ref_err) = _grad_ok(g, z, key)
+        print(f"{name} {key}: grad err vs ref f32 {e32:.2e}, vs f64 {e64:.2e} "
+              f"(ref f32 vs f64 {ref_err:.2e})")
+        assert ok, (key, e32, e64, ref_err)
 
 
 @pytest.mark.parametrize("name", RENDER_CASES)
@@ -101,10 +113,10 @@ def test_rs_field_path_matches_reference(name):
     keys = ["means", "log_scales", "rotations", "colors"] + (
         ["opacity_logits"] if logits is not None else [])
     for key, g in zip(keys, grads):
-        e32 = rel_err(g, z[f"rs_{key}_f32"])
-        print(f"{name} rs {key}: grad err vs ref f32 {e32:.2e}, "
-              f"vs f64 {rel_err(g, z[f'rs_{key}_f64']):.2e}")
-        assert e32 <= GRAD_TOL, (key, e32)
+        ok, (e32, e64, ref_err) = _grad_ok(g, z, key, prefix="rs")
+        print(f"{name} rs {key}: grad err vs ref f32 {e32:.2e}, vs f64 {e64:.2e} "
+              f"(ref f32 vs f64 {ref_err:.2e})")
+        assert ok, (key, e32, e64, ref_err)
 
 
 def test_rs_projection_matches_reference_conics_and_radii():
@@ -146,7 +158,7 @@ def test_truncated_index_renders_identically():
     m, c, col, r, op = _case(z)
     H, W = int(z["H"]), int(z["W"])
     rec = R.pack_records(m, c, col, r, op, H, W)
-    full = R.index_from_records(rec, m.shape[0], H, W)
+    full = R.index_from_records(rec, m.shape[0], H, W, exact=True)
     part = R.index_from_records(rec, m.shape[0], H, W, capacity=full.capacity // 3)
     out_f, den_f = R._forward(rec, m.shape[0], full, H, W, True, 1e-8, 0.0, m.device)
     out_p, den_p = R._forward(rec, m.shape[0], part, H, W, True, 1e-8, 0.0, m.device)
