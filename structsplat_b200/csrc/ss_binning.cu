@@ -101,8 +101,9 @@ __device__ __forceinline__ Splat load_splat(const Splat* rec, int64_t i) {
 }
 
 // Calls visit(gaussian, tile) for every (tile, Gaussian) pair of the index, in any order.
-// Each lane enumerates small rectangles itself; a rectangle of more than kSmallRect tiles is
-// enumerated by the whole warp so one huge Gaussian cannot serialise a lane.
+// Each lane enumerates a rectangle of up to kSmallRect tiles itself (unrolled, so independent
+// atomics are in flight together); a larger rectangle is enumerated by the whole warp so one
+// huge Gaussian cannot serialise a lane.  Tile coordinates advance incrementally (no division).
 template <bool CULL, typename Visit>
 __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int ts, int tiles_x,
                                                 float cutoff2, Visit visit) {
@@ -114,10 +115,16 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
   if (cnt > 0 && cnt <= kSmallRect) {
     Splat s;
     if (CULL) s = load_splat(rec, i);
-    for (int k = 0; k < cnt; ++k) {
-      int gx = r.gx0 + k % r.gw, gy = r.gy0 + k / r.gw;
-      if (CULL && culled(s, gx, gy, ts, cutoff2)) continue;
-      visit((int)i, gy * tiles_x + gx);
+    int gx = r.gx0, gy = r.gy0;
+#pragma unroll
+    for (int k = 0; k < kSmallRect; ++k) {
+      if (k < cnt) {
+        if (!(CULL && culled(s, gx, gy, ts, cutoff2))) visit(k, (int)i, gy * tiles_x + gx);
+        if (++gx == r.gx0 + r.gw) {
+          gx = r.gx0;
+          ++gy;
+        }
+      }
     }
   }
   unsigned big = __ballot_sync(0xffffffffu, cnt > kSmallRect);
@@ -131,10 +138,16 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
     long long gi = __shfl_sync(0xffffffffu, (long long)i, src);
     Splat s;
     if (CULL) s = load_splat(rec, gi);
+    const int step_y = 32 / gw, step_x = 32 - step_y * gw;
+    int gy = gy0 + lane / gw, gx = gx0 + lane % gw;
     for (int k = lane; k < total; k += 32) {
-      int gx = gx0 + k % gw, gy = gy0 + k / gw;
-      if (CULL && culled(s, gx, gy, ts, cutoff2)) continue;
-      visit((int)gi, gy * tiles_x + gx);
+      if (!(CULL && culled(s, gx, gy, ts, cutoff2))) visit(-1, (int)gi, gy * tiles_x + gx);
+      gx += step_x;
+      gy += step_y;
+      if (gx >= gx0 + gw) {
+        gx -= gw;
+        ++gy;
+      }
     }
   }
 }
@@ -143,11 +156,12 @@ template <bool CULL>
 __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
                                   float cutoff2, int* __restrict__ tile_count) {
   enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2,
-                        [&](int, int t) { atomicAdd(tile_count + t, 1); });
+                        [&](int, int, int t) { atomicAdd(tile_count + t, 1); });
 }
 
 // Writes int32 offsets, checks capacity, then claims one slot per pair.  Slots are claimed by
-// counting each tile's counter back down, which leaves the counters at zero.
+// counting each tile's counter back down, which leaves the counters at zero.  A lane's own
+// (small) rectangle claims all its slots first and stores afterwards, so the atomics overlap.
 template <bool CULL>
 __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
                                  float cutoff2, int64_t T, const long long* __restrict__ off64,
@@ -163,10 +177,24 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
     if (total > 2147483647LL) raise_status(status, SS_STATUS_INDEX_INT32);
     if (total > cap) raise_status(status, SS_STATUS_INDEX_OVERFLOW);
   }
-  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2, [&](int g, int t) {
-    long long pos = off64[t] + (atomicSub(tile_count + t, 1) - 1);
-    if (pos < cap) gids[pos] = g;
+  long long pos[kSmallRect];
+#pragma unroll
+  for (int k = 0; k < kSmallRect; ++k) pos[k] = -1;
+  int owner = -1;
+  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2, [&](int k, int g, int t) {
+    long long p = off64[t] + (atomicSub(tile_count + t, 1) - 1);
+    if (k < 0) {
+      if (p < cap) gids[p] = g;
+    } else {
+#pragma unroll
+      for (int q = 0; q < kSmallRect; ++q)
+        if (q == k) pos[q] = p;
+      owner = g;
+    }
   });
+#pragma unroll
+  for (int k = 0; k < kSmallRect; ++k)
+    if (pos[k] >= 0 && pos[k] < cap) gids[pos[k]] = owner;
 }
 
 // Ascending sort of buf[0..len) using a bitonic network over the next power of two in which
@@ -175,10 +203,12 @@ template <typename Sync>
 __device__ void bitonic_sort(int* buf, int len, int tid, int nthreads, Sync sync) {
   int n2 = 1;
   while (n2 < len) n2 <<= 1;
-  for (int k = 2; k <= n2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
+  for (int lk = 1; (1 << lk) <= n2; ++lk) {
+    const int k = 1 << lk;
+    for (int lj = lk - 1; lj >= 0; --lj) {
+      const int j = 1 << lj;
       for (int p = tid; p < (n2 >> 1); p += nthreads) {
-        int blk = p / j, r = p - blk * j, a, b;
+        int blk = p >> lj, r = p & (j - 1), a, b;
         if (j == (k >> 1)) {
           a = blk * k + r;
           b = blk * k + k - 1 - r;

@@ -81,8 +81,37 @@ __device__ __forceinline__ void stage_chunk(float4 (*dst)[4], const Splat* rec, 
   }
 }
 
+constexpr int kFwdThreads = 128;   // 4 warps, each an 8x8 pixel sub-block, 2 pixels per lane
+
+// Issues the copies of entries [k0, k0+m) with kFwdThreads threads (two 16-byte pieces each).
+__device__ __forceinline__ void stage_chunk128(float4 (*dst)[4], const Splat* rec,
+                                               const TileList& L, int64_t k0, int m) {
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int q = threadIdx.x + r * kFwdThreads;
+    const int slot = q >> 2, piece = q & 3;
+    if (slot < m) {
+      const int g = L.gid(k0 + slot);
+      cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
+    }
+  }
+}
+
+// Mask of the staged entries [32 r, 32 r + 32) whose support rectangle touches the 8x8 block
+// at (sx0, sy0): lane l tests entry 32 r + l, a ballot collects the answers.
+__device__ __forceinline__ unsigned hit_mask(const float4 (*st)[4], int m, int sx0, int sy0,
+                                             int lane, int r) {
+  const int j = lane + 32 * r;
+  bool hit = false;
+  if (j < m) {
+    const int4 b = *reinterpret_cast<const int4*>(&st[j][3]);
+    hit = b.x < sx0 + 8 && b.z > sx0 && b.y < sy0 + 8 && b.w > sy0;
+  }
+  return __ballot_sync(0xffffffffu, hit);
+}
+
 template <bool NORMALIZE, bool FADE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kFwdThreads)
     forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
                    int64_t cap, const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
                    float eps, float tail, float* __restrict__ out, float* __restrict__ den) {
@@ -90,62 +119,76 @@ __global__ void __launch_bounds__(kThreads)
   const int tile = blockIdx.x;
   const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int sx0 = tx0 + (warp & 1) * 8, sy0 = ty0 + (warp >> 1) * 4;
-  const int px = sx0 + (lane & 7), py = sy0 + (lane >> 3);
-  const float fx = (float)px, fy = (float)py;
+  const int sx0 = tx0 + (warp & 1) * 8, sy0 = ty0 + (warp >> 1) * 8;
+  const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3), py1 = py0 + 4;
+  const float fx = (float)px, fy0 = (float)py0;
   const TileList L = tile_list(gids, offsets, cap, n, tile);
   const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
 
-  float nr = 0.f, ng = 0.f, nb = 0.f, d = 0.f;
-  if (nchunks > 0) stage_chunk(stage[0], rec, L, 0, chunk_len(L.count, 0));
+  float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
+  if (nchunks > 0) stage_chunk128(stage[0], rec, L, 0, chunk_len(L.count, 0));
   cp_async_commit();
   for (int c = 0; c < nchunks; ++c) {
-    int64_t k0 = (int64_t)c * kChunk;
+    const int64_t k0 = (int64_t)c * kChunk;
     if (c + 1 < nchunks)
-      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk,
-                  chunk_len(L.count, k0 + kChunk));
+      stage_chunk128(stage[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
     cp_async_commit();
     cp_async_wait_one();
     __syncthreads();
     const int m = chunk_len(L.count, k0);
     const float4(*st)[4] = stage[c & 1];
-    for (int j = 0; j < m; ++j) {
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+    unsigned hits = hit_mask(st, m, sx0, sy0, lane, half);
+    while (hits) {
+      const int j = 32 * half + __ffs(hits) - 1;
+      hits &= hits - 1;
       const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
-      if (r.x >= sx0 + 8 || r.z <= sx0 || r.y >= sy0 + 4 || r.w <= sy0) continue;
       const float4 p0 = st[j][0], p1 = st[j][1];
       const float cb = st[j][2].x;
-      const bool in = px >= r.x && px < r.z && py >= r.y && py < r.w;
-      const float dx = fx - p0.x, dy = fy - p0.y;
-      const float e = fmaf(dx, fmaf(p0.z, dx, p0.w * dy), p1.x * dy * dy);
-      const float raw = fast_exp2(e);
-      const float vis = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-      const float w = in ? vis * p1.y : 0.0f;
-      nr = fmaf(w, p1.z, nr);
-      ng = fmaf(w, p1.w, ng);
-      nb = fmaf(w, cb, nb);
-      d += w;
+      const bool inx = px >= r.x && px < r.z;
+      const bool in0 = inx && py0 >= r.y && py0 < r.w;
+      const bool in1 = inx && py1 >= r.y && py1 < r.w;
+      const float dx = fx - p0.x, dy0 = fy0 - p0.y, dy1 = dy0 + 4.0f;
+      const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+      const float raw0 = fast_exp2(fmaf(dy0, fmaf(p1.x, dy0, bdx), adx2));
+      const float raw1 = fast_exp2(fmaf(dy1, fmaf(p1.x, dy1, bdx), adx2));
+      const float vis0 = FADE ? fmaxf(raw0 - tail, 0.0f) : raw0;
+      const float vis1 = FADE ? fmaxf(raw1 - tail, 0.0f) : raw1;
+      const float w0 = in0 ? vis0 * p1.y : 0.0f;
+      const float w1 = in1 ? vis1 * p1.y : 0.0f;
+      acc0[0] = fmaf(w0, p1.z, acc0[0]);
+      acc0[1] = fmaf(w0, p1.w, acc0[1]);
+      acc0[2] = fmaf(w0, cb, acc0[2]);
+      acc0[3] += w0;
+      acc1[0] = fmaf(w1, p1.z, acc1[0]);
+      acc1[1] = fmaf(w1, p1.w, acc1[1]);
+      acc1[2] = fmaf(w1, cb, acc1[2]);
+      acc1[3] += w1;
+    }
     }
     __syncthreads();
   }
-  if (px < W && py < H) {
-    const int64_t p = (int64_t)py * W + px;
-    den[p] = d;
-    if (NORMALIZE) {
-      const float denom = d + eps;
-      out[3 * p] = nr / denom;
-      out[3 * p + 1] = ng / denom;
-      out[3 * p + 2] = nb / denom;
-    } else {
-      out[3 * p] = nr;
-      out[3 * p + 1] = ng;
-      out[3 * p + 2] = nb;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int py = k ? py1 : py0;
+    const float* a = k ? acc1 : acc0;
+    if (px < W && py < H) {
+      const int64_t p = (int64_t)py * W + px;
+      den[p] = a[3];
+      if (NORMALIZE) {
+        const float denom = a[3] + eps;
+        out[3 * p] = a[0] / denom;
+        out[3 * p + 1] = a[1] / denom;
+        out[3 * p + 2] = a[2] / denom;
+      } else {
+        out[3 * p] = a[0];
+        out[3 * p + 1] = a[1];
+        out[3 * p + 2] = a[2];
+      }
     }
   }
 }
-
-// 16-bit reciprocal multipliers: (idx * kRowMul[w]) >> 16 == idx / w for idx < 256, w <= 16.
-__constant__ int kRowMul[17] = {0,    65536, 32768, 21846, 16384, 13108, 10923, 9363, 8192,
-                                7282, 6554,  5958,  5462,  5042,  4682,  4370,  4096};
 
 template <bool FADE, bool DETERMINISTIC>
 __global__ void __launch_bounds__(kThreads)
@@ -214,29 +257,37 @@ __global__ void __launch_bounds__(kThreads)
         const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
         const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
         const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
-        const int w = cx1 - cx0, h = cy1 - cy0;
-        const int npx = (w > 0 && h > 0) ? w * h : 0;
-        const int mul = npx ? kRowMul[w] : 0;
-        for (int idx = hl; idx < npx; idx += 16) {
-          const int row = (idx * mul) >> 16, col = idx - row * w;
-          const float4 g = pix[(cy0 + row) * TS + cx0 + col];
-          const float dx = (float)(tx0 + cx0 + col) - p0.x;
-          const float dy = (float)(ty0 + cy0 + row) - p0.y;
-          const float e = fmaf(dx, fmaf(p0.z, dx, p0.w * dy), p1.x * dy * dy);
-          const float raw = fast_exp2(e);
-          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
-          acc[0] = fmaf(base_w, g.x, acc[0]);
-          acc[1] = fmaf(base_w, g.y, acc[1]);
-          acc[2] = fmaf(base_w, g.z, acc[2]);
-          acc[3] = fmaf(base_w, dw, acc[3]);
-          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
-          const float u = t * dx, v = t * dy;
-          acc[4] += u;
-          acc[5] += v;
-          acc[6] = fmaf(u, dx, acc[6]);
-          acc[7] = fmaf(u, dy, acc[7]);
-          acc[8] = fmaf(v, dy, acc[8]);
+        // Column strips: lane (hl & 7) takes every 8th column of the rectangle inside the
+        // tile, lane half (hl >> 3) the upper or lower half of its rows.  Along a column dx is
+        // constant, so Σt·dx, Σt·dx², Σt·dx·dy fold into per-column products.
+        const int half_rows = (cy1 - cy0 + 1) >> 1;
+        const int ry0 = cy0 + (hl >> 3) * half_rows;
+        const int ry1 = min(ry0 + half_rows, cy1);
+        const float dy0 = (float)(ty0 + ry0) - p0.y;
+        for (int cx = cx0 + (hl & 7); cx < cx1; cx += 8) {
+          const float dx = (float)(tx0 + cx) - p0.x;
+          const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+          float tc = 0.f, uc = 0.f, dy = dy0;
+          const float4* gp = pix + ry0 * TS + cx;
+          for (int ry = ry0; ry < ry1; ++ry, dy += 1.0f, gp += TS) {
+            const float4 g = *gp;
+            const float raw = fast_exp2(fmaf(dy, fmaf(p1.x, dy, bdx), adx2));
+            const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+            const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
+            acc[0] = fmaf(base_w, g.x, acc[0]);
+            acc[1] = fmaf(base_w, g.y, acc[1]);
+            acc[2] = fmaf(base_w, g.z, acc[2]);
+            acc[3] = fmaf(base_w, dw, acc[3]);
+            const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+            const float u = t * dy;
+            tc += t;
+            uc += u;
+            acc[8] = fmaf(u, dy, acc[8]);
+          }
+          acc[4] = fmaf(dx, tc, acc[4]);
+          acc[5] += uc;
+          acc[6] = fmaf(dx * dx, tc, acc[6]);
+          acc[7] = fmaf(dx, uc, acc[7]);
         }
       }
 #pragma unroll
@@ -358,7 +409,7 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
   const Splat* rec = static_cast<const Splat*>(records);
   const bool fade = fade_tail > 0.0f;
 #define SS_FWD(NORM, FADE)                                                                    \
-  forward_kernel<NORM, FADE><<<(unsigned)T, kThreads, 0, s>>>(rec, n, tile_gids, gid_capacity, \
+  forward_kernel<NORM, FADE><<<(unsigned)T, kFwdThreads, 0, s>>>(rec, n, tile_gids, gid_capacity, \
                                                               tile_offsets, height, width,    \
                                                               tiles_x, eps, fade_tail, out, den)
   if (normalize) {

@@ -88,13 +88,3 @@ def test_empty_problem_needs_no_device(lib):
     rc, _ = _status(lib, "ss_render_forward", None, 0, None, 0, None, 0, 7, 16, 1,
                     ctypes.c_float(1e-8), ctypes.c_float(0.0), None, None, None, None)
     assert rc == 0
-
-
-def test_row_multipliers_divide_exactly():
-    """The backward kernel's (idx * mul[w]) >> 16 replaces idx / w for idx < 256, w <= 16."""
-    src = (REPO / "structsplat_b200" / "csrc" / "ss_render.cu").read_text()
-    table = re.search(r"kRowMul\[17\] = \{([^}]*)\}", src).group(1)
-    mul = [int(v) for v in table.replace("\n", " ").split(",")]
-    for w in range(1, 17):
-        for idx in range(16 * w):
-            assert (idx * mul[w]) >> 16 == idx // w, (w, idx)

@@ -1,7 +1,6 @@
 """Graph-captured plan and fit: same results as the eager autograd path."""
 from __future__ import annotations
 
-import numpy as np
 import pytest
 import torch
 
@@ -86,4 +85,3 @@ def test_graph_fit_matches_eager_fit_and_improves_psnr():
     assert h_graph["psnr"][-1] > h_graph["psnr"][0]
     assert abs(h_graph["psnr"][-1] - h_eager["psnr"][-1]) <= 0.01
     assert not h_graph["overflowed"]
-    del np
