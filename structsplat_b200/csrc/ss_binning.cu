@@ -6,7 +6,11 @@
 // every downstream sum deterministic.  No sort over all pairs is needed: per-tile counts come
 // from atomics, a device-wide scan gives the offsets, the fill claims slots with per-tile atomic
 // cursors, and a per-tile bitonic sort in shared memory restores ascending ids.
+#include <climits>
+
 #include <cub/device/device_scan.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include "ss_common.cuh"
 
@@ -17,6 +21,20 @@ constexpr int kThreads = 256;
 constexpr int kSmallRect = 8;          // tiles a lane enumerates alone; larger rects use the warp
 constexpr int kWarpSortMax = 1024;     // per-warp shared-memory sort capacity (ints)
 constexpr int kBigSortSmem = 16384;    // per-CTA shared-memory sort capacity (ints)
+// Per-tile counters sit one per 32-byte sector: a tile receives one atomic per Gaussian that
+// touches it, and packing 8 neighbouring tiles' counters into a sector would serialise their
+// atomics in the L2.
+constexpr int kCounterStride = 8;
+
+struct CounterLoad {
+  const int* base;
+  __host__ __device__ int operator()(int64_t t) const { return base[t * kCounterStride]; }
+};
+
+inline auto counter_iter(const int* base) {
+  return thrust::make_transform_iterator(thrust::make_counting_iterator<int64_t>(0),
+                                         CounterLoad{base});
+}
 
 struct TileGrid {
   int ts, tiles_x, tiles_y;
@@ -46,13 +64,14 @@ inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 size_t scan_temp_bytes(int64_t items) {
   size_t bytes = 0;
-  cub::DeviceScan::ExclusiveScan(nullptr, bytes, (const int*)nullptr, (long long*)nullptr,
+  cub::DeviceScan::ExclusiveScan(nullptr, bytes, counter_iter(nullptr), (long long*)nullptr,
                                  ::cuda::std::plus<long long>(), (long long)0, (int)items);
   return bytes;
 }
 
 size_t index_workspace_bytes(int64_t T) {
-  return align256(sizeof(int) * (T + 1)) + align256(sizeof(long long) * (T + 1)) +
+  return align256(sizeof(int) * kCounterStride * (T + 1)) +
+         align256(sizeof(long long) * (T + 1)) +
          align256(sizeof(int) * (T > 0 ? T : 1)) + align256(sizeof(int)) +
          align256(scan_temp_bytes(T + 1));
 }
@@ -61,7 +80,7 @@ IndexWorkspace carve(void* base, int64_t T) {
   IndexWorkspace w;
   char* p = static_cast<char*>(base);
   w.tile_count = reinterpret_cast<int*>(p);
-  p += align256(sizeof(int) * (T + 1));
+  p += align256(sizeof(int) * kCounterStride * (T + 1));
   w.offsets64 = reinterpret_cast<long long*>(p);
   p += align256(sizeof(long long) * (T + 1));
   w.big_tiles = reinterpret_cast<int*>(p);
@@ -156,7 +175,7 @@ template <bool CULL>
 __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
                                   float cutoff2, int* __restrict__ tile_count) {
   enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2,
-                        [&](int, int, int t) { atomicAdd(tile_count + t, 1); });
+                        [&](int, int, int t) { atomicAdd(tile_count + (int64_t)t * kCounterStride, 1); });
 }
 
 // Writes int32 offsets, checks capacity, then claims one slot per pair.  Slots are claimed by
@@ -182,7 +201,7 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
   for (int k = 0; k < kSmallRect; ++k) pos[k] = -1;
   int owner = -1;
   enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2, [&](int k, int g, int t) {
-    long long p = off64[t] + (atomicSub(tile_count + t, 1) - 1);
+    long long p = off64[t] + (atomicSub(tile_count + (int64_t)t * kCounterStride, 1) - 1);
     if (k < 0) {
       if (p < cap) gids[p] = g;
     } else {
@@ -229,7 +248,53 @@ __device__ void bitonic_sort(int* buf, int len, int tid, int nthreads, Sync sync
   }
 }
 
-// One warp per tile; lists longer than kWarpSortMax are queued for tile_sort_big_kernel.
+// Ascending sort of up to 32*K keys held in registers across a warp: key k of lane l is element
+// 32k + l, missing elements are INT_MAX.  Standard bitonic network: at block size `size` and
+// distance j, elements e and e^j are compared and the block (e & size) == 0 sorts upward.
+// Distances below 32 exchange through xor shuffles, larger ones swap registers in-lane.
+template <int K>
+__device__ __forceinline__ void warp_bitonic(int (&v)[K], int lane) {
+#pragma unroll
+  for (int size = 2; size <= 32 * K; size <<= 1) {
+#pragma unroll
+    for (int j = size >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int kp = k ^ (j >> 5);
+          if (kp > k) {
+            const bool up = ((32 * k + lane) & size) == 0;
+            const int lo = min(v[k], v[kp]), hi = max(v[k], v[kp]);
+            v[k] = up ? lo : hi;
+            v[kp] = up ? hi : lo;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          const int other = __shfl_xor_sync(0xffffffffu, v[k], j);
+          const bool up = ((32 * k + lane) & size) == 0;
+          const bool lower = (lane & j) == 0;
+          v[k] = (up == lower) ? min(v[k], other) : max(v[k], other);
+        }
+      }
+    }
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void warp_sort_list(int32_t* __restrict__ g, int len, int lane) {
+  int v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 32 * k + lane < len ? g[32 * k + lane] : INT_MAX;
+  warp_bitonic<K>(v, lane);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (32 * k + lane < len) g[32 * k + lane] = v[k];
+}
+
+// One warp per tile: lists up to 256 ids sort in registers, up to kWarpSortMax in shared
+// memory; longer lists are queued for tile_sort_big_kernel.
 __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __restrict__ offsets,
                                                              int32_t* __restrict__ gids,
                                                              int64_t cap, int64_t T,
@@ -242,15 +307,24 @@ __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __re
   if (hi > cap) return;  // truncated list: the renderers scan all Gaussians for this tile
   int len = (int)(hi - lo);
   if (len <= 1) return;
-  if (len > kWarpSortMax) {
-    if (lane == 0) big_tiles[atomicAdd(big_count, 1)] = (int)t;
-    return;
+  int32_t* g = gids + lo;
+  if (len <= 32) {
+    warp_sort_list<1>(g, len, lane);
+  } else if (len <= 64) {
+    warp_sort_list<2>(g, len, lane);
+  } else if (len <= 128) {
+    warp_sort_list<4>(g, len, lane);
+  } else if (len <= 256) {
+    warp_sort_list<8>(g, len, lane);
+  } else if (len <= kWarpSortMax) {
+    int* b = buf[warp];
+    for (int k = lane; k < len; k += 32) b[k] = g[k];
+    __syncwarp();
+    bitonic_sort(b, len, lane, 32, [] { __syncwarp(); });
+    for (int k = lane; k < len; k += 32) g[k] = b[k];
+  } else if (lane == 0) {
+    big_tiles[atomicAdd(big_count, 1)] = (int)t;
   }
-  int* b = buf[warp];
-  for (int k = lane; k < len; k += 32) b[k] = gids[lo + k];
-  __syncwarp();
-  bitonic_sort(b, len, lane, 32, [] { __syncwarp(); });
-  for (int k = lane; k < len; k += 32) gids[lo + k] = b[k];
 }
 
 // Long lists: one CTA per list, in shared memory up to kBigSortSmem ids, else in place.
@@ -333,7 +407,8 @@ int ss_tile_index_count(const void* records, int64_t n, int height, int width, i
                 workspace_bytes, index_workspace_bytes(g.T));
   cudaStream_t s = as_stream(stream);
   IndexWorkspace w = carve(workspace, g.T);
-  if (cudaMemsetAsync(w.tile_count, 0, sizeof(int) * (g.T + 1), s) != cudaSuccess)
+  if (cudaMemsetAsync(w.tile_count, 0, sizeof(int) * kCounterStride * (g.T + 1), s) !=
+      cudaSuccess)
     return check_launch("tile_index_count memset");
   const Splat* rec = static_cast<const Splat*>(records);
   float cutoff2 = sigma_cutoff * sigma_cutoff;
@@ -348,7 +423,8 @@ int ss_tile_index_count(const void* records, int64_t n, int height, int width, i
     if ((rc = check_launch("tile_count"))) return rc;
   }
   size_t sb = w.scan_bytes;
-  cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, w.tile_count, w.offsets64,
+  cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, counter_iter(w.tile_count),
+                                                 w.offsets64,
                                                  ::cuda::std::plus<long long>(), (long long)0,
                                                  (int)(g.T + 1), s);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, "tile offsets scan: %s", cudaGetErrorString(e));

@@ -10,18 +10,26 @@ namespace {
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-// Workspace: [records n*64 B][tile-index workspace]
+// Workspace: [records n*64 B][tile-index workspace][backward moments]
 struct RefWorkspace {
   void* records;
   void* index_ws;
   size_t index_bytes;
+  void* backward_ws;
+  size_t backward_bytes;
 };
+
+size_t backward_bytes(int64_t n) {
+  size_t b = 0;
+  ss_render_backward_workspace_bytes(n, 0, 0, &b);
+  return b;
+}
 
 int carve_ref(void* ws, size_t ws_bytes, int64_t n, int H, int W, int ts, RefWorkspace* out) {
   size_t idx = 0;
   int rc = ss_tile_index_workspace_bytes(n, H, W, ts, &idx);
   if (rc) return rc;
-  size_t need = align256((size_t)n * sizeof(Splat)) + idx;
+  size_t need = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n);
   if (!ws || ws_bytes < need)
     return fail(SS_ERR_INVALID_ARGUMENT, "workspace too small (%zu < %zu)", ws_bytes, need);
   if (reinterpret_cast<uintptr_t>(ws) % 256)
@@ -29,6 +37,8 @@ int carve_ref(void* ws, size_t ws_bytes, int64_t n, int H, int W, int ts, RefWor
   out->records = ws;
   out->index_ws = static_cast<char*>(ws) + align256((size_t)n * sizeof(Splat));
   out->index_bytes = idx;
+  out->backward_ws = static_cast<char*>(out->index_ws) + align256(idx);
+  out->backward_bytes = backward_bytes(n);
   return SS_OK;
 }
 
@@ -51,7 +61,7 @@ int ss_reference_workspace_bytes(int64_t n, int height, int width, int tile_size
   int rc = ss_tile_index_workspace_bytes(n, height, width, tile_size, &idx);
   if (rc) return rc;
   (void)gid_capacity;
-  *bytes = align256((size_t)n * sizeof(Splat)) + idx;
+  *bytes = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n);
   return SS_OK;
 }
 
@@ -111,8 +121,8 @@ int ss_backward_tiled(const float* grad_out, const float* means, const float* co
   return ss_render_backward(grad_out, w.records, n, den, out, tile_gids, gid_capacity,
                             tile_offsets, height, width, tile_size, normalize, eps,
                             tail_of(support_fade, sigma_cutoff), opacities != nullptr,
-                            grad_means, grad_conics, grad_colors, grad_opacities, 0, nullptr, 0,
-                            status, stream);
+                            grad_means, grad_conics, grad_colors, grad_opacities, 0,
+                            w.backward_ws, w.backward_bytes, status, stream);
 }
 
 }  // extern "C"

@@ -190,18 +190,56 @@ __global__ void __launch_bounds__(kFwdThreads)
   }
 }
 
+// One level of a reduce-scatter butterfly: lanes whose `bit` is clear keep slots [0, K) of v,
+// the others keep slots [K, N) (as their new slots 0..); each side receives the partner's copy
+// of the slots it keeps and adds it.  Missing slots count as zero.
+template <int N, int K>
+__device__ __forceinline__ void scatter_level(const float (&v)[N], float (&w)[K], bool bit,
+                                              int lane_mask) {
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const float hi_v = (K + i < N) ? v[K + i] : 0.0f;
+    const float send = bit ? v[i] : hi_v;
+    const float keep = bit ? hi_v : v[i];
+    w[i] = keep + __shfl_xor_sync(0xffffffffu, send, lane_mask);
+  }
+}
+
+// Reduce-scatter of the nine moments over the 32 lanes of a warp: after the xor butterflies
+// 16, 8, 4, 2, 1 lane l holds the warp total of moment moment_of_lane(l) (or nothing, -1).
+__device__ __forceinline__ float reduce_scatter9(const float (&v)[kMoments], int lane) {
+  float a[5], b[3], c[2], d[1];
+  scatter_level<9, 5>(v, a, lane & 16, 16);   // 0-4 | 5-8
+  scatter_level<5, 3>(a, b, lane & 8, 8);     // 0-2 | 3-4
+  scatter_level<3, 2>(b, c, lane & 4, 4);     // 0-1 | 2
+  scatter_level<2, 1>(c, d, lane & 2, 2);     // 0   | 1
+  return d[0] + __shfl_xor_sync(0xffffffffu, d[0], 1);
+}
+
+// Which moment lane l holds after reduce_scatter9 (-1: none); lanes l and l^1 hold the same.
+__device__ __forceinline__ int moment_of_lane(int lane) {
+  const int b16 = (lane >> 4) & 1, b8 = (lane >> 3) & 1, b4 = (lane >> 2) & 1,
+            b2 = (lane >> 1) & 1;
+  // level 1 picks group {0..4} / {5..8}; level 2 slots {0,1,2} / {3,4}; level 3 {0,1} / {2};
+  // level 4 {0} / {1}.
+  int slot;
+  if (!b8) slot = b4 ? (b2 ? -1 : 2) : b2;           // slots 0, 1, 2
+  else slot = b4 ? -1 : 3 + b2;                       // slots 3, 4
+  if (slot < 0) return -1;
+  const int m = b16 ? 5 + slot : slot;
+  return (m < kMoments && (lane & 1) == 0) ? m : -1;
+}
+
 template <bool FADE, bool DETERMINISTIC>
 __global__ void __launch_bounds__(kThreads)
     backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec, int64_t n,
                     const float* __restrict__ den, const float* __restrict__ out,
                     const int32_t* __restrict__ gids, int64_t cap,
                     const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
-                    int normalize, float eps, float tail, int has_opacity,
-                    float* __restrict__ g_means, float* __restrict__ g_conics,
-                    float* __restrict__ g_colors, float* __restrict__ g_opac,
-                    float4* __restrict__ partials, uint32_t* status) {
+                    int normalize, float eps, float tail, float* __restrict__ moments,
+                    float* __restrict__ partials, uint32_t* status) {
   __shared__ __align__(16) float4 stage[2][kChunk][4];
-  __shared__ float4 pix[TS * TS];
+  __shared__ float4 pix[TS * TS + 1];
   const int tile = blockIdx.x;
   const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
   {
@@ -223,8 +261,10 @@ __global__ void __launch_bounds__(kThreads)
     }
     pix[threadIdx.x] = v;
   }
+  if (threadIdx.x == 0) pix[TS * TS] = make_float4(0.f, 0.f, 0.f, 0.f);  // masked slots read it
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int half = lane >> 4, hl = lane & 15;
+  const int my_moment = moment_of_lane(lane);
+  const int col_slot = lane & 7, row_seg = lane >> 3;
   const TileList L = tile_list(gids, offsets, cap, n, tile);
   if (DETERMINISTIC && L.direct) {
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
@@ -236,93 +276,104 @@ __global__ void __launch_bounds__(kThreads)
   for (int c = 0; c < nchunks; ++c) {
     const int64_t k0 = (int64_t)c * kChunk;
     if (c + 1 < nchunks)
-      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk,
-                  chunk_len(L.count, k0 + kChunk));
+      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
     cp_async_commit();
     cp_async_wait_one();
     __syncthreads();
     const int m = chunk_len(L.count, k0);
     const float4(*st)[4] = stage[c & 1];
-    // Both halves of a warp run the same number of iterations so the shuffles stay converged.
-    for (int base = 2 * warp; base < m; base += 2 * (kThreads / 32)) {
-      const int j = base + half;
+    // One staged Gaussian per warp.  Lane (col_slot, row_seg) walks columns col_slot,
+    // col_slot + 8, … of the rectangle inside the tile and the row_seg-th quarter of its rows;
+    // all loop bounds are the Gaussian's, so the warp never diverges.  Slots outside the
+    // rectangle read a zero pixel with a -inf exponent and contribute nothing.
+    for (int j = warp; j < m; j += kThreads / 32) {
+      const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
+      const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+      const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
+      const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
+      const int seg_rows = (cy1 - cy0 + 3) >> 2;
+      const int ry0 = cy0 + row_seg * seg_rows;
+      const int rows = max(min(seg_rows, cy1 - ry0), 0);
+      const int passes = (cx1 - cx0 + 7) >> 3;
       float acc[kMoments];
 #pragma unroll
       for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
-      float4 p0 = make_float4(0.f, 0.f, 0.f, 0.f), p1 = p0, p2 = p0;
-      if (j < m) {
-        p0 = st[j][0];
-        p1 = st[j][1];
-        p2 = st[j][2];
-        const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
-        const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
-        const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
-        // Column strips: lane (hl & 7) takes every 8th column of the rectangle inside the
-        // tile, lane half (hl >> 3) the upper or lower half of its rows.  Along a column dx is
-        // constant, so Σt·dx, Σt·dx², Σt·dx·dy fold into per-column products.
-        const int half_rows = (cy1 - cy0 + 1) >> 1;
-        const int ry0 = cy0 + (hl >> 3) * half_rows;
-        const int ry1 = min(ry0 + half_rows, cy1);
-        const float dy0 = (float)(ty0 + ry0) - p0.y;
-        for (int cx = cx0 + (hl & 7); cx < cx1; cx += 8) {
-          const float dx = (float)(tx0 + cx) - p0.x;
-          const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
-          float tc = 0.f, uc = 0.f, dy = dy0;
-          const float4* gp = pix + ry0 * TS + cx;
-          for (int ry = ry0; ry < ry1; ++ry, dy += 1.0f, gp += TS) {
-            const float4 g = *gp;
-            const float raw = fast_exp2(fmaf(dy, fmaf(p1.x, dy, bdx), adx2));
-            const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-            const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
-            acc[0] = fmaf(base_w, g.x, acc[0]);
-            acc[1] = fmaf(base_w, g.y, acc[1]);
-            acc[2] = fmaf(base_w, g.z, acc[2]);
-            acc[3] = fmaf(base_w, dw, acc[3]);
-            const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
-            const float u = t * dy;
-            tc += t;
-            uc += u;
-            acc[8] = fmaf(u, dy, acc[8]);
-          }
-          acc[4] = fmaf(dx, tc, acc[4]);
-          acc[5] += uc;
-          acc[6] = fmaf(dx * dx, tc, acc[6]);
-          acc[7] = fmaf(dx, uc, acc[7]);
+      for (int pass = 0; pass < passes; ++pass) {
+        const int cx = cx0 + col_slot + 8 * pass;
+        const bool col_ok = cx < cx1;
+        const float dx = (float)(tx0 + cx) - p0.x;
+        const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+        float tc = 0.f, uc = 0.f;
+        float dy = (float)(ty0 + ry0) - p0.y;
+        int pidx = ry0 * TS + cx;
+        for (int k = 0; k < seg_rows; ++k, dy += 1.0f, pidx += TS) {
+          const bool ok = col_ok && k < rows;
+          const float4 g = pix[ok ? pidx : TS * TS];
+          const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
+          const float raw = fast_exp2(ok ? e : -INFINITY);
+          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
+          acc[0] = fmaf(base_w, g.x, acc[0]);
+          acc[1] = fmaf(base_w, g.y, acc[1]);
+          acc[2] = fmaf(base_w, g.z, acc[2]);
+          acc[3] = fmaf(base_w, dw, acc[3]);
+          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+          const float u = t * dy;
+          tc += t;
+          uc += u;
+          acc[8] = fmaf(u, dy, acc[8]);
         }
+        acc[4] = fmaf(dx, tc, acc[4]);
+        acc[5] += uc;
+        acc[6] = fmaf(dx * dx, tc, acc[6]);
+        acc[7] = fmaf(dx, uc, acc[7]);
       }
-#pragma unroll
-      for (int k = 0; k < kMoments; ++k) {
-        float v = acc[k];
-        v += __shfl_xor_sync(0xffffffffu, v, 8);
-        v += __shfl_xor_sync(0xffffffffu, v, 4);
-        v += __shfl_xor_sync(0xffffffffu, v, 2);
-        v += __shfl_xor_sync(0xffffffffu, v, 1);
-        acc[k] = v;
-      }
-      if (hl == 0 && j < m) {
+      const float total = reduce_scatter9(acc, lane);
+      if (my_moment >= 0) {
         const int64_t entry = L.first + k0 + j;
         if (DETERMINISTIC) {
-          float4* dst = partials + 3 * entry;
-          dst[0] = make_float4(acc[0], acc[1], acc[2], acc[3]);
-          dst[1] = make_float4(acc[4], acc[5], acc[6], acc[7]);
-          dst[2] = make_float4(acc[8], 0.f, 0.f, 0.f);
+          partials[entry * kPartialFloats + my_moment] = total;
         } else {
-          const int g = L.gid(k0 + j);
-          const float op = p1.y, a = p2.y, b = p2.z, cc = p2.w;
-          atomicAdd(g_means + 2 * g, op * (a * acc[4] + b * acc[5]));
-          atomicAdd(g_means + 2 * g + 1, op * (b * acc[4] + cc * acc[5]));
-          atomicAdd(g_conics + 3 * g, -0.5f * op * acc[6]);
-          atomicAdd(g_conics + 3 * g + 1, -op * acc[7]);
-          atomicAdd(g_conics + 3 * g + 2, -0.5f * op * acc[8]);
-          atomicAdd(g_colors + 3 * g, op * acc[0]);
-          atomicAdd(g_colors + 3 * g + 1, op * acc[1]);
-          atomicAdd(g_colors + 3 * g + 2, op * acc[2]);
-          if (has_opacity) atomicAdd(g_opac + g, acc[3]);
+          atomicAdd(moments + (int64_t)my_moment * n + L.gid(k0 + j), total);
         }
       }
     }
     __syncthreads();
   }
+}
+
+// Gradients from a Gaussian's nine summed moments m (see the header of this file).
+__device__ __forceinline__ void write_gradients(const Splat* rec, int64_t g, const float (&m)[9],
+                                                int has_opacity, float* g_means,
+                                                float* g_conics, float* g_colors,
+                                                float* g_opac) {
+  const float4 p1 = reinterpret_cast<const float4*>(rec + g)[1];
+  const float4 p2 = reinterpret_cast<const float4*>(rec + g)[2];
+  const float op = p1.y, a = p2.y, b = p2.z, c = p2.w;
+  g_means[2 * g] = op * (a * m[4] + b * m[5]);
+  g_means[2 * g + 1] = op * (b * m[4] + c * m[5]);
+  g_conics[3 * g] = -0.5f * op * m[6];
+  g_conics[3 * g + 1] = -op * m[7];
+  g_conics[3 * g + 2] = -0.5f * op * m[8];
+  g_colors[3 * g] = op * m[0];
+  g_colors[3 * g + 1] = op * m[1];
+  g_colors[3 * g + 2] = op * m[2];
+  if (has_opacity) g_opac[g] = m[3];
+}
+
+// Fast-mode epilogue: per-Gaussian factors applied once to the atomically summed moments.
+__global__ void finalize_moments_kernel(const Splat* __restrict__ rec, int64_t n,
+                                        const float* __restrict__ moments, int has_opacity,
+                                        float* __restrict__ g_means,
+                                        float* __restrict__ g_conics,
+                                        float* __restrict__ g_colors,
+                                        float* __restrict__ g_opac) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  float m[kMoments];
+#pragma unroll
+  for (int k = 0; k < kMoments; ++k) m[k] = moments[k * n + g];
+  write_gradients(rec, g, m, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
 // Deterministic second pass: Gaussian g sums its per-tile partials over the tiles of its
@@ -331,14 +382,12 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
                                        const int32_t* __restrict__ gids, int64_t cap,
                                        const int32_t* __restrict__ offsets, int tiles_x,
-                                       const float4* __restrict__ partials, int has_opacity,
+                                       const float* __restrict__ partials, int has_opacity,
                                        float* __restrict__ g_means, float* __restrict__ g_conics,
                                        float* __restrict__ g_colors,
                                        float* __restrict__ g_opac) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
-  const float4* src = reinterpret_cast<const float4*>(rec + g);
-  const float4 p1 = src[1], p2 = src[2];
   const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
   float acc[kMoments] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (r.z > r.x && r.w > r.y) {
@@ -354,24 +403,14 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
           if (gids[mid] < g) lo = mid + 1; else hi = mid;
         }
         if (lo < end && gids[lo] == g) {
-          const float4 a = partials[3 * lo], b = partials[3 * lo + 1], c = partials[3 * lo + 2];
-          acc[0] += a.x; acc[1] += a.y; acc[2] += a.z; acc[3] += a.w;
-          acc[4] += b.x; acc[5] += b.y; acc[6] += b.z; acc[7] += b.w;
-          acc[8] += c.x;
+          const float* pp = partials + lo * kPartialFloats;
+#pragma unroll
+          for (int k = 0; k < kMoments; ++k) acc[k] += pp[k];
         }
       }
     }
   }
-  const float op = p1.y, a = p2.y, b = p2.z, cc = p2.w;
-  g_means[2 * g] = op * (a * acc[4] + b * acc[5]);
-  g_means[2 * g + 1] = op * (b * acc[4] + cc * acc[5]);
-  g_conics[3 * g] = -0.5f * op * acc[6];
-  g_conics[3 * g + 1] = -op * acc[7];
-  g_conics[3 * g + 2] = -0.5f * op * acc[8];
-  g_colors[3 * g] = op * acc[0];
-  g_colors[3 * g + 1] = op * acc[1];
-  g_colors[3 * g + 2] = op * acc[2];
-  if (has_opacity) g_opac[g] = acc[3];
+  write_gradients(rec, g, acc, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
 int check_render_args(int64_t n, int H, int W, int ts, float eps) {
@@ -425,7 +464,8 @@ int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int dete
                                        size_t* bytes) {
   if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
   if (n < 0 || gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
-  *bytes = deterministic ? (size_t)gid_capacity * kPartialFloats * sizeof(float) : 0;
+  *bytes = deterministic ? (size_t)gid_capacity * kPartialFloats * sizeof(float)
+                        : (size_t)n * kMoments * sizeof(float);
   return SS_OK;
 }
 
@@ -443,31 +483,33 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
     return fail(SS_ERR_INVALID_ARGUMENT, "null gradient output");
   cudaStream_t s = as_stream(stream);
   const int64_t npx = (int64_t)height * width;
-  if (!deterministic || npx == 0) {
+  if (npx == 0) {  // nothing is rendered: every gradient is zero
     cudaMemsetAsync(grad_means, 0, sizeof(float) * 2 * n, s);
     cudaMemsetAsync(grad_conics, 0, sizeof(float) * 3 * n, s);
     cudaMemsetAsync(grad_colors, 0, sizeof(float) * 3 * n, s);
     if (has_opacity) cudaMemsetAsync(grad_opacities, 0, sizeof(float) * n, s);
-    if ((rc = check_launch("backward zero-fill"))) return rc;
+    return check_launch("backward zero-fill");
   }
-  if (npx == 0) return SS_OK;
   if (!grad_out || !records || !den || !out || !tile_offsets)
     return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  if (normalize && !(eps > 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "bad eps");
   size_t need = 0;
   ss_render_backward_workspace_bytes(n, gid_capacity, deterministic, &need);
-  if (deterministic && (workspace_bytes < need || !workspace))
-    return fail(SS_ERR_INVALID_ARGUMENT, "deterministic backward workspace too small");
+  if (workspace_bytes < need || !workspace)
+    return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+                workspace_bytes, need);
   const int tiles_x = (width + TS - 1) / TS, tiles_y = (height + TS - 1) / TS;
   const int64_t T = (int64_t)tiles_x * tiles_y;
   const Splat* rec = static_cast<const Splat*>(records);
   const bool fade = fade_tail > 0.0f;
-  float4* partials = static_cast<float4*>(workspace);
+  float* ws = static_cast<float*>(workspace);
+  if (!deterministic) {
+    if (cudaMemsetAsync(ws, 0, sizeof(float) * kMoments * n, s) != cudaSuccess)
+      return check_launch("backward moment zero-fill");
+  }
 #define SS_BWD(FADE, DET)                                                                       \
   backward_kernel<FADE, DET><<<(unsigned)T, kThreads, 0, s>>>(                                  \
       grad_out, rec, n, den, out, tile_gids, gid_capacity, tile_offsets, height, width, tiles_x, \
-      normalize, eps, fade_tail, has_opacity, grad_means, grad_conics, grad_colors,             \
-      grad_opacities, partials, status)
+      normalize, eps, fade_tail, ws, ws, status)
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
@@ -475,13 +517,17 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
   }
 #undef SS_BWD
   if ((rc = check_launch("render_backward"))) return rc;
-  if (deterministic) {
-    reduce_partials_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-        rec, n, tile_gids, gid_capacity, tile_offsets, tiles_x, partials, has_opacity, grad_means,
-        grad_conics,
-        grad_colors, grad_opacities);
-    if ((rc = check_launch("reduce_partials"))) return rc;
-  }
+  const unsigned gblocks = (unsigned)((n + kThreads - 1) / kThreads);
+  if (deterministic)
+    reduce_partials_kernel<<<gblocks, kThreads, 0, s>>>(rec, n, tile_gids, gid_capacity,
+                                                        tile_offsets, tiles_x, ws, has_opacity,
+                                                        grad_means, grad_conics, grad_colors,
+                                                        grad_opacities);
+  else
+    finalize_moments_kernel<<<gblocks, kThreads, 0, s>>>(rec, n, ws, has_opacity, grad_means,
+                                                         grad_conics, grad_colors,
+                                                         grad_opacities);
+  if ((rc = check_launch("backward epilogue"))) return rc;
   return SS_OK;
 }
 
