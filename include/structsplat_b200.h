@@ -100,6 +100,21 @@ int ss_tile_index_fill(const void* records, int64_t n, int height, int width, in
                        int32_t* tile_gids, int64_t gid_capacity, void* workspace,
                        size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
 
+/* Allocation-free variant of ss_build_tile_index, for callers that cannot allocate device
+ * memory while building an index (an engine that owns all device memory through its own pool,
+ * a plugin limited to the buffers it is handed, code that must not trigger the device
+ * synchronisation an allocation implies).  It takes no workspace: its scratch is a 5 MiB
+ * device array compiled into the library and held on every GPU that loads it.  Limits:
+ * n <= 65536 Gaussians and at most 16384 tiles (SS_ERR_CAPACITY beyond).  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised.  The first call on each
+ * device resolves the array's address (cudaGetSymbolAddress) with that device current and
+ * should come before any stream capture on it.  No counterpart in the reference. */
+int ss_build_tile_index_static(const float* means, const float* conics, const int64_t* radii,
+                               int64_t n, int height, int width, int tile_size,
+                               int ellipse_cull, float sigma_cutoff, int32_t* tile_gids,
+                               int64_t gid_capacity, int32_t* tile_offsets, uint32_t* status,
+                               ss_stream_t stream);
+
 /* ---------------------------------------------------------------- render
  * Supported render tile sizes: 16 (the reference default).  fade_tail is
  * alpha*exp(-cutoff^2/2) rounded to float (0 = no fade); eps > 0 and finite.

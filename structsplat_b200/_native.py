@@ -32,6 +32,8 @@ SIGNATURES = {
                             _vp, _vp],
     "ss_tile_index_fill": [_vp, _i64, _int, _int, _int, _int, _f32, _vp, _vp, _i64, _vp,
                            ctypes.c_size_t, _vp, _vp],
+    "ss_build_tile_index_static": [_vp, _vp, _vp, _i64, _int, _int, _int, _int, _f32, _vp, _i64,
+                                   _vp, _vp, _vp],
     "ss_render_forward": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _f32, _f32, _vp, _vp,
                           _vp, _vp],
     "ss_render_backward_workspace_bytes": [_i64, _i64, _int, _szp],
