@@ -124,14 +124,15 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
                       int tile_size, int normalize, float eps, float fade_tail, float* out,
                       float* den, uint32_t* status, ss_stream_t stream);
 
-/* Workspace for the deterministic backward (0 bytes for the atomic one). */
-int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
-                                       size_t* bytes);
+/* Workspace of ss_render_backward: per-pixel gradient inputs (16 B per pixel) plus per-Gaussian
+ * moment accumulators (36 B per Gaussian) or, deterministic, per-entry partials (48 B each). */
+int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,
+                                       int deterministic, size_t* bytes);
 /* Gradients of sum(out * grad_out) w.r.t. means (n,2), conics (n,3), colors (n,3) and, when
- * has_opacity, opacities (n).  Outputs are overwritten.  deterministic=0 reduces each
- * (tile, Gaussian) pair in-warp and adds it with one atomic per component; deterministic=1
- * stores the per-pair partials and sums them per Gaussian in ascending tile order, which is
- * bitwise reproducible run to run. */
+ * has_opacity, opacities (n).  Outputs are overwritten.  Each warp reduces one Gaussian's part
+ * inside a 128x128-pixel block (a single tile when fade_tail > 0, as the index may then be
+ * ellipse-culled); deterministic=0 adds it with one atomic per moment, deterministic=1 stores
+ * it and sums a Gaussian's parts in ascending block order, which is bitwise reproducible. */
 int ss_render_backward(const float* grad_out, const void* records, int64_t n, const float* den,
                        const float* out, const int32_t* tile_gids, int64_t gid_capacity,
                        const int32_t* tile_offsets, int height, int width, int tile_size,

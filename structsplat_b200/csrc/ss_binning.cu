@@ -19,7 +19,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kSmallRect = 8;          // tiles a lane enumerates alone; larger rects use the warp
-constexpr int kWarpSortMax = 1024;     // per-warp shared-memory sort capacity (ints)
+constexpr int kWarpSortMax = 1024;     // per-warp register sort capacity (ints)
 constexpr int kBigSortSmem = 16384;    // per-CTA shared-memory sort capacity (ints)
 // Per-tile counters sit one per 32-byte sector: a tile receives one atomic per Gaussian that
 // touches it, and packing 8 neighbouring tiles' counters into a sector would serialise their
@@ -293,13 +293,12 @@ __device__ __forceinline__ void warp_sort_list(int32_t* __restrict__ g, int len,
     if (32 * k + lane < len) g[32 * k + lane] = v[k];
 }
 
-// One warp per tile: lists up to 256 ids sort in registers, up to kWarpSortMax in shared
-// memory; longer lists are queued for tile_sort_big_kernel.
+// One warp per tile: lists up to kWarpSortMax ids sort in registers (32 K keys for the smallest
+// power-of-two K that holds the list); longer lists are queued for tile_sort_big_kernel.
 __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __restrict__ offsets,
                                                              int32_t* __restrict__ gids,
                                                              int64_t cap, int64_t T,
                                                              int* big_tiles, int* big_count) {
-  __shared__ int buf[kThreads / 32][kWarpSortMax];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + warp;
   if (t >= T) return;
@@ -316,12 +315,10 @@ __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __re
     warp_sort_list<4>(g, len, lane);
   } else if (len <= 256) {
     warp_sort_list<8>(g, len, lane);
+  } else if (len <= 512) {
+    warp_sort_list<16>(g, len, lane);
   } else if (len <= kWarpSortMax) {
-    int* b = buf[warp];
-    for (int k = lane; k < len; k += 32) b[k] = g[k];
-    __syncwarp();
-    bitonic_sort(b, len, lane, 32, [] { __syncwarp(); });
-    for (int k = lane; k < len; k += 32) g[k] = b[k];
+    warp_sort_list<32>(g, len, lane);
   } else if (lane == 0) {
     big_tiles[atomicAdd(big_count, 1)] = (int)t;
   }

@@ -19,9 +19,9 @@ struct RefWorkspace {
   size_t backward_bytes;
 };
 
-size_t backward_bytes(int64_t n) {
+size_t backward_bytes(int64_t n, int H, int W) {
   size_t b = 0;
-  ss_render_backward_workspace_bytes(n, 0, 0, &b);
+  ss_render_backward_workspace_bytes(n, 0, H, W, 0, &b);
   return b;
 }
 
@@ -29,7 +29,7 @@ int carve_ref(void* ws, size_t ws_bytes, int64_t n, int H, int W, int ts, RefWor
   size_t idx = 0;
   int rc = ss_tile_index_workspace_bytes(n, H, W, ts, &idx);
   if (rc) return rc;
-  size_t need = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n);
+  size_t need = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n, H, W);
   if (!ws || ws_bytes < need)
     return fail(SS_ERR_INVALID_ARGUMENT, "workspace too small (%zu < %zu)", ws_bytes, need);
   if (reinterpret_cast<uintptr_t>(ws) % 256)
@@ -38,7 +38,7 @@ int carve_ref(void* ws, size_t ws_bytes, int64_t n, int H, int W, int ts, RefWor
   out->index_ws = static_cast<char*>(ws) + align256((size_t)n * sizeof(Splat));
   out->index_bytes = idx;
   out->backward_ws = static_cast<char*>(out->index_ws) + align256(idx);
-  out->backward_bytes = backward_bytes(n);
+  out->backward_bytes = backward_bytes(n, H, W);
   return SS_OK;
 }
 
@@ -61,7 +61,7 @@ int ss_reference_workspace_bytes(int64_t n, int height, int width, int tile_size
   int rc = ss_tile_index_workspace_bytes(n, height, width, tile_size, &idx);
   if (rc) return rc;
   (void)gid_capacity;
-  *bytes = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n);
+  *bytes = align256((size_t)n * sizeof(Splat)) + align256(idx) + backward_bytes(n, height, width);
   return SS_OK;
 }
 

@@ -1,36 +1,49 @@
 // Tiled forward and backward of the clipped-support normalized / additive renderer.
 //
-// Forward (render_ext.cu:349-431 contract): one CTA per 16x16 tile.  The tile's Gaussian list is
-// staged 64 records at a time into shared memory with cp.async, double-buffered, so the next
-// chunk's gather from L2 overlaps the current chunk's math.  Each warp owns an 8x4 pixel
-// sub-block (one pixel per lane) and skips, warp-uniformly, every staged Gaussian whose support
-// rectangle misses the sub-block; inside, a lane's in-rectangle test masks its own pixel.  The
-// weight is 2^(qa dx^2 + qb dx dy + qc dy^2) on the SFU.  The epilogue writes den raw and
-// out = num / (den + eps) or num.
+// Both kernels run one CTA per TS x TS tile (TS = 16 or 32) and stage the tile's Gaussian list
+// 64 records at a time into shared memory with cp.async, double-buffered, so the L2 gather of
+// the next chunk overlaps the math on the current one.
 //
-// Backward (render_ext.cu:696-847 contract): one CTA per tile.  A prologue turns grad_out, out
-// and den into per-pixel (dnum_r, dnum_g, dnum_b, dden) in shared memory.  Work is then
-// Gaussian-major: each half-warp takes one staged Gaussian and walks exactly the pixels of its
-// support rectangle inside the tile (no out-of-rectangle work), accumulating nine moments
-//   R_c = Σ base·dnum_c,  G = Σ base·dw,  S1 = Σ t dx,  S2 = Σ t dy,  S3 = Σ t dx²,
-//   S4 = Σ t dx dy,  S5 = Σ t dy²,   with dw = dnum·c + dden and t = raw·dw (0 where the fade
-// clamps), from which
+// Forward (render_ext.cu:349-431 contract): each warp owns an 8x8 pixel block (two pixels per
+// lane, rows r and r+4).  For every staged chunk a warp builds, with two ballots, the mask of
+// the Gaussians whose support rectangle touches its block and walks only those; a lane masks
+// its own pixels with the in-rectangle test.  The weight is 2^(qa dx^2 + qb dx dy + qc dy^2)
+// on the SFU.  The epilogue writes den raw and out = num / (den + eps) or num.
+//
+// Backward (render_ext.cu:696-847 contract): a prologue turns grad_out, out and den into the
+// per-pixel (dnum_r, dnum_g, dnum_b, dden) of the tile in shared memory.  Work is then
+// Gaussian-major: one warp per staged Gaussian walks exactly the pixels of its support
+// rectangle inside the tile — lane (c, s) takes columns c, c+8, … and the s-th quarter of the
+// rows — and accumulates nine moments
+//   R_k = Σ base·dnum_k,  G = Σ base·dw,  S1 = Σ t dx,  S2 = Σ t dy,  S3 = Σ t dx²,
+//   S4 = Σ t dx dy,  S5 = Σ t dy²,     dw = dnum·c + dden,  t = raw·dw (0 where the fade clamps)
+// from which
 //   dL/dμx = o(a S1 + b S2),  dL/dμy = o(b S1 + c S2),  dL/da = -o S3/2,  dL/db = -o S4,
-//   dL/dc = -o S5/2,  dL/dc_k = o R_k,  dL/do = G
-// which is the reference's per-pixel formula (render_ext.cu:785-818) summed over pixels.  The
-// nine moments are reduced over the 16 lanes with xor shuffles and either added with one atomic
-// per component (fast mode) or stored per (tile, Gaussian) entry and summed per Gaussian in
-// ascending tile order by a second kernel (deterministic mode).
+//   dL/dc = -o S5/2,  dL/dc_k = o R_k,  dL/do = G,
+// i.e. the reference's per-pixel formulas (render_ext.cu:785-818) summed over pixels.  Along a
+// column dx is constant, so S1, S3 and S4 fold into per-column products.  The moments are
+// reduce-scattered over the warp (one moment per lane) and added with one atomic per moment into
+// per-Gaussian accumulators (fast mode), or stored per (tile, Gaussian) entry and summed per
+// Gaussian in ascending tile order by a second kernel (deterministic mode).  A per-Gaussian
+// epilogue applies o, a, b, c once.
 #include "ss_common.cuh"
 
 namespace ss {
 namespace {
 
-constexpr int TS = 16;
-constexpr int kThreads = 256;
-constexpr int kChunk = 64;      // Gaussians per shared-memory stage (4 x 16 B each)
+constexpr int kChunk = 64;          // Gaussians per shared-memory stage (4 x 16 B each)
 constexpr int kMoments = 9;
-constexpr int kPartialFloats = 12;  // one deterministic partial: 9 moments padded to 3 float4
+constexpr int kPartialFloats = 12;  // one deterministic partial: 9 moments, padded
+constexpr int kEpilogueThreads = 256;
+
+template <int TS>
+struct Tiling {
+  static constexpr int kWarps = (TS / 8) * (TS / 8);  // forward: one 8x8 block per warp
+  static constexpr int kFwdThreads = 32 * kWarps;
+  static constexpr int kBwdThreads = TS == 16 ? 256 : 512;
+  // backward whole-list stage: what fits in 48 KB of static shared memory beside the pixels
+  static constexpr int kBwdStageAll = TS == 16 ? 512 : 448;
+};
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -70,33 +83,6 @@ __device__ __forceinline__ int chunk_len(int64_t count, int64_t k0) {
   return r < kChunk ? (int)r : kChunk;
 }
 
-// Issues the copies of list entries [k0, k0+m) into one stage; thread t copies 16-byte piece
-// (t & 3) of entry (t >> 2).
-__device__ __forceinline__ void stage_chunk(float4 (*dst)[4], const Splat* rec, const TileList& L,
-                                            int64_t k0, int m) {
-  int slot = threadIdx.x >> 2, piece = threadIdx.x & 3;
-  if (slot < m) {
-    int g = L.gid(k0 + slot);
-    cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
-  }
-}
-
-constexpr int kFwdThreads = 128;   // 4 warps, each an 8x8 pixel sub-block, 2 pixels per lane
-
-// Issues the copies of entries [k0, k0+m) with kFwdThreads threads (two 16-byte pieces each).
-__device__ __forceinline__ void stage_chunk128(float4 (*dst)[4], const Splat* rec,
-                                               const TileList& L, int64_t k0, int m) {
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int q = threadIdx.x + r * kFwdThreads;
-    const int slot = q >> 2, piece = q & 3;
-    if (slot < m) {
-      const int g = L.gid(k0 + slot);
-      cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
-    }
-  }
-}
-
 // Mask of the staged entries [32 r, 32 r + 32) whose support rectangle touches the 8x8 block
 // at (sx0, sy0): lane l tests entry 32 r + l, a ballot collects the answers.
 __device__ __forceinline__ unsigned hit_mask(const float4 (*st)[4], int m, int sx0, int sy0,
@@ -110,38 +96,32 @@ __device__ __forceinline__ unsigned hit_mask(const float4 (*st)[4], int m, int s
   return __ballot_sync(0xffffffffu, hit);
 }
 
-template <bool NORMALIZE, bool FADE>
-__global__ void __launch_bounds__(kFwdThreads)
-    forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
-                   int64_t cap, const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
-                   float eps, float tail, float* __restrict__ out, float* __restrict__ den) {
-  __shared__ __align__(16) float4 stage[2][kChunk][4];
-  const int tile = blockIdx.x;
-  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int sx0 = tx0 + (warp & 1) * 8, sy0 = ty0 + (warp >> 1) * 8;
-  const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3), py1 = py0 + 4;
-  const float fx = (float)px, fy0 = (float)py0;
-  const TileList L = tile_list(gids, offsets, cap, n, tile);
-  const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
+// Lists up to kStageAll Gaussians are staged whole (one barrier per tile; the warps then run
+// independently); longer lists stream through a double buffer of two kChunk-entry stages.
+constexpr int kStageAll = 512;
 
-  float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
-  if (nchunks > 0) stage_chunk128(stage[0], rec, L, 0, chunk_len(L.count, 0));
-  cp_async_commit();
-  for (int c = 0; c < nchunks; ++c) {
-    const int64_t k0 = (int64_t)c * kChunk;
-    if (c + 1 < nchunks)
-      stage_chunk128(stage[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
-    cp_async_commit();
-    cp_async_wait_one();
-    __syncthreads();
-    const int m = chunk_len(L.count, k0);
-    const float4(*st)[4] = stage[c & 1];
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-    unsigned hits = hit_mask(st, m, sx0, sy0, lane, half);
+// Issues the copies of entries [k0, k0+m) into `dst` with NT threads: 16-byte piece (q & 3) of
+// entry (q >> 2) for q = threadIdx.x, threadIdx.x + NT, …
+template <int NT>
+__device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
+                                            const TileList& L, int64_t k0, int m) {
+  for (int q = threadIdx.x; q < 4 * m; q += NT) {
+    const int slot = q >> 2, piece = q & 3;
+    const int g = L.gid(k0 + slot);
+    cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
+  }
+}
+
+// Accumulates the staged entries [0, m) into one warp's two pixels per lane.
+template <bool FADE>
+__device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int sx0, int sy0,
+                                              int lane, int px, int py0, float fx, float fy0,
+                                              float tail, float (&acc0)[4], float (&acc1)[4]) {
+  const int py1 = py0 + 4;
+  for (int base = 0; base < m; base += 32) {
+    unsigned hits = hit_mask(st + base, m - base, sx0, sy0, lane, 0);
     while (hits) {
-      const int j = 32 * half + __ffs(hits) - 1;
+      const int j = base + __ffs(hits) - 1;
       hits &= hits - 1;
       const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
       const float4 p0 = st[j][0], p1 = st[j][1];
@@ -166,8 +146,47 @@ __global__ void __launch_bounds__(kFwdThreads)
       acc1[2] = fmaf(w1, cb, acc1[2]);
       acc1[3] += w1;
     }
-    }
+  }
+}
+
+template <int TS, bool NORMALIZE, bool FADE>
+__global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
+    forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
+                   int64_t cap, const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
+                   float eps, float tail, float* __restrict__ out, float* __restrict__ den) {
+  constexpr int NT = Tiling<TS>::kFwdThreads;
+  __shared__ __align__(16) float4 stage[kStageAll][4];
+  const int tile = blockIdx.x;
+  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sx0 = tx0 + (warp % (TS / 8)) * 8, sy0 = ty0 + (warp / (TS / 8)) * 8;
+  const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3), py1 = py0 + 4;
+  const float fx = (float)px, fy0 = (float)py0;
+  const TileList L = tile_list(gids, offsets, cap, n, tile);
+
+  float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
+  if (L.count <= kStageAll) {
+    stage_range<NT>(stage, rec, L, 0, (int)L.count);
+    cp_async_commit();
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    forward_block<FADE>(stage, (int)L.count, sx0, sy0, lane, px, py0, fx, fy0, tail, acc0, acc1);
+  } else {
+    float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
+    const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
+    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0));
+    cp_async_commit();
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t k0 = (int64_t)c * kChunk;
+      if (c + 1 < nchunks)
+        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
+      cp_async_commit();
+      cp_async_wait_one();
+      __syncthreads();
+      forward_block<FADE>(buf[c & 1], chunk_len(L.count, k0), sx0, sy0, lane, px, py0, fx, fy0,
+                          tail, acc0, acc1);
+      __syncthreads();
+    }
   }
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
@@ -209,59 +228,57 @@ __device__ __forceinline__ void scatter_level(const float (&v)[N], float (&w)[K]
 // 16, 8, 4, 2, 1 lane l holds the warp total of moment moment_of_lane(l) (or nothing, -1).
 __device__ __forceinline__ float reduce_scatter9(const float (&v)[kMoments], int lane) {
   float a[5], b[3], c[2], d[1];
-  scatter_level<9, 5>(v, a, lane & 16, 16);   // 0-4 | 5-8
-  scatter_level<5, 3>(a, b, lane & 8, 8);     // 0-2 | 3-4
-  scatter_level<3, 2>(b, c, lane & 4, 4);     // 0-1 | 2
-  scatter_level<2, 1>(c, d, lane & 2, 2);     // 0   | 1
+  scatter_level<9, 5>(v, a, lane & 16, 16);  // 0-4 | 5-8
+  scatter_level<5, 3>(a, b, lane & 8, 8);    // 0-2 | 3-4
+  scatter_level<3, 2>(b, c, lane & 4, 4);    // 0-1 | 2
+  scatter_level<2, 1>(c, d, lane & 2, 2);    // 0   | 1
   return d[0] + __shfl_xor_sync(0xffffffffu, d[0], 1);
 }
 
-// Which moment lane l holds after reduce_scatter9 (-1: none); lanes l and l^1 hold the same.
+// Which moment lane l holds after reduce_scatter9 (-1: none); only even lanes report.
 __device__ __forceinline__ int moment_of_lane(int lane) {
   const int b16 = (lane >> 4) & 1, b8 = (lane >> 3) & 1, b4 = (lane >> 2) & 1,
             b2 = (lane >> 1) & 1;
-  // level 1 picks group {0..4} / {5..8}; level 2 slots {0,1,2} / {3,4}; level 3 {0,1} / {2};
-  // level 4 {0} / {1}.
   int slot;
-  if (!b8) slot = b4 ? (b2 ? -1 : 2) : b2;           // slots 0, 1, 2
-  else slot = b4 ? -1 : 3 + b2;                       // slots 3, 4
+  if (!b8) slot = b4 ? (b2 ? -1 : 2) : b2;  // slots 0, 1, 2
+  else slot = b4 ? -1 : 3 + b2;              // slots 3, 4
   if (slot < 0) return -1;
   const int m = b16 ? 5 + slot : slot;
   return (m < kMoments && (lane & 1) == 0) ? m : -1;
 }
 
-template <bool FADE, bool DETERMINISTIC>
-__global__ void __launch_bounds__(kThreads)
-    backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec, int64_t n,
-                    const float* __restrict__ den, const float* __restrict__ out,
+template <int TS, bool FADE, bool DETERMINISTIC>
+__global__ void __launch_bounds__(Tiling<TS>::kBwdThreads, TS == 16 ? 4 : 2)
+    backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec,
+                    int64_t n, const float* __restrict__ den, const float* __restrict__ out,
                     const int32_t* __restrict__ gids, int64_t cap,
                     const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
                     int normalize, float eps, float tail, float* __restrict__ moments,
                     float* __restrict__ partials, uint32_t* status) {
-  __shared__ __align__(16) float4 stage[2][kChunk][4];
-  __shared__ float4 pix[TS * TS + 1];
+  constexpr int NT = Tiling<TS>::kBwdThreads;
+  constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
+  __shared__ __align__(16) float4 stage[kStageMax][4];
+  __shared__ float4 pix[TS * TS + 1];  // the last entry is a zero pixel for masked slots
+  __shared__ int next_entry;
   const int tile = blockIdx.x;
   const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
-  {
-    const int lx = threadIdx.x & (TS - 1), ly = threadIdx.x / TS;
-    const int x = tx0 + lx, y = ty0 + ly;
+  for (int q = threadIdx.x; q <= TS * TS; q += NT) {
+    const int x = tx0 + (q % TS), y = ty0 + (q / TS);
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (x < W && y < H) {
+    if (q < TS * TS && x < W && y < H) {
       const int64_t p = (int64_t)y * W + x;
       const float gr = grad_out[3 * p], gg = grad_out[3 * p + 1], gb = grad_out[3 * p + 2];
+      v = make_float4(gr, gg, gb, 0.f);
       if (normalize) {
         const float denom = den[p] + eps;
         v.x = gr / denom;
         v.y = gg / denom;
         v.z = gb / denom;
         v.w = -(gr * out[3 * p] + gg * out[3 * p + 1] + gb * out[3 * p + 2]) / denom;
-      } else {
-        v = make_float4(gr, gg, gb, 0.f);
       }
     }
-    pix[threadIdx.x] = v;
+    pix[q] = v;
   }
-  if (threadIdx.x == 0) pix[TS * TS] = make_float4(0.f, 0.f, 0.f, 0.f);  // masked slots read it
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int my_moment = moment_of_lane(lane);
   const int col_slot = lane & 7, row_seg = lane >> 3;
@@ -270,75 +287,89 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
     return;
   }
-  const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
-  if (nchunks > 0) stage_chunk(stage[0], rec, L, 0, chunk_len(L.count, 0));
-  cp_async_commit();
-  for (int c = 0; c < nchunks; ++c) {
-    const int64_t k0 = (int64_t)c * kChunk;
-    if (c + 1 < nchunks)
-      stage_chunk(stage[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
-    cp_async_commit();
-    cp_async_wait_one();
-    __syncthreads();
-    const int m = chunk_len(L.count, k0);
-    const float4(*st)[4] = stage[c & 1];
-    // One staged Gaussian per warp.  Lane (col_slot, row_seg) walks columns col_slot,
-    // col_slot + 8, … of the rectangle inside the tile and the row_seg-th quarter of its rows;
-    // all loop bounds are the Gaussian's, so the warp never diverges.  Slots outside the
-    // rectangle read a zero pixel with a -inf exponent and contribute nothing.
-    for (int j = warp; j < m; j += kThreads / 32) {
-      const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
-      const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
-      const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
-      const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
-      const int seg_rows = (cy1 - cy0 + 3) >> 2;
-      const int ry0 = cy0 + row_seg * seg_rows;
-      const int rows = max(min(seg_rows, cy1 - ry0), 0);
-      const int passes = (cx1 - cx0 + 7) >> 3;
-      float acc[kMoments];
+  auto work = [&](const float4(*st)[4], int j, int64_t k0) {
+    const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
+    const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+    const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
+    const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
+    const int seg_rows = (cy1 - cy0 + 3) >> 2;
+    const int ry0 = cy0 + row_seg * seg_rows;
+    const int rows = max(min(seg_rows, cy1 - ry0), 0);
+    const int passes = (cx1 - cx0 + 7) >> 3;
+    float acc[kMoments];
 #pragma unroll
-      for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
-      for (int pass = 0; pass < passes; ++pass) {
-        const int cx = cx0 + col_slot + 8 * pass;
-        const bool col_ok = cx < cx1;
-        const float dx = (float)(tx0 + cx) - p0.x;
-        const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
-        float tc = 0.f, uc = 0.f;
-        float dy = (float)(ty0 + ry0) - p0.y;
-        int pidx = ry0 * TS + cx;
-        for (int k = 0; k < seg_rows; ++k, dy += 1.0f, pidx += TS) {
-          const bool ok = col_ok && k < rows;
-          const float4 g = pix[ok ? pidx : TS * TS];
-          const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
-          const float raw = fast_exp2(ok ? e : -INFINITY);
-          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
-          acc[0] = fmaf(base_w, g.x, acc[0]);
-          acc[1] = fmaf(base_w, g.y, acc[1]);
-          acc[2] = fmaf(base_w, g.z, acc[2]);
-          acc[3] = fmaf(base_w, dw, acc[3]);
-          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
-          const float u = t * dy;
-          tc += t;
-          uc += u;
-          acc[8] = fmaf(u, dy, acc[8]);
-        }
-        acc[4] = fmaf(dx, tc, acc[4]);
-        acc[5] += uc;
-        acc[6] = fmaf(dx * dx, tc, acc[6]);
-        acc[7] = fmaf(dx, uc, acc[7]);
+    for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
+    for (int pass = 0; pass < passes; ++pass) {
+      const int cx = cx0 + col_slot + 8 * pass;
+      const bool col_ok = cx < cx1;
+      const float dx = (float)(tx0 + cx) - p0.x;
+      const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+      float tc = 0.f, uc = 0.f;
+      float dy = (float)(ty0 + ry0) - p0.y;
+      int pidx = ry0 * TS + cx;
+      for (int k = 0; k < seg_rows; ++k, dy += 1.0f, pidx += TS) {
+        const bool ok = col_ok && k < rows;
+        const float4 g = pix[ok ? pidx : TS * TS];
+        const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
+        const float raw = fast_exp2(ok ? e : -INFINITY);
+        const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+        const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
+        acc[0] = fmaf(base_w, g.x, acc[0]);
+        acc[1] = fmaf(base_w, g.y, acc[1]);
+        acc[2] = fmaf(base_w, g.z, acc[2]);
+        acc[3] = fmaf(base_w, dw, acc[3]);
+        const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+        const float u = t * dy;
+        tc += t;
+        uc += u;
+        acc[8] = fmaf(u, dy, acc[8]);
       }
-      const float total = reduce_scatter9(acc, lane);
-      if (my_moment >= 0) {
-        const int64_t entry = L.first + k0 + j;
-        if (DETERMINISTIC) {
-          partials[entry * kPartialFloats + my_moment] = total;
-        } else {
-          atomicAdd(moments + (int64_t)my_moment * n + L.gid(k0 + j), total);
-        }
+      acc[4] = fmaf(dx, tc, acc[4]);
+      acc[5] += uc;
+      acc[6] = fmaf(dx * dx, tc, acc[6]);
+      acc[7] = fmaf(dx, uc, acc[7]);
+    }
+    const float total = reduce_scatter9(acc, lane);
+    if (my_moment >= 0) {
+      const int64_t entry = L.first + k0 + j;
+      if (DETERMINISTIC) {
+        partials[entry * kPartialFloats + my_moment] = total;
+      } else {
+        atomicAdd(moments + (int64_t)my_moment * n + L.gid(k0 + j), total);
       }
     }
+  };
+  if (L.count <= kStageMax) {
+    // whole list staged once; warps take Gaussians from a shared counter (load balancing)
+    if (threadIdx.x == 0) next_entry = 0;
+    stage_range<NT>(stage, rec, L, 0, (int)L.count);
+    cp_async_commit();
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    const int count = (int)L.count;
+    for (;;) {
+      int j = 0;
+      if (lane == 0) j = atomicAdd(&next_entry, 1);
+      j = __shfl_sync(0xffffffffu, j, 0);
+      if (j >= count) break;
+      work(stage, j, 0);
+    }
+  } else {
+    float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
+    const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
+    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0));
+    cp_async_commit();
+    for (int c = 0; c < nchunks; ++c) {
+      const int64_t k0 = (int64_t)c * kChunk;
+      if (c + 1 < nchunks)
+        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
+      cp_async_commit();
+      cp_async_wait_one();
+      __syncthreads();
+      const int m = chunk_len(L.count, k0);
+      for (int j = warp; j < m; j += NT / 32) work(buf[c & 1], j, k0);
+      __syncthreads();
+    }
   }
 }
 
@@ -381,7 +412,7 @@ __global__ void finalize_moments_kernel(const Splat* __restrict__ rec, int64_t n
 // ascending list), then applies the per-Gaussian factors once.
 __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
                                        const int32_t* __restrict__ gids, int64_t cap,
-                                       const int32_t* __restrict__ offsets, int tiles_x,
+                                       const int32_t* __restrict__ offsets, int tiles_x, int ts,
                                        const float* __restrict__ partials, int has_opacity,
                                        float* __restrict__ g_means, float* __restrict__ g_conics,
                                        float* __restrict__ g_colors,
@@ -391,7 +422,7 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
   const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
   float acc[kMoments] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (r.z > r.x && r.w > r.y) {
-    const int gx0 = r.x / TS, gx1 = (r.z - 1) / TS, gy0 = r.y / TS, gy1 = (r.w - 1) / TS;
+    const int gx0 = r.x / ts, gx1 = (r.z - 1) / ts, gy0 = r.y / ts, gy1 = (r.w - 1) / ts;
     for (int gy = gy0; gy <= gy1; ++gy) {
       for (int gx = gx0; gx <= gx1; ++gx) {
         const int t = gy * tiles_x + gx;
@@ -416,12 +447,48 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
 int check_render_args(int64_t n, int H, int W, int ts, float eps) {
   if (n < 0 || H < 0 || W < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
   if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
-  if (ts != TS) return fail(SS_ERR_UNSUPPORTED, "render tile_size must be %d, got %d", TS, ts);
+  if (ts != 16 && ts != 32)
+    return fail(SS_ERR_UNSUPPORTED, "render tile_size must be 16 or 32, got %d", ts);
   if (!(eps > 0.0f) || !isfinite(eps))
     return fail(SS_ERR_INVALID_ARGUMENT, "normalization_eps must be finite and > 0");
-  if ((int64_t)H * W > (int64_t)INT32_MAX * 4)
-    return fail(SS_ERR_INVALID_ARGUMENT, "image too large");
   return SS_OK;
+}
+
+template <int TS>
+void launch_forward(unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
+                    const int32_t* gids, int64_t cap, const int32_t* offsets, int H, int W,
+                    int tiles_x, bool normalize, float eps, float tail, float* out, float* den) {
+  constexpr int NT = Tiling<TS>::kFwdThreads;
+  const bool fade = tail > 0.0f;
+#define SS_FWD(NORM, FADE)                                                                   \
+  forward_kernel<TS, NORM, FADE><<<T, NT, 0, s>>>(rec, n, gids, cap, offsets, H, W, tiles_x, \
+                                                  eps, tail, out, den)
+  if (normalize) {
+    if (fade) SS_FWD(true, true); else SS_FWD(true, false);
+  } else {
+    if (fade) SS_FWD(false, true); else SS_FWD(false, false);
+  }
+#undef SS_FWD
+}
+
+template <int TS>
+void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float* grad_out,
+                     const Splat* rec, int64_t n, const float* den, const float* out,
+                     const int32_t* gids, int64_t cap, const int32_t* offsets, int H, int W,
+                     int tiles_x, int normalize, float eps, float tail, float* ws,
+                     uint32_t* status) {
+  constexpr int NT = Tiling<TS>::kBwdThreads;
+  const bool fade = tail > 0.0f;
+#define SS_BWD(FADE, DET)                                                                      \
+  backward_kernel<TS, FADE, DET><<<T, NT, 0, s>>>(grad_out, rec, n, den, out, gids, cap,      \
+                                                  offsets, H, W, tiles_x, normalize, eps, tail, \
+                                                  ws, ws, status)
+  if (deterministic) {
+    if (fade) SS_BWD(true, true); else SS_BWD(false, true);
+  } else {
+    if (fade) SS_BWD(true, false); else SS_BWD(false, false);
+  }
+#undef SS_BWD
 }
 
 }  // namespace
@@ -442,30 +509,26 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
   if (npx == 0) return SS_OK;
   if (!out || !den || !tile_offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
-  const int tiles_x = (width + TS - 1) / TS, tiles_y = (height + TS - 1) / TS;
-  const int64_t T = (int64_t)tiles_x * tiles_y;
-  cudaStream_t s = as_stream(stream);
+  const int tiles_x = (width + tile_size - 1) / tile_size;
+  const int64_t T = (int64_t)tiles_x * ((height + tile_size - 1) / tile_size);
   const Splat* rec = static_cast<const Splat*>(records);
-  const bool fade = fade_tail > 0.0f;
-#define SS_FWD(NORM, FADE)                                                                    \
-  forward_kernel<NORM, FADE><<<(unsigned)T, kFwdThreads, 0, s>>>(rec, n, tile_gids, gid_capacity, \
-                                                              tile_offsets, height, width,    \
-                                                              tiles_x, eps, fade_tail, out, den)
-  if (normalize) {
-    if (fade) SS_FWD(true, true); else SS_FWD(true, false);
-  } else {
-    if (fade) SS_FWD(false, true); else SS_FWD(false, false);
-  }
-#undef SS_FWD
+  cudaStream_t s = as_stream(stream);
+  if (tile_size == 16)
+    launch_forward<16>((unsigned)T, s, rec, n, tile_gids, gid_capacity, tile_offsets, height,
+                       width, tiles_x, normalize, eps, fade_tail, out, den);
+  else
+    launch_forward<32>((unsigned)T, s, rec, n, tile_gids, gid_capacity, tile_offsets, height,
+                       width, tiles_x, normalize, eps, fade_tail, out, den);
   return check_launch("render_forward");
 }
 
-int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
-                                       size_t* bytes) {
+int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,
+                                       int deterministic, size_t* bytes) {
   if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
-  if (n < 0 || gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  if (n < 0 || gid_capacity < 0 || height < 0 || width < 0)
+    return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
   *bytes = deterministic ? (size_t)gid_capacity * kPartialFloats * sizeof(float)
-                        : (size_t)n * kMoments * sizeof(float);
+                         : (size_t)n * kMoments * sizeof(float);
   return SS_OK;
 }
 
@@ -493,42 +556,36 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
   if (!grad_out || !records || !den || !out || !tile_offsets)
     return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   size_t need = 0;
-  ss_render_backward_workspace_bytes(n, gid_capacity, deterministic, &need);
+  ss_render_backward_workspace_bytes(n, gid_capacity, height, width, deterministic, &need);
   if (workspace_bytes < need || !workspace)
     return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
                 workspace_bytes, need);
-  const int tiles_x = (width + TS - 1) / TS, tiles_y = (height + TS - 1) / TS;
-  const int64_t T = (int64_t)tiles_x * tiles_y;
+  const int tiles_x = (width + tile_size - 1) / tile_size;
+  const int64_t T = (int64_t)tiles_x * ((height + tile_size - 1) / tile_size);
   const Splat* rec = static_cast<const Splat*>(records);
-  const bool fade = fade_tail > 0.0f;
   float* ws = static_cast<float*>(workspace);
   if (!deterministic) {
     if (cudaMemsetAsync(ws, 0, sizeof(float) * kMoments * n, s) != cudaSuccess)
       return check_launch("backward moment zero-fill");
   }
-#define SS_BWD(FADE, DET)                                                                       \
-  backward_kernel<FADE, DET><<<(unsigned)T, kThreads, 0, s>>>(                                  \
-      grad_out, rec, n, den, out, tile_gids, gid_capacity, tile_offsets, height, width, tiles_x, \
-      normalize, eps, fade_tail, ws, ws, status)
-  if (deterministic) {
-    if (fade) SS_BWD(true, true); else SS_BWD(false, true);
-  } else {
-    if (fade) SS_BWD(true, false); else SS_BWD(false, false);
-  }
-#undef SS_BWD
-  if ((rc = check_launch("render_backward"))) return rc;
-  const unsigned gblocks = (unsigned)((n + kThreads - 1) / kThreads);
-  if (deterministic)
-    reduce_partials_kernel<<<gblocks, kThreads, 0, s>>>(rec, n, tile_gids, gid_capacity,
-                                                        tile_offsets, tiles_x, ws, has_opacity,
-                                                        grad_means, grad_conics, grad_colors,
-                                                        grad_opacities);
+  if (tile_size == 16)
+    launch_backward<16>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, tile_gids,
+                        gid_capacity, tile_offsets, height, width, tiles_x, normalize, eps,
+                        fade_tail, ws, status);
   else
-    finalize_moments_kernel<<<gblocks, kThreads, 0, s>>>(rec, n, ws, has_opacity, grad_means,
-                                                         grad_conics, grad_colors,
-                                                         grad_opacities);
-  if ((rc = check_launch("backward epilogue"))) return rc;
-  return SS_OK;
+    launch_backward<32>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, tile_gids,
+                        gid_capacity, tile_offsets, height, width, tiles_x, normalize, eps,
+                        fade_tail, ws, status);
+  if ((rc = check_launch("render_backward"))) return rc;
+  const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
+  if (deterministic)
+    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, tile_gids, gid_capacity, tile_offsets, tiles_x, tile_size, ws, has_opacity,
+        grad_means, grad_conics, grad_colors, grad_opacities);
+  else
+    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
+  return check_launch("backward epilogue");
 }
 
 }  // extern "C"

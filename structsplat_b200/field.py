@@ -13,8 +13,9 @@ from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
 from . import _native
-from .render import (DEFAULT_EPS, RECORD_FLOATS, TileIndex, _backward, _forward, _p, _stream,
-                     fade_tail, index_from_records, resolve_fade_alpha, tile_grid, validate_eps)
+from .render import (DEFAULT_EPS, RECORD_FLOATS, RENDER_TILE, TileIndex, _backward, _forward, _p,
+                     _stream, fade_tail, index_from_records, resolve_fade_alpha, tile_grid,
+                     validate_eps)
 
 
 def project(means, log_scales, rotations, colors, opacity_logits, H: int, W: int,
@@ -80,7 +81,7 @@ def render_gaussians(means, log_scales, rotations, colors, H: int, W: int,
                      opacity_logits=None, normalize: bool = True, eps: float = DEFAULT_EPS,
                      sigma_cutoff: float = 3.0, dilation: float = 0.0,
                      support_fade: bool = False, support_fade_alpha: float | None = None,
-                     tile_size: int = 16, tile_ellipse_cull: bool = True,
+                     tile_size: int = RENDER_TILE, tile_ellipse_cull: bool = True,
                      deterministic: bool = False):
     """Render an RS field; differentiable w.r.t. all five parameter tensors.
 
@@ -98,6 +99,8 @@ def render_gaussians(means, log_scales, rotations, colors, H: int, W: int,
         raise ValueError("field tensors must be means (N,2), log_scales (N,2), rotations (N,), "
                          "colors (N,3)")
     tile_grid(H, W, tile_size)
+    if tile_size not in (16, 32):
+        raise ValueError(f"render tile_size must be 16 or 32, got {tile_size}")
     if normalize:
         eps = validate_eps(eps)
     alpha = resolve_fade_alpha(support_fade, support_fade_alpha)

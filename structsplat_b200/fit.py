@@ -19,7 +19,8 @@ from dataclasses import dataclass, field
 import torch
 
 from . import _native
-from .render import DEFAULT_EPS, RECORD_FLOATS, _p, _stream, fade_tail, tile_grid, validate_eps
+from .render import (DEFAULT_EPS, RECORD_FLOATS, RENDER_TILE, _p, _stream, fade_tail, tile_grid,
+                     validate_eps)
 
 PARAM_NAMES = ("means", "log_scales", "rotations", "colors", "opacity_logits")
 
@@ -38,7 +39,7 @@ class RenderPlan:
     has_opacity: bool = True
     capacity: int = 0
     deterministic: bool = False
-    tile_size: int = 16
+    tile_size: int = RENDER_TILE
     device: torch.device = field(default_factory=lambda: torch.device("cuda"))
 
     def __post_init__(self):
@@ -60,7 +61,8 @@ class RenderPlan:
             self.capacity = 1
         self.gids = torch.empty(self.capacity, device=d, dtype=torch.int32)
         self.bwd_ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n,
-                                               self.capacity, int(self.deterministic))
+                                               self.capacity, self.H, self.W,
+                                               int(self.deterministic))
         self.bwd_ws = torch.empty(max(self.bwd_ws_bytes, 16), device=d, dtype=torch.uint8)
         self.image = torch.zeros(self.H, self.W, 3, **f32)
         self.den = torch.zeros(self.H, self.W, **f32)

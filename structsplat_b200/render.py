@@ -210,7 +210,7 @@ def _backward(grad_out, records, n, den, out, index: TileIndex, H, W, normalize,
     g_conics = torch.empty(n, 3, device=dev, dtype=torch.float32)
     g_colors = torch.empty(n, 3, device=dev, dtype=torch.float32)
     g_opac = torch.empty(n, device=dev, dtype=torch.float32) if has_opacity else None
-    ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n, index.capacity,
+    ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n, index.capacity, H, W,
                                   int(deterministic))
     ws = torch.empty(max(ws_bytes, 16), device=dev, dtype=torch.uint8)
     _native.call("ss_render_backward", _p(grad_out), _p(records), n, _p(den), _p(out),
@@ -258,20 +258,27 @@ class _B200Render(Function):
                 g_opac if (has_op and need[4]) else None) + (None,) * 9
 
 
+RENDER_TILE = 32  # default render tile (16 is also supported; the forward is identical)
+
+
 def render_b200(means, conics, colors, radii, H: int, W: int, opacities=None,
-                normalize: bool = True, eps: float = DEFAULT_EPS, tile_size: int = 16,
+                normalize: bool = True, eps: float = DEFAULT_EPS, tile_size: int = RENDER_TILE,
                 support_fade: bool = False, sigma_cutoff: float = 3.0,
                 support_fade_alpha: float | None = None, tile_ellipse_cull: bool = True,
                 deterministic: bool = False):
     """Render with the reference's exact normalized / additive equations on the B200 library.
 
-    Arguments mirror ``render_cuda_exact``.  ``tile_ellipse_cull`` only takes effect with the
-    full support fade, the one case where culled pairs have exactly zero weight.
+    Arguments mirror ``render_cuda_exact``; ``tile_size`` may be 16 (the reference default) or
+    32 — every pixel still sums its Gaussians in ascending id, so the image is the same.
+    ``tile_ellipse_cull`` only takes effect with the full support fade, the one case where
+    culled pairs have exactly zero weight.
     ``deterministic`` selects the two-pass backward whose gradients are bitwise reproducible.
     """
     _check_cuda_f32(means, conics, colors)
     _check_shapes(means, conics, colors, radii, opacities)
     tile_grid(H, W, tile_size)
+    if tile_size not in (16, 32):
+        raise ValueError(f"render tile_size must be 16 or 32, got {tile_size}")
     if normalize:
         eps = validate_eps(eps)
     alpha = resolve_fade_alpha(support_fade, support_fade_alpha)

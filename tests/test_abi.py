@@ -77,8 +77,12 @@ def test_argument_validation_without_gpu(lib):
                       ctypes.c_double(0.02), ctypes.c_double(0.15), None, None, None, None, None,
                       None, None, None, 0, None)
     assert rc == 1 and "central gradients" in msg
-    rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 1, ctypes.byref(size))
+    rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 16, 16, 1,
+                      ctypes.byref(size))
     assert rc == 0 and size.value == 100 * 48
+    rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 16, 16, 0,
+                      ctypes.byref(size))
+    assert rc == 0 and size.value == 10 * 36
 
 
 def test_empty_problem_needs_no_device(lib):

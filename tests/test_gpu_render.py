@@ -201,3 +201,26 @@ def test_zero_sized_image():
     img = render_b200(m, torch.ones(1, 3, device="cuda"), torch.ones(1, 3, device="cuda"),
                       torch.ones(1, 2, dtype=torch.long, device="cuda"), 0, 5)
     assert img.shape == (0, 5, 3)
+
+
+@pytest.mark.parametrize("name", ["render_synthetic_64_256.npz", "render_elongated_fade.npz",
+                                  "render_matrix_add_op_d3_f1.npz"])
+def test_render_tile_sizes_agree(name):
+    """16x16 and 32x32 render tiles visit each pixel's Gaussians in the same (ascending) order:
+    identical images, gradients equal to rounding."""
+    require_cuda()
+    z = golden(name)
+    outs = []
+    for ts in (16, 32):
+        m, c, col, r, op = _case(z)
+        leaves = [m, c, col] + ([op] if op is not None else [])
+        for t in leaves:
+            t.requires_grad_(True)
+        alpha = float(z["fade_alpha"])
+        img = render_b200(m, c, col, r, int(z["H"]), int(z["W"]), opacities=op,
+                          normalize=bool(z["normalize"]), eps=float(z["eps"]),
+                          support_fade=alpha > 0, support_fade_alpha=alpha, tile_size=ts)
+        outs.append((img.detach(), torch.autograd.grad(img, leaves, cuda(z["grad_out"]))))
+    assert torch.equal(outs[0][0], outs[1][0])
+    for a, b in zip(outs[0][1], outs[1][1]):
+        assert rel_err(a, b) <= 1e-5
