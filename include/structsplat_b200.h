@@ -44,6 +44,28 @@ enum {
 #define SS_STATUS_INDEX_INT32 0x2u     /* entry total exceeded INT32_MAX */
 #define SS_STATUS_DETERMINISTIC_TRUNCATED 0x4u /* deterministic backward met a truncated index */
 
+/* ---------------------------------------------------------------- batches
+ * A batch renders B images of any sizes as one tile set, so every stage is one launch for the
+ * whole batch.  Image b has tiles_x_b = ceil(W_b/ts) by ceil(H_b/ts) tiles numbered row-major
+ * from first_tile_b (images in order, first_tile_0 = 0); its Gaussians are the ids
+ * [gaussian_base[b], gaussian_base[b+1]) of the concatenated field; its pixels are rows
+ * [pixel_base[b], pixel_base[b] + H_b W_b) of the concatenated (P,3) images and (P) weight sums.
+ * Means and support rectangles are image-local.  Every image renders exactly as it would alone
+ * (the same entries in the same ascending order), so a batch of one image is the plain call.
+ * All tables are device arrays built once per batch shape; the struct itself is read on the
+ * host at each call and may be a stack variable. */
+typedef struct ss_batch {
+  int images;                    /* B >= 1 */
+  int tile_size;                 /* 16 or 32 for the render calls */
+  int64_t tiles;                 /* total tiles T */
+  int64_t pixels;                /* total pixels P */
+  const int32_t* image_table;    /* device (B,4): height, width, tiles_x, first_tile */
+  const int64_t* pixel_base;     /* device (B) */
+  const int32_t* gaussian_base;  /* device (B+1); gaussian_base[B] = n */
+  const int32_t* gaussian_image; /* device (n): image of each Gaussian */
+  const int32_t* tile_image;     /* device (T): image of each tile */
+} ss_batch;
+
 /* ---------------------------------------------------------------- library */
 const char* ss_last_error(void);
 int ss_version(void);
@@ -115,8 +137,24 @@ int ss_build_tile_index_static(const float* means, const float* conics, const in
                                int64_t gid_capacity, int32_t* tile_offsets, uint32_t* status,
                                ss_stream_t stream);
 
+/* Batched forms of ss_project_rs / ss_tile_index_* (see ss_batch).  height/width/tile_size
+ * come from the batch; the index workspace depends only on batch->tiles. */
+int ss_batch_project_rs(const ss_batch* batch, const float* means, const float* log_scales,
+                        const float* rotations, const float* colors,
+                        const float* opacity_logits, int64_t n, float dilation,
+                        float sigma_cutoff, void* records, ss_stream_t stream);
+int ss_batch_tile_index_workspace_bytes(const ss_batch* batch, int64_t n, size_t* bytes);
+int ss_batch_tile_index_count(const ss_batch* batch, const void* records, int64_t n,
+                              int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets,
+                              void* workspace, size_t workspace_bytes, uint32_t* status,
+                              ss_stream_t stream);
+int ss_batch_tile_index_fill(const ss_batch* batch, const void* records, int64_t n,
+                             int ellipse_cull, float sigma_cutoff, const int32_t* tile_offsets,
+                             int32_t* tile_gids, int64_t gid_capacity, void* workspace,
+                             size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+
 /* ---------------------------------------------------------------- render
- * Supported render tile sizes: 16 (the reference default).  fade_tail is
+ * Supported render tile sizes: 16 (the reference default) and 32.  fade_tail is
  * alpha*exp(-cutoff^2/2) rounded to float (0 = no fade); eps > 0 and finite.
  * out (H,W,3) f32 image; den (H,W) f32 raw weight sum without eps. */
 int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
@@ -124,15 +162,14 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
                       int tile_size, int normalize, float eps, float fade_tail, float* out,
                       float* den, uint32_t* status, ss_stream_t stream);
 
-/* Workspace of ss_render_backward: per-pixel gradient inputs (16 B per pixel) plus per-Gaussian
- * moment accumulators (36 B per Gaussian) or, deterministic, per-entry partials (48 B each). */
+/* Workspace of ss_render_backward: per-Gaussian moment accumulators (36 B per Gaussian) or,
+ * deterministic, per-entry partials (48 B per entry of capacity); height and width are unused. */
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,
                                        int deterministic, size_t* bytes);
 /* Gradients of sum(out * grad_out) w.r.t. means (n,2), conics (n,3), colors (n,3) and, when
  * has_opacity, opacities (n).  Outputs are overwritten.  Each warp reduces one Gaussian's part
- * inside a 128x128-pixel block (a single tile when fade_tail > 0, as the index may then be
- * ellipse-culled); deterministic=0 adds it with one atomic per moment, deterministic=1 stores
- * it and sums a Gaussian's parts in ascending block order, which is bitwise reproducible. */
+ * inside one tile; deterministic=0 adds it with one atomic per moment, deterministic=1 stores
+ * it and sums a Gaussian's parts in ascending tile order, which is bitwise reproducible. */
 int ss_render_backward(const float* grad_out, const void* records, int64_t n, const float* den,
                        const float* out, const int32_t* tile_gids, int64_t gid_capacity,
                        const int32_t* tile_offsets, int height, int width, int tile_size,
@@ -140,6 +177,66 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
                        float* grad_means, float* grad_conics, float* grad_colors,
                        float* grad_opacities, int deterministic, void* workspace,
                        size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+
+/* Batched forms of the two render calls: out (P,3), den (P), grad_out (P,3). */
+int ss_batch_render_forward(const ss_batch* batch, const void* records, int64_t n,
+                            const int32_t* tile_gids, int64_t gid_capacity,
+                            const int32_t* tile_offsets, int normalize, float eps,
+                            float fade_tail, float* out, float* den, uint32_t* status,
+                            ss_stream_t stream);
+int ss_batch_render_backward(const ss_batch* batch, const float* grad_out, const void* records,
+                             int64_t n, const float* den, const float* out,
+                             const int32_t* tile_gids, int64_t gid_capacity,
+                             const int32_t* tile_offsets, int normalize, float eps,
+                             float fade_tail, int has_opacity, float* grad_means,
+                             float* grad_conics, float* grad_colors, float* grad_opacities,
+                             int deterministic, void* workspace, size_t workspace_bytes,
+                             uint32_t* status, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- fit iteration
+ * The reference's plain fit iteration (fit.py:3182-3366: render -> pixel loss -> backward ->
+ * torch.optim.Adam step over the five parameter groups of gaussians.py:203-214 -> log-scale
+ * clamp) as three launches after the index build, for a batch of independent fits.
+ *
+ * ss_fit_forward_loss renders, evaluates the per-image pixel loss of fit.py:800-814
+ * (loss_kind 0 l1, 1 l2, 2 charbonnier with charbonnier_eps; the loss of image b is the mean
+ * over its pixels of the channel mean) and writes, per pixel, the backward's input
+ * pixel_grad (P,4) = (dL/dnum_r, dL/dnum_g, dL/dnum_b, dL/dden).  image (P,3) and den (P) are
+ * optional outputs (NULL skips them); loss (B,2), optional, receives per image the loss and
+ * the mean squared error added atomically (zero it first).  target is (P,3). */
+int ss_fit_forward_loss(const ss_batch* batch, const void* records, int64_t n,
+                        const int32_t* tile_gids, int64_t gid_capacity,
+                        const int32_t* tile_offsets, int normalize, float eps, float fade_tail,
+                        const float* target, int loss_kind, float charbonnier_eps,
+                        float* pixel_grad, float* image, float* den, float* loss,
+                        uint32_t* status, ss_stream_t stream);
+/* Workspace of ss_fit_backward: moments (36 B per Gaussian) or, deterministic, per-entry
+ * partials (48 B per entry of capacity). */
+int ss_fit_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
+                                    size_t* bytes);
+/* Render backward from pixel_grad into the workspace.  Fast mode adds into per-Gaussian
+ * moments that must be zero on entry: zero them once, ss_fit_adam_update re-zeroes them. */
+int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
+                    const int32_t* tile_gids, int64_t gid_capacity, const int32_t* tile_offsets,
+                    float fade_tail, const float* pixel_grad, int deterministic,
+                    void* workspace, size_t workspace_bytes, uint32_t* status,
+                    ss_stream_t stream);
+/* Gradients of the five parameter groups from the backward's workspace, then one Adam step
+ * (torch.optim.Adam's multi-tensor step: lerp first moment, step factors formed in double, no
+ * weight decay), then the clamp of log_scales to [log_scale_lo, log_scale_hi[image]] that the
+ * reference's loop applies after the step.  params / exp_avg / exp_avg_sq: 5 device pointers
+ * each, in the order means (n,2), log_scales (n,2), rotations (n), colors (n,3),
+ * opacity_logits (n) (the last may be NULL in all three); lrs: 5 host doubles (the parameter
+ * groups' learning rates); log_scale_hi: device (B) floats.  step_state: device int[2], zero
+ * before the first step; it holds the step count, so the call can be replayed from a CUDA
+ * graph.  In fast mode the moments are zeroed for the next ss_fit_backward. */
+int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
+                       const int32_t* tile_gids, int64_t gid_capacity,
+                       const int32_t* tile_offsets, int deterministic, void* workspace,
+                       float dilation, float* const* params, float* const* exp_avg,
+                       float* const* exp_avg_sq, const double* lrs, double beta1, double beta2,
+                       double adam_eps, float log_scale_lo, const float* log_scale_hi,
+                       int* step_state, ss_stream_t stream);
 
 /* ---------------------------------------------------------------- reference-shaped calls
  * One-call equivalents of the reference extension's entry points, taking its tensor

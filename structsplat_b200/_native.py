@@ -19,6 +19,19 @@ _f32 = ctypes.c_float
 _f64 = ctypes.c_double
 _szp = ctypes.POINTER(ctypes.c_size_t)
 
+
+class SsBatch(ctypes.Structure):
+    """``ss_batch`` of the C header: a batch of images rendered as one tile set."""
+    _fields_ = [("images", ctypes.c_int), ("tile_size", ctypes.c_int),
+                ("tiles", ctypes.c_int64), ("pixels", ctypes.c_int64),
+                ("image_table", _vp), ("pixel_base", _vp), ("gaussian_base", _vp),
+                ("gaussian_image", _vp), ("tile_image", _vp)]
+
+
+_bp = ctypes.POINTER(SsBatch)
+_pp = ctypes.POINTER(_vp)
+_dp = ctypes.POINTER(_f64)
+
 # name -> argtypes (all return int status unless listed in _RESTYPES)
 SIGNATURES = {
     "ss_last_error": [],
@@ -48,6 +61,24 @@ SIGNATURES = {
     "ss_backward_tiled": [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int,
                           _int, _int, _f32, _int, _int, _f32, _vp, _vp, _vp, _vp, _vp,
                           ctypes.c_size_t, _vp, _vp],
+    "ss_batch_project_rs": [_bp, _vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _vp, _vp],
+    "ss_batch_tile_index_workspace_bytes": [_bp, _i64, _szp],
+    "ss_batch_tile_index_count": [_bp, _vp, _i64, _int, _f32, _vp, _vp, ctypes.c_size_t, _vp,
+                                  _vp],
+    "ss_batch_tile_index_fill": [_bp, _vp, _i64, _int, _f32, _vp, _vp, _i64, _vp,
+                                 ctypes.c_size_t, _vp, _vp],
+    "ss_batch_render_forward": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _f32, _f32, _vp, _vp, _vp,
+                                _vp],
+    "ss_batch_render_backward": [_bp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _f32,
+                                 _f32, _int, _vp, _vp, _vp, _vp, _int, _vp, ctypes.c_size_t,
+                                 _vp, _vp],
+    "ss_fit_forward_loss": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _f32, _f32, _vp, _int, _f32,
+                            _vp, _vp, _vp, _vp, _vp, _vp],
+    "ss_fit_backward_workspace_bytes": [_i64, _i64, _int, _szp],
+    "ss_fit_backward": [_bp, _vp, _i64, _vp, _i64, _vp, _f32, _vp, _int, _vp, ctypes.c_size_t,
+                        _vp, _vp],
+    "ss_fit_adam_update": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _vp, _f32, _pp, _pp, _pp, _dp,
+                           _f64, _f64, _f64, _f32, _vp, _vp, _vp],
     "ss_structure_tensor_workspace_bytes": [_int, _int, _int, _szp],
     "ss_structure_tensor": [_vp, _int, _int, _int, _vp, _int, _vp, _int, _int, _int, _f64, _f64,
                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],

@@ -124,12 +124,19 @@ __device__ __forceinline__ Splat load_splat(const Splat* rec, int64_t i) {
 // atomics are in flight together); a larger rectangle is enumerated by the whole warp so one
 // huge Gaussian cannot serialise a lane.  Tile coordinates advance incrementally (no division).
 template <bool CULL, typename Visit>
-__device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int ts, int tiles_x,
-                                                float cutoff2, Visit visit) {
+__device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int ts,
+                                                const Frames& frames, float cutoff2,
+                                                Visit visit) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int lane = threadIdx.x & 31;
   TileRect r{0, 0, 0, 0};
-  if (i < n) r = tile_rect_of(rec, i, ts);
+  int tiles_x = 0, first_tile = 0;
+  if (i < n) {
+    r = tile_rect_of(rec, i, ts);
+    const Frame fr = frame_of_gaussian(frames, i, n);
+    tiles_x = fr.tiles_x;
+    first_tile = fr.first_tile;
+  }
   int cnt = r.gw * r.gh;
   if (cnt > 0 && cnt <= kSmallRect) {
     Splat s;
@@ -138,7 +145,8 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
 #pragma unroll
     for (int k = 0; k < kSmallRect; ++k) {
       if (k < cnt) {
-        if (!(CULL && culled(s, gx, gy, ts, cutoff2))) visit(k, (int)i, gy * tiles_x + gx);
+        if (!(CULL && culled(s, gx, gy, ts, cutoff2)))
+          visit(k, (int)i, first_tile + gy * tiles_x + gx);
         if (++gx == r.gx0 + r.gw) {
           gx = r.gx0;
           ++gy;
@@ -154,13 +162,16 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
     int gy0 = __shfl_sync(0xffffffffu, r.gy0, src);
     int gw = __shfl_sync(0xffffffffu, r.gw, src);
     int total = __shfl_sync(0xffffffffu, cnt, src);
+    const int tx_src = __shfl_sync(0xffffffffu, tiles_x, src);
+    const int base_src = __shfl_sync(0xffffffffu, first_tile, src);
     long long gi = __shfl_sync(0xffffffffu, (long long)i, src);
     Splat s;
     if (CULL) s = load_splat(rec, gi);
     const int step_y = 32 / gw, step_x = 32 - step_y * gw;
     int gy = gy0 + lane / gw, gx = gx0 + lane % gw;
     for (int k = lane; k < total; k += 32) {
-      if (!(CULL && culled(s, gx, gy, ts, cutoff2))) visit(-1, (int)gi, gy * tiles_x + gx);
+      if (!(CULL && culled(s, gx, gy, ts, cutoff2)))
+        visit(-1, (int)gi, base_src + gy * tx_src + gx);
       gx += step_x;
       gy += step_y;
       if (gx >= gx0 + gw) {
@@ -172,9 +183,9 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
 }
 
 template <bool CULL>
-__global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
+__global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, Frames frames,
                                   float cutoff2, int* __restrict__ tile_count) {
-  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2,
+  enumerate_pairs<CULL>(rec, n, ts, frames, cutoff2,
                         [&](int, int, int t) { atomicAdd(tile_count + (int64_t)t * kCounterStride, 1); });
 }
 
@@ -182,7 +193,7 @@ __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int 
 // counting each tile's counter back down, which leaves the counters at zero.  A lane's own
 // (small) rectangle claims all its slots first and stores afterwards, so the atomics overlap.
 template <bool CULL>
-__global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int ts, int tiles_x,
+__global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int ts, Frames frames,
                                  float cutoff2, int64_t T, const long long* __restrict__ off64,
                                  int* __restrict__ tile_count, int32_t* __restrict__ offsets32,
                                  int32_t* __restrict__ gids, int64_t cap, int* big_count,
@@ -200,7 +211,7 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
 #pragma unroll
   for (int k = 0; k < kSmallRect; ++k) pos[k] = -1;
   int owner = -1;
-  enumerate_pairs<CULL>(rec, n, ts, tiles_x, cutoff2, [&](int k, int g, int t) {
+  enumerate_pairs<CULL>(rec, n, ts, frames, cutoff2, [&](int k, int g, int t) {
     long long p = off64[t] + (atomicSub(tile_count + (int64_t)t * kCounterStride, 1) - 1);
     if (k < 0) {
       if (p < cap) gids[p] = g;
@@ -374,6 +385,88 @@ int check_index_args(int64_t n, int H, int W, int ts) {
   return SS_OK;
 }
 
+
+// Stage 1 over any tile set (one image or a batch): counts, scan, int32 offsets.
+int index_count(const Frames& frames, int ts, int64_t T, const void* records, int64_t n,
+                int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets, void* workspace,
+                size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  int rc;
+  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  if (workspace_bytes < index_workspace_bytes(T))
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small (%zu < %zu)",
+                workspace_bytes, index_workspace_bytes(T));
+  cudaStream_t s = as_stream(stream);
+  IndexWorkspace w = carve(workspace, T);
+  if (cudaMemsetAsync(w.tile_count, 0, sizeof(int) * kCounterStride * (T + 1), s) !=
+      cudaSuccess)
+    return check_launch("tile_index_count memset");
+  const Splat* rec = static_cast<const Splat*>(records);
+  float cutoff2 = sigma_cutoff * sigma_cutoff;
+  if (n > 0 && T > 0) {
+    int blocks = (int)((n + kThreads - 1) / kThreads);
+    if (ellipse_cull)
+      tile_count_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2,
+                                                          w.tile_count);
+    else
+      tile_count_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2,
+                                                           w.tile_count);
+    if ((rc = check_launch("tile_count"))) return rc;
+  }
+  size_t sb = w.scan_bytes;
+  cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, counter_iter(w.tile_count),
+                                                 w.offsets64,
+                                                 ::cuda::std::plus<long long>(), (long long)0,
+                                                 (int)(T + 1), s);
+  if (e != cudaSuccess) return fail(SS_ERR_CUDA, "tile offsets scan: %s", cudaGetErrorString(e));
+  // int32 offsets for callers that only run stage 1 (the fill rewrites them identically).
+  tile_fill_kernel<false><<<(int)((T + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+      rec, 0, ts, frames, cutoff2, T, w.offsets64, w.tile_count, tile_offsets, nullptr,
+      INT64_MAX, w.big_count, nullptr);
+  (void)status;
+  return check_launch("tile_offsets");
+}
+
+// Stage 2 over any tile set: fill, per-tile sort.
+int index_fill(const Frames& frames, int ts, int64_t T, const void* records, int64_t n,
+               int ellipse_cull, float sigma_cutoff, const int32_t* tile_offsets,
+               int32_t* tile_gids, int64_t gid_capacity, void* workspace,
+               size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  int rc;
+  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative gid capacity");
+  if (gid_capacity > 0 && !tile_gids) return fail(SS_ERR_INVALID_ARGUMENT, "null tile_gids");
+  if (workspace_bytes < index_workspace_bytes(T))
+    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small");
+  if (T == 0) return SS_OK;
+  cudaStream_t s = as_stream(stream);
+  IndexWorkspace w = carve(workspace, T);
+  const Splat* rec = static_cast<const Splat*>(records);
+  float cutoff2 = sigma_cutoff * sigma_cutoff;
+  int64_t threads_needed = n > T + 1 ? n : T + 1;
+  int blocks = (int)((threads_needed + kThreads - 1) / kThreads);
+  int32_t* offsets32 = const_cast<int32_t*>(tile_offsets);
+  if (ellipse_cull)
+    tile_fill_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2, T,
+                                                       w.offsets64, w.tile_count, offsets32,
+                                                       tile_gids, gid_capacity, w.big_count,
+                                                       status);
+  else
+    tile_fill_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2, T,
+                                                        w.offsets64, w.tile_count, offsets32,
+                                                        tile_gids, gid_capacity, w.big_count,
+                                                        status);
+  if ((rc = check_launch("tile_fill"))) return rc;
+  int sort_blocks = (int)((T + (kThreads / 32) - 1) / (kThreads / 32));
+  tile_sort_kernel<<<sort_blocks, kThreads, 0, s>>>(tile_offsets, tile_gids, gid_capacity, T,
+                                                     w.big_tiles, w.big_count);
+  if ((rc = check_launch("tile_sort"))) return rc;
+  if ((rc = allow_big_sort_smem())) return rc;
+  tile_sort_big_kernel<<<kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s>>>(
+      tile_offsets, tile_gids, w.big_tiles, w.big_count);
+  return check_launch("tile_sort_big");
+}
+
 }  // namespace
 }  // namespace ss
 
@@ -390,47 +483,35 @@ int ss_tile_index_workspace_bytes(int64_t n, int height, int width, int tile_siz
   return SS_OK;
 }
 
+int ss_batch_tile_index_workspace_bytes(const ss_batch* batch, int64_t n, size_t* bytes) {
+  Frames f;
+  int rc = frames_of_batch(batch, n, &f);
+  if (rc) return rc;
+  if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
+  *bytes = index_workspace_bytes(batch->tiles);
+  return SS_OK;
+}
+
 int ss_tile_index_count(const void* records, int64_t n, int height, int width, int tile_size,
                         int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets,
                         void* workspace, size_t workspace_bytes, uint32_t* status,
                         ss_stream_t stream) {
   int rc = check_index_args(n, height, width, tile_size);
   if (rc) return rc;
-  TileGrid g = make_grid(height, width, tile_size);
-  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
-  if (workspace_bytes < index_workspace_bytes(g.T))
-    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small (%zu < %zu)",
-                workspace_bytes, index_workspace_bytes(g.T));
-  cudaStream_t s = as_stream(stream);
-  IndexWorkspace w = carve(workspace, g.T);
-  if (cudaMemsetAsync(w.tile_count, 0, sizeof(int) * kCounterStride * (g.T + 1), s) !=
-      cudaSuccess)
-    return check_launch("tile_index_count memset");
-  const Splat* rec = static_cast<const Splat*>(records);
-  float cutoff2 = sigma_cutoff * sigma_cutoff;
-  if (n > 0 && g.T > 0) {
-    int blocks = (int)((n + kThreads - 1) / kThreads);
-    if (ellipse_cull)
-      tile_count_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2,
-                                                          w.tile_count);
-    else
-      tile_count_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2,
-                                                           w.tile_count);
-    if ((rc = check_launch("tile_count"))) return rc;
-  }
-  size_t sb = w.scan_bytes;
-  cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, counter_iter(w.tile_count),
-                                                 w.offsets64,
-                                                 ::cuda::std::plus<long long>(), (long long)0,
-                                                 (int)(g.T + 1), s);
-  if (e != cudaSuccess) return fail(SS_ERR_CUDA, "tile offsets scan: %s", cudaGetErrorString(e));
-  // int32 offsets for callers that only run stage 1 (the fill rewrites them identically).
-  tile_fill_kernel<false><<<(int)((g.T + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
-      rec, 0, g.ts, g.tiles_x, cutoff2, g.T, w.offsets64, w.tile_count, tile_offsets, nullptr,
-      INT64_MAX, w.big_count, nullptr);
-  (void)status;
-  return check_launch("tile_offsets");
+  return index_count(single_frame(height, width, tile_size), tile_size,
+                     make_grid(height, width, tile_size).T, records, n, ellipse_cull,
+                     sigma_cutoff, tile_offsets, workspace, workspace_bytes, status, stream);
+}
+
+int ss_batch_tile_index_count(const ss_batch* batch, const void* records, int64_t n,
+                              int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets,
+                              void* workspace, size_t workspace_bytes, uint32_t* status,
+                              ss_stream_t stream) {
+  Frames f;
+  int rc = frames_of_batch(batch, n, &f);
+  if (rc) return rc;
+  return index_count(f, batch->tile_size, batch->tiles, records, n, ellipse_cull, sigma_cutoff,
+                     tile_offsets, workspace, workspace_bytes, status, stream);
 }
 
 int ss_tile_index_fill(const void* records, int64_t n, int height, int width, int tile_size,
@@ -439,39 +520,22 @@ int ss_tile_index_fill(const void* records, int64_t n, int height, int width, in
                        size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
   int rc = check_index_args(n, height, width, tile_size);
   if (rc) return rc;
-  TileGrid g = make_grid(height, width, tile_size);
-  if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  if (gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative gid capacity");
-  if (gid_capacity > 0 && !tile_gids) return fail(SS_ERR_INVALID_ARGUMENT, "null tile_gids");
-  if (workspace_bytes < index_workspace_bytes(g.T))
-    return fail(SS_ERR_INVALID_ARGUMENT, "tile index workspace too small");
-  if (g.T == 0) return SS_OK;
-  cudaStream_t s = as_stream(stream);
-  IndexWorkspace w = carve(workspace, g.T);
-  const Splat* rec = static_cast<const Splat*>(records);
-  float cutoff2 = sigma_cutoff * sigma_cutoff;
-  int64_t threads_needed = n > g.T + 1 ? n : g.T + 1;
-  int blocks = (int)((threads_needed + kThreads - 1) / kThreads);
-  int32_t* offsets32 = const_cast<int32_t*>(tile_offsets);
-  if (ellipse_cull)
-    tile_fill_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2, g.T,
-                                                       w.offsets64, w.tile_count, offsets32,
-                                                       tile_gids, gid_capacity, w.big_count,
-                                                       status);
-  else
-    tile_fill_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, g.ts, g.tiles_x, cutoff2, g.T,
-                                                        w.offsets64, w.tile_count, offsets32,
-                                                        tile_gids, gid_capacity, w.big_count,
-                                                        status);
-  if ((rc = check_launch("tile_fill"))) return rc;
-  int sort_blocks = (int)((g.T + (kThreads / 32) - 1) / (kThreads / 32));
-  tile_sort_kernel<<<sort_blocks, kThreads, 0, s>>>(tile_offsets, tile_gids, gid_capacity, g.T,
-                                                     w.big_tiles, w.big_count);
-  if ((rc = check_launch("tile_sort"))) return rc;
-  if ((rc = allow_big_sort_smem())) return rc;
-  tile_sort_big_kernel<<<kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s>>>(
-      tile_offsets, tile_gids, w.big_tiles, w.big_count);
-  return check_launch("tile_sort_big");
+  return index_fill(single_frame(height, width, tile_size), tile_size,
+                    make_grid(height, width, tile_size).T, records, n, ellipse_cull,
+                    sigma_cutoff, tile_offsets, tile_gids, gid_capacity, workspace,
+                    workspace_bytes, status, stream);
+}
+
+int ss_batch_tile_index_fill(const ss_batch* batch, const void* records, int64_t n,
+                             int ellipse_cull, float sigma_cutoff, const int32_t* tile_offsets,
+                             int32_t* tile_gids, int64_t gid_capacity, void* workspace,
+                             size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  Frames f;
+  int rc = frames_of_batch(batch, n, &f);
+  if (rc) return rc;
+  return index_fill(f, batch->tile_size, batch->tiles, records, n, ellipse_cull, sigma_cutoff,
+                    tile_offsets, tile_gids, gid_capacity, workspace, workspace_bytes, status,
+                    stream);
 }
 
 }  // extern "C"

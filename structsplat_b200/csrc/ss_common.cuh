@@ -137,6 +137,133 @@ __device__ __forceinline__ bool culled(const Splat& s, int gx, int gy, int ts, f
   return m > cutoff2 + 1e-5f * fmaxf(cutoff2, 1.0f);
 }
 
+// Chain rule of the RS conic (gaussians.py:275-300): conic gradient (ga, gb, gc) -> log-scale
+// and rotation gradients.  With u = 1/(sx^2+d), v = 1/(sy^2+d) the conic is
+// a = C^2 u + S^2 v, b = CS (u - v), c = S^2 u + C^2 v.
+__device__ __forceinline__ void rs_conic_chain(float ls0, float ls1, float th, float dilation,
+                                               float ga, float gb, float gc, float& g_ls0,
+                                               float& g_ls1, float& g_rot) {
+  const float sx = expf(ls0), sy = expf(ls1);
+  const float sx2 = sx * sx, sy2 = sy * sy;
+  const float u = 1.0f / (sx2 + dilation), v = 1.0f / (sy2 + dilation);
+  float cs, sn;
+  sincosf(th, &sn, &cs);
+  const float cc = cs * cs, s2 = sn * sn, csn = cs * sn;
+  const float gu = ga * cc + gb * csn + gc * s2;
+  const float gv = ga * s2 - gb * csn + gc * cc;
+  g_ls0 = gu * (-2.0f * sx2 * u * u);
+  g_ls1 = gv * (-2.0f * sy2 * v * v);
+  g_rot = (u - v) * (2.0f * csn * (gc - ga) + (cc - s2) * gb);
+}
+
+// d sigmoid(x) / dx applied to an opacity gradient (gaussians.py:270-273).
+__device__ __forceinline__ float logit_chain(float logit, float g_op) {
+  const float o = 1.0f / (1.0f + expf(-logit));
+  return g_op * o * (1.0f - o);
+}
+
+// Where the images of a batch live.  A batch of B images is rendered as one set of tiles: the
+// tiles of image b are tiles [first_tile_b, first_tile_b + tiles_b), numbered row-major inside
+// the image; its Gaussians are ids [gauss_base[b], gauss_base[b+1]); its pixels are pixels
+// [pixel_base[b], pixel_base[b] + H_b W_b) of the concatenated row-major images.  Means, support
+// rectangles and pixel coordinates stay image-local, so every image renders exactly as it would
+// alone.  A single image is the batch with image == nullptr, described by H, W and tiles_x.
+struct Frames {
+  const int4* image;           // per image {H, W, tiles_x, first tile}, or nullptr
+  const long long* pixel_base;  // per image
+  const int* gauss_base;        // per image + 1
+  const int* gauss_image;       // per Gaussian
+  const int* tile_image;        // per tile
+  int H, W, tiles_x;            // the single image (image == nullptr)
+};
+
+// One image of a batch, as seen from a tile or a Gaussian.
+struct Frame {
+  int image, H, W, tiles_x, first_tile;
+  long long pixel_base;
+  int gauss_first, gauss_count;
+};
+
+// Validates a batch description (host side) and converts it to Frames.
+int frames_of_batch(const ss_batch* batch, int64_t n, Frames* out);
+
+inline Frames single_frame(int H, int W, int ts) {
+  Frames f{};
+  f.H = H;
+  f.W = W;
+  f.tiles_x = ts > 0 ? (W + ts - 1) / ts : 0;
+  return f;
+}
+
+__device__ __forceinline__ Frame frame_of_image(const Frames& f, int b, int64_t n) {
+  Frame r;
+  r.image = b;
+  if (!f.image) {
+    r.H = f.H;
+    r.W = f.W;
+    r.tiles_x = f.tiles_x;
+    r.first_tile = 0;
+    r.pixel_base = 0;
+    r.gauss_first = 0;
+    r.gauss_count = (int)n;
+    return r;
+  }
+  const int4 d = f.image[b];
+  r.H = d.x;
+  r.W = d.y;
+  r.tiles_x = d.z;
+  r.first_tile = d.w;
+  r.pixel_base = f.pixel_base[b];
+  r.gauss_first = f.gauss_base[b];
+  r.gauss_count = f.gauss_base[b + 1] - r.gauss_first;
+  return r;
+}
+
+__device__ __forceinline__ Frame frame_of_tile(const Frames& f, int tile, int64_t n) {
+  return frame_of_image(f, f.image ? f.tile_image[tile] : 0, n);
+}
+
+__device__ __forceinline__ Frame frame_of_gaussian(const Frames& f, int64_t g, int64_t n) {
+  return frame_of_image(f, f.image ? f.gauss_image[g] : 0, n);
+}
+
+// The backward's per-(tile, Gaussian) record in deterministic mode: nine moments, padded.
+constexpr int kMoments = 9;
+constexpr int kPartialFloats = 12;
+
+// Deterministic second pass for Gaussian g: sums its per-entry moment partials over the tiles
+// of its support rectangle in ascending tile order, each entry found by binary search in the
+// tile's ascending list.  Tiles whose list was truncated by the capacity contribute nothing (the
+// backward reports them).
+__device__ __forceinline__ void sum_partials(const Splat* rec, int64_t g, int64_t n, int ts,
+                                             const Frames& frames, const int32_t* gids,
+                                             int64_t cap, const int32_t* offsets,
+                                             const float* partials, float (&acc)[kMoments]) {
+#pragma unroll
+  for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
+  const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
+  if (!(r.z > r.x && r.w > r.y)) return;
+  const Frame fr = frame_of_gaussian(frames, g, n);
+  const int gx0 = r.x / ts, gx1 = (r.z - 1) / ts, gy0 = r.y / ts, gy1 = (r.w - 1) / ts;
+  for (int gy = gy0; gy <= gy1; ++gy) {
+    for (int gx = gx0; gx <= gx1; ++gx) {
+      const int t = fr.first_tile + gy * fr.tiles_x + gx;
+      int64_t lo = offsets[t], hi = offsets[t + 1];
+      if (hi > cap) continue;
+      const int64_t end = hi;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (gids[mid] < g) lo = mid + 1; else hi = mid;
+      }
+      if (lo < end && gids[lo] == g) {
+        const float* pp = partials + lo * kPartialFloats;
+#pragma unroll
+        for (int k = 0; k < kMoments; ++k) acc[k] += pp[k];
+      }
+    }
+  }
+}
+
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bits) {
   if (status) atomicOr(status, bits);
 }

@@ -32,8 +32,6 @@ namespace ss {
 namespace {
 
 constexpr int kChunk = 64;          // Gaussians per shared-memory stage (4 x 16 B each)
-constexpr int kMoments = 9;
-constexpr int kPartialFloats = 12;  // one deterministic partial: 9 moments, padded
 constexpr int kEpilogueThreads = 256;
 
 template <int TS>
@@ -57,7 +55,8 @@ __device__ __forceinline__ void cp_async_wait_one() {
 }
 
 // Source of a tile's Gaussians: its index list, or — when the list was truncated by the
-// capacity — every Gaussian in ascending id (the same order, so results are identical).
+// capacity — every Gaussian of its image in ascending id (the same order, so results are
+// identical).
 struct TileList {
   const int32_t* gids;
   int64_t first, count;
@@ -68,13 +67,13 @@ struct TileList {
 };
 
 __device__ __forceinline__ TileList tile_list(const int32_t* gids, const int32_t* offsets,
-                                              int64_t cap, int64_t n, int tile) {
+                                              int64_t cap, const Frame& fr, int tile) {
   TileList L;
   int64_t lo = offsets[tile], hi = offsets[tile + 1];
   L.gids = gids;
   L.direct = hi > cap;
-  L.first = L.direct ? 0 : lo;
-  L.count = L.direct ? n : hi - lo;
+  L.first = L.direct ? fr.gauss_first : lo;
+  L.count = L.direct ? fr.gauss_count : hi - lo;
   return L;
 }
 
@@ -149,20 +148,33 @@ __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int 
   }
 }
 
-template <int TS, bool NORMALIZE, bool FADE>
+// Pixel losses of fit.py:800-809 (mean over channels, then over the image's pixels).
+enum LossKind { kNoLoss = 0, kL1 = 1, kL2 = 2, kCharbonnier = 3 };
+
+// Forward of one tile.  LOSS == kNoLoss: writes out and den.  Otherwise (a fit iteration) it
+// also evaluates the pixel loss against target and writes the backward's per-pixel input
+// pixel_grad = (dL/dnum_rgb, dL/dden) (out and den only when given) and adds each image's loss
+// and mean squared error into loss[2 b], loss[2 b + 1].  The loss gradient repeats autograd's
+// arithmetic for the mean-of-means (1/(H W) then /3) so it is bitwise the eager gradient.
+template <int TS, bool NORMALIZE, bool FADE, int LOSS>
 __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
     forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
-                   int64_t cap, const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
-                   float eps, float tail, float* __restrict__ out, float* __restrict__ den) {
+                   int64_t cap, const int32_t* __restrict__ offsets, Frames frames, float eps,
+                   float tail, float* __restrict__ out, float* __restrict__ den,
+                   const float* __restrict__ target, float4* __restrict__ pixel_grad,
+                   float* __restrict__ loss, float charb_eps2) {
   constexpr int NT = Tiling<TS>::kFwdThreads;
   __shared__ __align__(16) float4 stage[kStageAll][4];
   const int tile = blockIdx.x;
-  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
+  const Frame fr = frame_of_tile(frames, tile, n);
+  const int local = tile - fr.first_tile;
+  const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
+  const int H = fr.H, W = fr.W;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sx0 = tx0 + (warp % (TS / 8)) * 8, sy0 = ty0 + (warp / (TS / 8)) * 8;
   const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3), py1 = py0 + 4;
   const float fx = (float)px, fy0 = (float)py0;
-  const TileList L = tile_list(gids, offsets, cap, n, tile);
+  const TileList L = tile_list(gids, offsets, cap, fr, tile);
 
   float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
   if (L.count <= kStageAll) {
@@ -188,23 +200,67 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
       __syncthreads();
     }
   }
+  float loss_sum = 0.f, sq_sum = 0.f;
+  const float per_pixel = 1.0f / (float)((int64_t)H * W);  // autograd: grad / numel
+  const float per_value = per_pixel / 3.0f;                 // then the channel mean
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     const int py = k ? py1 : py0;
     const float* a = k ? acc1 : acc0;
     if (px < W && py < H) {
-      const int64_t p = (int64_t)py * W + px;
-      den[p] = a[3];
-      if (NORMALIZE) {
-        const float denom = a[3] + eps;
-        out[3 * p] = a[0] / denom;
-        out[3 * p + 1] = a[1] / denom;
-        out[3 * p + 2] = a[2] / denom;
-      } else {
-        out[3 * p] = a[0];
-        out[3 * p + 1] = a[1];
-        out[3 * p + 2] = a[2];
+      const int64_t p = fr.pixel_base + (int64_t)py * W + px;
+      float o[3];
+      const float denom = a[3] + eps;
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) o[ch] = NORMALIZE ? a[ch] / denom : a[ch];
+      if (LOSS == kNoLoss || den) den[p] = a[3];
+      if (LOSS == kNoLoss || out) {
+        out[3 * p] = o[0];
+        out[3 * p + 1] = o[1];
+        out[3 * p + 2] = o[2];
       }
+      if (LOSS != kNoLoss) {
+        float g[3], lp = 0.f, sq = 0.f;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+          const float d = o[ch] - target[3 * p + ch];
+          const float d2 = d * d;
+          sq += d2;
+          if (LOSS == kL2) {
+            g[ch] = per_value * d + per_value * d;
+            lp += d2;
+          } else if (LOSS == kL1) {
+            g[ch] = per_value * (float)((d > 0.f) - (d < 0.f));
+            lp += fabsf(d);
+          } else {
+            const float r = sqrtf(d2 + charb_eps2);
+            const float q = per_value / (2.0f * r);
+            g[ch] = q * d + q * d;
+            lp += r;
+          }
+        }
+        float4 v;
+        if (NORMALIZE) {
+          v = make_float4(g[0] / denom, g[1] / denom, g[2] / denom,
+                          -(g[0] * o[0] + g[1] * o[1] + g[2] * o[2]) / denom);
+        } else {
+          v = make_float4(g[0], g[1], g[2], 0.f);
+        }
+        pixel_grad[p] = v;
+        loss_sum += lp;
+        sq_sum += sq;
+      }
+    }
+  }
+  if (LOSS != kNoLoss && loss) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      loss_sum += __shfl_xor_sync(0xffffffffu, loss_sum, o);
+      sq_sum += __shfl_xor_sync(0xffffffffu, sq_sum, o);
+    }
+    if (lane == 0) {
+      atomicAdd(loss + 2 * fr.image, loss_sum * per_value);
+      atomicAdd(loss + 2 * fr.image + 1, sq_sum * per_value);
     }
   }
 }
@@ -247,12 +303,14 @@ __device__ __forceinline__ int moment_of_lane(int lane) {
   return (m < kMoments && (lane & 1) == 0) ? m : -1;
 }
 
-template <int TS, bool FADE, bool DETERMINISTIC>
+// Backward of one tile.  PIXGRAD: the per-pixel inputs come ready-made from the fit forward
+// (pixel_grad); otherwise they are formed from grad_out, out and den.
+template <int TS, bool FADE, bool DETERMINISTIC, bool PIXGRAD>
 __global__ void __launch_bounds__(Tiling<TS>::kBwdThreads, TS == 16 ? 4 : 2)
     backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec,
                     int64_t n, const float* __restrict__ den, const float* __restrict__ out,
-                    const int32_t* __restrict__ gids, int64_t cap,
-                    const int32_t* __restrict__ offsets, int H, int W, int tiles_x,
+                    const float4* __restrict__ pixel_grad, const int32_t* __restrict__ gids,
+                    int64_t cap, const int32_t* __restrict__ offsets, Frames frames,
                     int normalize, float eps, float tail, float* __restrict__ moments,
                     float* __restrict__ partials, uint32_t* status) {
   constexpr int NT = Tiling<TS>::kBwdThreads;
@@ -261,12 +319,17 @@ __global__ void __launch_bounds__(Tiling<TS>::kBwdThreads, TS == 16 ? 4 : 2)
   __shared__ float4 pix[TS * TS + 1];  // the last entry is a zero pixel for masked slots
   __shared__ int next_entry;
   const int tile = blockIdx.x;
-  const int tx0 = (tile % tiles_x) * TS, ty0 = (tile / tiles_x) * TS;
+  const Frame fr = frame_of_tile(frames, tile, n);
+  const int local = tile - fr.first_tile;
+  const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
+  const int H = fr.H, W = fr.W;
   for (int q = threadIdx.x; q <= TS * TS; q += NT) {
     const int x = tx0 + (q % TS), y = ty0 + (q / TS);
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (q < TS * TS && x < W && y < H) {
-      const int64_t p = (int64_t)y * W + x;
+    if (PIXGRAD) {
+      if (q < TS * TS && x < W && y < H) v = pixel_grad[fr.pixel_base + (int64_t)y * W + x];
+    } else if (q < TS * TS && x < W && y < H) {
+      const int64_t p = fr.pixel_base + (int64_t)y * W + x;
       const float gr = grad_out[3 * p], gg = grad_out[3 * p + 1], gb = grad_out[3 * p + 2];
       v = make_float4(gr, gg, gb, 0.f);
       if (normalize) {
@@ -282,7 +345,7 @@ __global__ void __launch_bounds__(Tiling<TS>::kBwdThreads, TS == 16 ? 4 : 2)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int my_moment = moment_of_lane(lane);
   const int col_slot = lane & 7, row_seg = lane >> 3;
-  const TileList L = tile_list(gids, offsets, cap, n, tile);
+  const TileList L = tile_list(gids, offsets, cap, fr, tile);
   if (DETERMINISTIC && L.direct) {
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
     return;
@@ -407,40 +470,20 @@ __global__ void finalize_moments_kernel(const Splat* __restrict__ rec, int64_t n
   write_gradients(rec, g, m, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
-// Deterministic second pass: Gaussian g sums its per-tile partials over the tiles of its
-// support rectangle in ascending tile order (each located by binary search in the tile's
-// ascending list), then applies the per-Gaussian factors once.
+// Deterministic second pass: per-Gaussian sum of the per-entry partials (sum_partials), then
+// the per-Gaussian factors.
 __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
                                        const int32_t* __restrict__ gids, int64_t cap,
-                                       const int32_t* __restrict__ offsets, int tiles_x, int ts,
-                                       const float* __restrict__ partials, int has_opacity,
-                                       float* __restrict__ g_means, float* __restrict__ g_conics,
+                                       const int32_t* __restrict__ offsets, Frames frames,
+                                       int ts, const float* __restrict__ partials,
+                                       int has_opacity, float* __restrict__ g_means,
+                                       float* __restrict__ g_conics,
                                        float* __restrict__ g_colors,
                                        float* __restrict__ g_opac) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
-  const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
-  float acc[kMoments] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (r.z > r.x && r.w > r.y) {
-    const int gx0 = r.x / ts, gx1 = (r.z - 1) / ts, gy0 = r.y / ts, gy1 = (r.w - 1) / ts;
-    for (int gy = gy0; gy <= gy1; ++gy) {
-      for (int gx = gx0; gx <= gx1; ++gx) {
-        const int t = gy * tiles_x + gx;
-        int64_t lo = offsets[t], hi = offsets[t + 1];
-        if (hi > cap) continue;  // truncated list (reported by the backward kernel)
-        const int64_t end = hi;
-        while (lo < hi) {
-          const int64_t mid = (lo + hi) >> 1;
-          if (gids[mid] < g) lo = mid + 1; else hi = mid;
-        }
-        if (lo < end && gids[lo] == g) {
-          const float* pp = partials + lo * kPartialFloats;
-#pragma unroll
-          for (int k = 0; k < kMoments; ++k) acc[k] += pp[k];
-        }
-      }
-    }
-  }
+  float acc[kMoments];
+  sum_partials(rec, g, n, ts, frames, gids, cap, offsets, partials, acc);
   write_gradients(rec, g, acc, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
@@ -454,15 +497,34 @@ int check_render_args(int64_t n, int H, int W, int ts, float eps) {
   return SS_OK;
 }
 
-template <int TS>
-void launch_forward(unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
-                    const int32_t* gids, int64_t cap, const int32_t* offsets, int H, int W,
-                    int tiles_x, bool normalize, float eps, float tail, float* out, float* den) {
+template <int TS, bool NORM, bool FADE>
+void launch_forward_loss(int loss_kind, unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
+                         const int32_t* gids, int64_t cap, const int32_t* offsets,
+                         const Frames& f, float eps, float tail, float* out, float* den,
+                         const float* target, float4* pixel_grad, float* loss, float ce2) {
   constexpr int NT = Tiling<TS>::kFwdThreads;
+#define SS_FWD(LOSS)                                                                          \
+  forward_kernel<TS, NORM, FADE, LOSS><<<T, NT, 0, s>>>(rec, n, gids, cap, offsets, f, eps,   \
+                                                        tail, out, den, target, pixel_grad,   \
+                                                        loss, ce2)
+  switch (loss_kind) {
+    case kL1: SS_FWD(kL1); break;
+    case kL2: SS_FWD(kL2); break;
+    case kCharbonnier: SS_FWD(kCharbonnier); break;
+    default: SS_FWD(kNoLoss); break;
+  }
+#undef SS_FWD
+}
+
+template <int TS>
+void launch_forward(int loss_kind, unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
+                    const int32_t* gids, int64_t cap, const int32_t* offsets, const Frames& f,
+                    bool normalize, float eps, float tail, float* out, float* den,
+                    const float* target, float4* pixel_grad, float* loss, float ce2) {
   const bool fade = tail > 0.0f;
-#define SS_FWD(NORM, FADE)                                                                   \
-  forward_kernel<TS, NORM, FADE><<<T, NT, 0, s>>>(rec, n, gids, cap, offsets, H, W, tiles_x, \
-                                                  eps, tail, out, den)
+#define SS_FWD(NORM, FADE)                                                                     \
+  launch_forward_loss<TS, NORM, FADE>(loss_kind, T, s, rec, n, gids, cap, offsets, f, eps,     \
+                                      tail, out, den, target, pixel_grad, loss, ce2)
   if (normalize) {
     if (fade) SS_FWD(true, true); else SS_FWD(true, false);
   } else {
@@ -471,24 +533,128 @@ void launch_forward(unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
 #undef SS_FWD
 }
 
-template <int TS>
+template <int TS, bool PIXGRAD>
 void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float* grad_out,
                      const Splat* rec, int64_t n, const float* den, const float* out,
-                     const int32_t* gids, int64_t cap, const int32_t* offsets, int H, int W,
-                     int tiles_x, int normalize, float eps, float tail, float* ws,
-                     uint32_t* status) {
+                     const float4* pixel_grad, const int32_t* gids, int64_t cap,
+                     const int32_t* offsets, const Frames& f, int normalize, float eps,
+                     float tail, float* ws, uint32_t* status) {
   constexpr int NT = Tiling<TS>::kBwdThreads;
   const bool fade = tail > 0.0f;
-#define SS_BWD(FADE, DET)                                                                      \
-  backward_kernel<TS, FADE, DET><<<T, NT, 0, s>>>(grad_out, rec, n, den, out, gids, cap,      \
-                                                  offsets, H, W, tiles_x, normalize, eps, tail, \
-                                                  ws, ws, status)
+#define SS_BWD(FADE, DET)                                                                     \
+  backward_kernel<TS, FADE, DET, PIXGRAD><<<T, NT, 0, s>>>(grad_out, rec, n, den, out,       \
+                                                           pixel_grad, gids, cap, offsets, f, \
+                                                           normalize, eps, tail, ws, ws, status)
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
     if (fade) SS_BWD(true, false); else SS_BWD(false, false);
   }
 #undef SS_BWD
+}
+
+// Forward over any tile set; loss_kind selects the plain render or a fit forward.
+int render_forward(const Frames& f, int ts, int64_t T, const void* records, int64_t n,
+                   const int32_t* gids, int64_t cap, const int32_t* offsets, int normalize,
+                   float eps, float tail, int loss_kind, const float* target, float ce2,
+                   float* pixel_grad, float* out, float* den, float* loss, cudaStream_t s) {
+  if (T == 0) return SS_OK;
+  if (!offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null tile offsets");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  if (T > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "too many tiles");
+  const Splat* rec = static_cast<const Splat*>(records);
+  float4* pg = reinterpret_cast<float4*>(pixel_grad);
+  if (ts == 16)
+    launch_forward<16>(loss_kind, (unsigned)T, s, rec, n, gids, cap, offsets, f, normalize, eps,
+                       tail, out, den, target, pg, loss, ce2);
+  else
+    launch_forward<32>(loss_kind, (unsigned)T, s, rec, n, gids, cap, offsets, f, normalize, eps,
+                       tail, out, den, target, pg, loss, ce2);
+  return check_launch("render_forward");
+}
+
+// Backward kernel (no epilogue) over any tile set.
+int render_backward_tiles(const Frames& f, int ts, int64_t T, const float* grad_out,
+                          const void* records, int64_t n, const float* den, const float* out,
+                          const float* pixel_grad, const int32_t* gids, int64_t cap,
+                          const int32_t* offsets, int normalize, float eps, float tail,
+                          int deterministic, float* ws, uint32_t* status, cudaStream_t s) {
+  if (T == 0 || n == 0) return SS_OK;
+  if (T > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "too many tiles");
+  const Splat* rec = static_cast<const Splat*>(records);
+  const float4* pg = reinterpret_cast<const float4*>(pixel_grad);
+  if (pixel_grad) {
+    if (ts == 16)
+      launch_backward<16, true>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, pg,
+                                gids, cap, offsets, f, normalize, eps, tail, ws, status);
+    else
+      launch_backward<32, true>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, pg,
+                                gids, cap, offsets, f, normalize, eps, tail, ws, status);
+  } else {
+    if (ts == 16)
+      launch_backward<16, false>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, pg,
+                                 gids, cap, offsets, f, normalize, eps, tail, ws, status);
+    else
+      launch_backward<32, false>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, pg,
+                                 gids, cap, offsets, f, normalize, eps, tail, ws, status);
+  }
+  return check_launch("render_backward");
+}
+
+size_t backward_ws_bytes(int64_t n, int64_t cap, int deterministic) {
+  return deterministic ? (size_t)cap * kPartialFloats * sizeof(float)
+                       : (size_t)n * kMoments * sizeof(float);
+}
+
+// Plain backward over any tile set: moments / partials, then the per-Gaussian epilogue.
+int render_backward(const Frames& f, int ts, int64_t T, int64_t npx, const float* grad_out,
+                    const void* records, int64_t n, const float* den, const float* out,
+                    const int32_t* gids, int64_t cap, const int32_t* offsets, int normalize,
+                    float eps, float tail, int has_opacity, float* grad_means,
+                    float* grad_conics, float* grad_colors, float* grad_opacities,
+                    int deterministic, void* workspace, size_t workspace_bytes,
+                    uint32_t* status, cudaStream_t s) {
+  if (n == 0) return SS_OK;
+  if (!grad_means || !grad_conics || !grad_colors || (has_opacity && !grad_opacities))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null gradient output");
+  if (npx == 0) {  // nothing is rendered: every gradient is zero
+    cudaMemsetAsync(grad_means, 0, sizeof(float) * 2 * n, s);
+    cudaMemsetAsync(grad_conics, 0, sizeof(float) * 3 * n, s);
+    cudaMemsetAsync(grad_colors, 0, sizeof(float) * 3 * n, s);
+    if (has_opacity) cudaMemsetAsync(grad_opacities, 0, sizeof(float) * n, s);
+    return check_launch("backward zero-fill");
+  }
+  if (!grad_out || !records || !den || !out || !offsets)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const size_t need = backward_ws_bytes(n, cap, deterministic);
+  if (workspace_bytes < need || !workspace)
+    return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+                workspace_bytes, need);
+  float* ws = static_cast<float*>(workspace);
+  int rc;
+  if (!deterministic) {
+    if (cudaMemsetAsync(ws, 0, sizeof(float) * kMoments * n, s) != cudaSuccess)
+      return check_launch("backward moment zero-fill");
+  }
+  if ((rc = render_backward_tiles(f, ts, T, grad_out, records, n, den, out, nullptr, gids, cap,
+                                  offsets, normalize, eps, tail, deterministic, ws, status, s)))
+    return rc;
+  const Splat* rec = static_cast<const Splat*>(records);
+  const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
+  if (deterministic)
+    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, gids, cap, offsets, f, ts, ws, has_opacity, grad_means, grad_conics,
+        grad_colors, grad_opacities);
+  else
+    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
+  return check_launch("backward epilogue");
+}
+
+int check_batch_render(const ss_batch* batch, int64_t n, float eps, Frames* f) {
+  int rc = frames_of_batch(batch, n, f);
+  if (rc) return rc;
+  return check_render_args(n, 0, 0, batch->tile_size, eps);
 }
 
 }  // namespace
@@ -505,21 +671,29 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
   int rc = check_render_args(n, height, width, tile_size, eps);
   if (rc) return rc;
   (void)status;
-  const int64_t npx = (int64_t)height * width;
-  if (npx == 0) return SS_OK;
-  if (!out || !den || !tile_offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
-  const int tiles_x = (width + tile_size - 1) / tile_size;
-  const int64_t T = (int64_t)tiles_x * ((height + tile_size - 1) / tile_size);
-  const Splat* rec = static_cast<const Splat*>(records);
-  cudaStream_t s = as_stream(stream);
-  if (tile_size == 16)
-    launch_forward<16>((unsigned)T, s, rec, n, tile_gids, gid_capacity, tile_offsets, height,
-                       width, tiles_x, normalize, eps, fade_tail, out, den);
-  else
-    launch_forward<32>((unsigned)T, s, rec, n, tile_gids, gid_capacity, tile_offsets, height,
-                       width, tiles_x, normalize, eps, fade_tail, out, den);
-  return check_launch("render_forward");
+  if ((int64_t)height * width == 0) return SS_OK;
+  if (!out || !den) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const int64_t T = (int64_t)((width + tile_size - 1) / tile_size) *
+                    ((height + tile_size - 1) / tile_size);
+  return render_forward(single_frame(height, width, tile_size), tile_size, T, records, n,
+                        tile_gids, gid_capacity, tile_offsets, normalize, eps, fade_tail,
+                        kNoLoss, nullptr, 0.f, nullptr, out, den, nullptr, as_stream(stream));
+}
+
+int ss_batch_render_forward(const ss_batch* batch, const void* records, int64_t n,
+                            const int32_t* tile_gids, int64_t gid_capacity,
+                            const int32_t* tile_offsets, int normalize, float eps,
+                            float fade_tail, float* out, float* den, uint32_t* status,
+                            ss_stream_t stream) {
+  Frames f;
+  int rc = check_batch_render(batch, n, eps, &f);
+  if (rc) return rc;
+  (void)status;
+  if (batch->pixels == 0) return SS_OK;
+  if (!out || !den) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  return render_forward(f, batch->tile_size, batch->tiles, records, n, tile_gids, gid_capacity,
+                        tile_offsets, normalize, eps, fade_tail, kNoLoss, nullptr, 0.f, nullptr,
+                        out, den, nullptr, as_stream(stream));
 }
 
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,
@@ -527,8 +701,7 @@ int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int heig
   if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
   if (n < 0 || gid_capacity < 0 || height < 0 || width < 0)
     return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
-  *bytes = deterministic ? (size_t)gid_capacity * kPartialFloats * sizeof(float)
-                         : (size_t)n * kMoments * sizeof(float);
+  *bytes = backward_ws_bytes(n, gid_capacity, deterministic);
   return SS_OK;
 }
 
@@ -541,51 +714,82 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
                        size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
   int rc = check_render_args(n, height, width, tile_size, eps);
   if (rc) return rc;
-  if (n == 0) return SS_OK;
-  if (!grad_means || !grad_conics || !grad_colors || (has_opacity && !grad_opacities))
-    return fail(SS_ERR_INVALID_ARGUMENT, "null gradient output");
-  cudaStream_t s = as_stream(stream);
-  const int64_t npx = (int64_t)height * width;
-  if (npx == 0) {  // nothing is rendered: every gradient is zero
-    cudaMemsetAsync(grad_means, 0, sizeof(float) * 2 * n, s);
-    cudaMemsetAsync(grad_conics, 0, sizeof(float) * 3 * n, s);
-    cudaMemsetAsync(grad_colors, 0, sizeof(float) * 3 * n, s);
-    if (has_opacity) cudaMemsetAsync(grad_opacities, 0, sizeof(float) * n, s);
-    return check_launch("backward zero-fill");
-  }
-  if (!grad_out || !records || !den || !out || !tile_offsets)
-    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  size_t need = 0;
-  ss_render_backward_workspace_bytes(n, gid_capacity, height, width, deterministic, &need);
+  const int64_t T = (int64_t)((width + tile_size - 1) / tile_size) *
+                    ((height + tile_size - 1) / tile_size);
+  return render_backward(single_frame(height, width, tile_size), tile_size, T,
+                         (int64_t)height * width, grad_out, records, n, den, out, tile_gids,
+                         gid_capacity, tile_offsets, normalize, eps, fade_tail, has_opacity,
+                         grad_means, grad_conics, grad_colors, grad_opacities, deterministic,
+                         workspace, workspace_bytes, status, as_stream(stream));
+}
+
+int ss_batch_render_backward(const ss_batch* batch, const float* grad_out, const void* records,
+                             int64_t n, const float* den, const float* out,
+                             const int32_t* tile_gids, int64_t gid_capacity,
+                             const int32_t* tile_offsets, int normalize, float eps,
+                             float fade_tail, int has_opacity, float* grad_means,
+                             float* grad_conics, float* grad_colors, float* grad_opacities,
+                             int deterministic, void* workspace, size_t workspace_bytes,
+                             uint32_t* status, ss_stream_t stream) {
+  Frames f;
+  int rc = check_batch_render(batch, n, eps, &f);
+  if (rc) return rc;
+  return render_backward(f, batch->tile_size, batch->tiles, batch->pixels, grad_out, records, n,
+                         den, out, tile_gids, gid_capacity, tile_offsets, normalize, eps,
+                         fade_tail, has_opacity, grad_means, grad_conics, grad_colors,
+                         grad_opacities, deterministic, workspace, workspace_bytes, status,
+                         as_stream(stream));
+}
+
+int ss_fit_forward_loss(const ss_batch* batch, const void* records, int64_t n,
+                        const int32_t* tile_gids, int64_t gid_capacity,
+                        const int32_t* tile_offsets, int normalize, float eps, float fade_tail,
+                        const float* target, int loss_kind, float charbonnier_eps,
+                        float* pixel_grad, float* image, float* den, float* loss,
+                        uint32_t* status, ss_stream_t stream) {
+  Frames f;
+  int rc = check_batch_render(batch, n, eps, &f);
+  if (rc) return rc;
+  (void)status;
+  if (loss_kind < 0 || loss_kind > 2)
+    return fail(SS_ERR_INVALID_ARGUMENT, "loss_kind must be 0 (l1), 1 (l2) or 2 (charbonnier)");
+  if (batch->pixels == 0) return SS_OK;
+  if (!target || !pixel_grad) return fail(SS_ERR_INVALID_ARGUMENT, "null target or pixel_grad");
+  if (reinterpret_cast<uintptr_t>(pixel_grad) % 16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "pixel_grad must be 16-byte aligned");
+  const int kinds[3] = {kL1, kL2, kCharbonnier};
+  const float ce2 = (float)((double)charbonnier_eps * (double)charbonnier_eps);
+  return render_forward(f, batch->tile_size, batch->tiles, records, n, tile_gids, gid_capacity,
+                        tile_offsets, normalize, eps, fade_tail, kinds[loss_kind], target, ce2,
+                        pixel_grad, image, den, loss, as_stream(stream));
+}
+
+int ss_fit_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
+                                    size_t* bytes) {
+  if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
+  if (n < 0 || gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  *bytes = backward_ws_bytes(n, gid_capacity, deterministic);
+  return SS_OK;
+}
+
+int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
+                    const int32_t* tile_gids, int64_t gid_capacity, const int32_t* tile_offsets,
+                    float fade_tail, const float* pixel_grad, int deterministic,
+                    void* workspace, size_t workspace_bytes, uint32_t* status,
+                    ss_stream_t stream) {
+  Frames f;
+  int rc = check_batch_render(batch, n, 1.0f, &f);
+  if (rc) return rc;
+  if (n == 0 || batch->pixels == 0) return SS_OK;
+  if (!records || !tile_offsets || !pixel_grad) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
   if (workspace_bytes < need || !workspace)
-    return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+    return fail(SS_ERR_INVALID_ARGUMENT, "fit backward workspace too small (%zu < %zu)",
                 workspace_bytes, need);
-  const int tiles_x = (width + tile_size - 1) / tile_size;
-  const int64_t T = (int64_t)tiles_x * ((height + tile_size - 1) / tile_size);
-  const Splat* rec = static_cast<const Splat*>(records);
-  float* ws = static_cast<float*>(workspace);
-  if (!deterministic) {
-    if (cudaMemsetAsync(ws, 0, sizeof(float) * kMoments * n, s) != cudaSuccess)
-      return check_launch("backward moment zero-fill");
-  }
-  if (tile_size == 16)
-    launch_backward<16>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, tile_gids,
-                        gid_capacity, tile_offsets, height, width, tiles_x, normalize, eps,
-                        fade_tail, ws, status);
-  else
-    launch_backward<32>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, tile_gids,
-                        gid_capacity, tile_offsets, height, width, tiles_x, normalize, eps,
-                        fade_tail, ws, status);
-  if ((rc = check_launch("render_backward"))) return rc;
-  const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
-  if (deterministic)
-    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, tile_gids, gid_capacity, tile_offsets, tiles_x, tile_size, ws, has_opacity,
-        grad_means, grad_conics, grad_colors, grad_opacities);
-  else
-    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
-  return check_launch("backward epilogue");
+  return render_backward_tiles(f, batch->tile_size, batch->tiles, nullptr, records, n, nullptr,
+                               nullptr, pixel_grad, tile_gids, gid_capacity, tile_offsets, 1,
+                               1.0f, fade_tail, deterministic, static_cast<float*>(workspace),
+                               status, as_stream(stream));
 }
 
 }  // extern "C"

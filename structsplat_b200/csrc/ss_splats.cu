@@ -23,6 +23,27 @@ int check_launch(const char* what) {
   return SS_OK;
 }
 
+int frames_of_batch(const ss_batch* batch, int64_t n, Frames* out) {
+  if (!batch) return fail(SS_ERR_INVALID_ARGUMENT, "null batch");
+  if (batch->images < 1) return fail(SS_ERR_INVALID_ARGUMENT, "batch needs at least one image");
+  if (batch->tile_size <= 0 || batch->tile_size * batch->tile_size > 1024)
+    return fail(SS_ERR_INVALID_ARGUMENT, "batch tile_size must be positive with ts^2 <= 1024");
+  if (batch->tiles < 0 || batch->tiles + 1 > (int64_t)INT32_MAX || batch->pixels < 0)
+    return fail(SS_ERR_INVALID_ARGUMENT, "batch tile or pixel total out of range");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "bad Gaussian count");
+  if (!batch->image_table || !batch->pixel_base || !batch->gaussian_base ||
+      (n > 0 && !batch->gaussian_image) || (batch->tiles > 0 && !batch->tile_image))
+    return fail(SS_ERR_INVALID_ARGUMENT, "batch table pointer is null");
+  Frames f{};
+  f.image = reinterpret_cast<const int4*>(batch->image_table);
+  f.pixel_base = reinterpret_cast<const long long*>(batch->pixel_base);
+  f.gauss_base = batch->gaussian_base;
+  f.gauss_image = batch->gaussian_image;
+  f.tile_image = batch->tile_image;
+  *out = f;
+  return SS_OK;
+}
+
 namespace {
 
 constexpr int kThreads = 256;
@@ -54,7 +75,7 @@ __global__ void project_rs_kernel(const float* __restrict__ means,
                                   const float* __restrict__ rotations,
                                   const float* __restrict__ colors,
                                   const float* __restrict__ logits, int64_t n, float dilation,
-                                  float cutoff, int H, int W, Splat* __restrict__ out,
+                                  float cutoff, Frames frames, Splat* __restrict__ out,
                                   float* __restrict__ conics_out,
                                   int64_t* __restrict__ radii_out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -81,7 +102,8 @@ __global__ void project_rs_kernel(const float* __restrict__ means,
   float op = logits ? 1.0f / (1.0f + expf(-logits[i])) : 1.0f;
   float mx = means[2 * i], my = means[2 * i + 1];
   int x0, y0, x1, y1;
-  support_rect(mx, my, rx, ry, H, W, x0, y0, x1, y1);
+  const Frame fr = frame_of_gaussian(frames, i, n);
+  support_rect(mx, my, rx, ry, fr.H, fr.W, x0, y0, x1, y1);
   store_splat(out + i, make_splat(mx, my, a, b, c, op, colors[3 * i], colors[3 * i + 1],
                                   colors[3 * i + 2], x0, y0, x1, y1));
   if (conics_out) {
@@ -110,22 +132,10 @@ __global__ void project_rs_backward_kernel(const float* __restrict__ log_scales,
                                            float* __restrict__ g_logits) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float sx = expf(log_scales[2 * i]), sy = expf(log_scales[2 * i + 1]);
-  float sx2 = sx * sx, sy2 = sy * sy;
-  float u = 1.0f / (sx2 + dilation), v = 1.0f / (sy2 + dilation);
-  float cs, sn;
-  sincosf(rotations[i], &sn, &cs);
-  float ga = g_conics[3 * i], gb = g_conics[3 * i + 1], gc = g_conics[3 * i + 2];
-  float cc = cs * cs, s2 = sn * sn, csn = cs * sn;
-  float gu = ga * cc + gb * csn + gc * s2;
-  float gv = ga * s2 - gb * csn + gc * cc;
-  g_log_scales[2 * i] = gu * (-2.0f * sx2 * u * u);
-  g_log_scales[2 * i + 1] = gv * (-2.0f * sy2 * v * v);
-  g_rot[i] = (u - v) * (2.0f * csn * (gc - ga) + (cc - s2) * gb);
-  if (logits && g_opac && g_logits) {
-    float o = 1.0f / (1.0f + expf(-logits[i]));
-    g_logits[i] = g_opac[i] * o * (1.0f - o);
-  }
+  rs_conic_chain(log_scales[2 * i], log_scales[2 * i + 1], rotations[i], dilation,
+                 g_conics[3 * i], g_conics[3 * i + 1], g_conics[3 * i + 2], g_log_scales[2 * i],
+                 g_log_scales[2 * i + 1], g_rot[i]);
+  if (logits && g_opac && g_logits) g_logits[i] = logit_chain(logits[i], g_opac[i]);
 }
 
 }  // namespace
@@ -157,11 +167,10 @@ int ss_pack_splats(const float* means, const float* conics, const float* colors,
   return check_launch("pack_splats");
 }
 
-int ss_project_rs(const float* means, const float* log_scales, const float* rotations,
-                  const float* colors, const float* opacity_logits, int64_t n, float dilation,
-                  float sigma_cutoff, int height, int width, void* records, float* conics_out,
-                  int64_t* radii_out, ss_stream_t stream) {
-  if (n < 0 || height < 0 || width < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+static int project_rs(const Frames& frames, const float* means, const float* log_scales,
+                      const float* rotations, const float* colors, const float* opacity_logits,
+                      int64_t n, float dilation, float sigma_cutoff, void* records,
+                      float* conics_out, int64_t* radii_out, ss_stream_t stream) {
   if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
   if (!(dilation >= 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "dilation must be >= 0");
   if (n == 0) return SS_OK;
@@ -170,9 +179,30 @@ int ss_project_rs(const float* means, const float* log_scales, const float* rota
   if (reinterpret_cast<uintptr_t>(records) % 16)
     return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
   project_rs_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
-      means, log_scales, rotations, colors, opacity_logits, n, dilation, sigma_cutoff, height,
-      width, reinterpret_cast<Splat*>(records), conics_out, radii_out);
+      means, log_scales, rotations, colors, opacity_logits, n, dilation, sigma_cutoff, frames,
+      reinterpret_cast<Splat*>(records), conics_out, radii_out);
   return check_launch("project_rs");
+}
+
+int ss_project_rs(const float* means, const float* log_scales, const float* rotations,
+                  const float* colors, const float* opacity_logits, int64_t n, float dilation,
+                  float sigma_cutoff, int height, int width, void* records, float* conics_out,
+                  int64_t* radii_out, ss_stream_t stream) {
+  if (n < 0 || height < 0 || width < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
+  return project_rs(single_frame(height, width, 1), means, log_scales, rotations, colors,
+                    opacity_logits, n, dilation, sigma_cutoff, records, conics_out, radii_out,
+                    stream);
+}
+
+int ss_batch_project_rs(const ss_batch* batch, const float* means, const float* log_scales,
+                        const float* rotations, const float* colors,
+                        const float* opacity_logits, int64_t n, float dilation,
+                        float sigma_cutoff, void* records, ss_stream_t stream) {
+  Frames f;
+  int rc = frames_of_batch(batch, n, &f);
+  if (rc) return rc;
+  return project_rs(f, means, log_scales, rotations, colors, opacity_logits, n, dilation,
+                    sigma_cutoff, records, nullptr, nullptr, stream);
 }
 
 int ss_project_rs_backward(const float* log_scales, const float* rotations,

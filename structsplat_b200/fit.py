@@ -9,7 +9,8 @@ capacity still renders exactly (truncated tiles scan every Gaussian) and raises
 to re-plan with a larger capacity.
 
 ``fit`` runs the reference's plain fitting iteration (render → pixel MSE → backward → Adam,
-``fit.py:3182-3351`` of the reference) with the whole iteration captured in one CUDA graph.
+``fit.py:3182-3351`` of the reference) through the batched fit path with one image, the whole
+iteration captured in one CUDA graph.
 """
 from __future__ import annotations
 
@@ -175,69 +176,24 @@ class CapturedStep:
 
 def fit(params: dict, target: torch.Tensor, iters: int = 100, lr: float = 1e-2,
         normalize: bool = True, sigma_cutoff: float = 3.0, log_every: int = 0,
-        graph: bool = True, capacity_headroom: float = 1.5):
-    """Adam fit of an RS field to ``target`` (H,W,3) with the pixel MSE loss.
+        graph: bool = True, settings=None, check_every: int = 50):
+    """Adam fit of one RS field to ``target`` (H,W,3): the reference's plain fit iteration.
 
-    ``params`` maps the five field names to CUDA float32 tensors (updated in place).  Returns a
-    history dict with the PSNR at every ``log_every`` iterations (and at the end).  With
-    ``graph=True`` one CUDA graph holds render, loss gradient, backward and the Adam update.
+    ``params`` maps the five field names to CUDA float32 tensors (updated in place).  With no
+    ``settings`` every parameter group uses learning rate ``lr`` and the loss is the pixel MSE.
+    Returns a history dict: the PSNR of the pre-update render at every ``log_every`` iterations
+    and ``final_psnr`` after the last update.  With ``graph=True`` one CUDA graph holds the
+    whole iteration (index build, render + loss, backward, fused Adam update).
     """
-    H, W, _ = target.shape
-    names = [k for k in PARAM_NAMES if params.get(k) is not None]
-    plan = RenderPlan.for_field(params, H, W, headroom=capacity_headroom, normalize=normalize,
-                                sigma_cutoff=sigma_cutoff)
-    grads = plan.grads()
-    tensors = [params[k] for k in names]
-    state = [(torch.zeros_like(t), torch.zeros_like(t)) for t in tensors]
-    step_t = torch.zeros(1, device=target.device, dtype=torch.float32)
-    grad_out = torch.empty_like(target)
-    scale = 2.0 / target.numel()
-    b1, b2, eps_adam = 0.9, 0.999, 1e-8
-
-    def iteration():
-        plan.forward(params)
-        torch.sub(plan.image, target, out=grad_out)
-        grad_out.mul_(scale)
-        plan.backward(grad_out, params)
-        step_t.add_(1.0)
-        bc1 = 1.0 - torch.pow(b1, step_t)
-        bc2 = 1.0 - torch.pow(b2, step_t)
-        for t, (m, v), k in zip(tensors, state, names):
-            g = grads[k]
-            m.mul_(b1).add_(g, alpha=1.0 - b1)
-            v.mul_(b2).addcmul_(g, g, value=1.0 - b2)
-            denom = (v / bc2).sqrt_().add_(eps_adam)
-            t.sub_(lr * (m / bc1) / denom)
-
-    history = {"iter": [], "psnr": []}
-
-    def log(it):
-        mse = torch.mean((plan.image - target) ** 2).item()
-        history["iter"].append(it)
-        history["psnr"].append(10.0 * math.log10(1.0 / max(mse, 1e-20)))
-
-    if graph:
-        # warm up (every lazily initialised resource must exist before capture), capture, then
-        # restore the field and the optimizer state the warm-up iterations advanced
-        snapshot = [t.detach().clone() for t in tensors]
-        iteration()
-        cap = CapturedStep(iteration, warmup=1)
-        with torch.no_grad():
-            for t, s in zip(tensors, snapshot):
-                t.copy_(s)
-        step_t.zero_()
-        for (m, v) in state:
-            m.zero_()
-            v.zero_()
-        run = cap.replay
-    else:
-        run = iteration
-    for it in range(1, iters + 1):
-        run()
-        if log_every and it % log_every == 0:
-            log(it)
-    if not history["iter"] or history["iter"][-1] != iters:
-        plan.forward(params)
-        log(iters)
-    history["overflowed"] = plan.overflowed()
-    return history
+    from .batch import FitSettings, fit_batch
+    if settings is None:
+        settings = FitSettings.uniform_lr(lr, normalize=normalize, sigma_cutoff=sigma_cutoff)
+    h = fit_batch([params], [target], iters=iters, settings=settings, graph=graph,
+                  log_every=log_every, check_every=check_every)
+    out = {"iter": list(h["iter"]), "psnr": [p[0] for p in h["psnr"]],
+           "final_psnr": h["final_psnr"][0], "replans": h["replans"],
+           "overflowed": h["plan"].overflowed()}
+    if not out["iter"] or out["iter"][-1] != iters:
+        out["iter"].append(iters)
+        out["psnr"].append(out["final_psnr"])
+    return out

@@ -92,3 +92,41 @@ def test_empty_problem_needs_no_device(lib):
     rc, _ = _status(lib, "ss_render_forward", None, 0, None, 0, None, 0, 7, 16, 1,
                     ctypes.c_float(1e-8), ctypes.c_float(0.0), None, None, None, None)
     assert rc == 0
+
+
+def test_batch_validation_without_gpu(lib):
+    size = ctypes.c_size_t(0)
+    rc, msg = _status(lib, "ss_batch_tile_index_workspace_bytes", None, 10, ctypes.byref(size))
+    assert rc == 1 and "null batch" in msg
+    b = _native.SsBatch(images=0, tile_size=16, tiles=0, pixels=0)
+    rc, msg = _status(lib, "ss_batch_tile_index_workspace_bytes", ctypes.byref(b), 10,
+                      ctypes.byref(size))
+    assert rc == 1 and "at least one image" in msg
+    b = _native.SsBatch(images=1, tile_size=16, tiles=4, pixels=16)
+    rc, msg = _status(lib, "ss_batch_tile_index_workspace_bytes", ctypes.byref(b), 10,
+                      ctypes.byref(size))
+    assert rc == 1 and "table pointer" in msg
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the size query reads no table
+    b = _native.SsBatch(images=1, tile_size=16, tiles=4, pixels=16, image_table=dummy,
+                        pixel_base=dummy, gaussian_base=dummy, gaussian_image=dummy,
+                        tile_image=dummy)
+    rc, _ = _status(lib, "ss_batch_tile_index_workspace_bytes", ctypes.byref(b), 10,
+                    ctypes.byref(size))
+    assert rc == 0 and size.value > 0
+    b.tile_size = 8
+    rc, msg = _status(lib, "ss_batch_render_forward", ctypes.byref(b), None, 0, None, 0, None, 1,
+                      ctypes.c_float(1e-8), ctypes.c_float(0.0), None, None, None, None)
+    assert rc == 4 and "tile_size" in msg
+    b.tile_size = 32
+    rc, msg = _status(lib, "ss_fit_forward_loss", ctypes.byref(b), None, 0, None, 0, None, 1,
+                      ctypes.c_float(1e-8), ctypes.c_float(0.0), None, 7, ctypes.c_float(1e-3),
+                      None, None, None, None, None, None)
+    assert rc == 1 and "loss_kind" in msg
+    rc, msg = _status(lib, "ss_fit_backward_workspace_bytes", 10, 100, 1, ctypes.byref(size))
+    assert rc == 0 and size.value == 100 * 48
+    lrs = (ctypes.c_double * 5)(*([1e-2] * 5))
+    ptrs = (ctypes.c_void_p * 5)()
+    rc, msg = _status(lib, "ss_fit_adam_update", ctypes.byref(b), None, 10, None, 0, None, 0,
+                      None, ctypes.c_float(0.0), ptrs, ptrs, ptrs, lrs, 0.9, 0.999, 1e-8,
+                      ctypes.c_float(-1.0), None, None, None)
+    assert rc == 1 and "null" in msg
