@@ -319,6 +319,168 @@ def ref_cuda_baseline(host, dev, steps=10):
     return res
 
 
+BATCH_SIZES = [(256, 256), (512, 512), (512, 768), (1024, 1024), (1536, 2048)]  # (H, W)
+BATCH_IMAGES, BATCH_DENSITY, BATCH_SEED = 64, 0.1, 7
+
+
+def _batch_target(args):
+    from structsplat_b200.synthetic import make_target
+    H, W, seed = args
+    return make_target(H, W, seed=seed)
+
+
+def batched_workload(images=BATCH_IMAGES, seed=BATCH_SEED):
+    """The batched-fit workload: image sizes drawn uniformly from BATCH_SIZES, 0.1 Gaussians per
+    pixel, seeded targets and fields (targets built in a spawn pool: no fork after CUDA init)."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from structsplat_b200.synthetic import make_field
+    rng = np.random.default_rng(seed)
+    sizes = [BATCH_SIZES[int(k)] for k in rng.integers(0, len(BATCH_SIZES), images)]
+    counts = [int(round(BATCH_DENSITY * h * w)) for h, w in sizes]
+    jobs = [(h, w, seed * 1000 + 2 * b) for b, (h, w) in enumerate(sizes)]
+    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
+                             mp_context=mp.get_context("spawn")) as pool:
+        targets = list(pool.map(_batch_target, jobs))
+    fields = [make_field(h, w, n, seed=seed * 1000 + 2 * b + 1)
+              for b, ((h, w), n) in enumerate(zip(sizes, counts))]
+    return sizes, counts, targets, fields
+
+
+def run_batched(args, dev, workload):
+    """C4: one batched graph-captured fit step for all images vs looping the per-image step."""
+    from structsplat_b200 import _native
+    from structsplat_b200.batch import Batch, FitPlan, FitSettings, GraphStep, psnr_from_mse
+    names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
+    sizes, counts, targets_np, fields_np = workload
+    B = len(sizes)
+    targets = [torch.tensor(t, device=dev) for t in targets_np]
+
+    def fresh():
+        return [{k: torch.tensor(getattr(f, k), device=dev) for k in names} for f in fields_np]
+
+    settings = FitSettings()
+    K, Wm = args.batch_steps, args.warmup
+
+    def timed(fn, iters):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(iters):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e)
+
+    # batched: one plan for every image, one graph per step
+    batch = Batch(sizes, counts, device=dev)
+    fb = fresh()
+    plan = FitPlan(batch, Batch.concat_fields(fb), batch.concat_images(targets), settings)
+    step = GraphStep(plan)
+    _native.CALLS.clear()
+    for _ in range(Wm):
+        step.replay()
+    with ClockSampler(dev.index) as clocks:
+        t_batch = timed(step.replay, K)
+    overflow = plan.overflowed()
+    _, loss_b = plan.render()
+    psnr_b = [psnr_from_mse(m) for m in loss_b[:, 1].tolist()]
+    entries = int(plan.offsets[-1].item())
+    mem_gb = torch.cuda.max_memory_allocated(dev) / 1e9
+    del step, plan
+
+    # per-image loop of the same step (eager launches), the plain per-image kernel
+    fl = fresh()
+    plans = []
+    for b in range(B):
+        bb = Batch([sizes[b]], [counts[b]], device=dev)
+        plans.append(FitPlan(bb, fl[b], targets[b].reshape(-1, 3), settings))
+
+    def loop_step():
+        for p in plans:
+            p.step()
+    for _ in range(Wm):
+        loop_step()
+    t_loop = timed(loop_step, K)
+    psnr_l = []
+    for p in plans:
+        _, loss = p.render()
+        psnr_l.append(psnr_from_mse(float(loss[0, 1])))
+    # per-image loop with every image's step captured in its own graph
+    graphs = [GraphStep(p) for p in plans]
+    t_loop_graph = timed(lambda: [g.replay() for g in graphs], K)
+    del graphs, plans
+
+    res = {
+        "workload": f"{B} images, sizes uniform over {{256x256, 512x512, 768x512, 1024x1024, "
+                    f"2048x1536}} (WxH), 0.1 Gaussians/px, seeded generator targets; "
+                    f"normalized, pixel MSE, Adam (reference per-group lrs)",
+        "images": B, "pixels": int(batch.pixels), "gaussians": int(batch.n),
+        "tile_entries": entries, "steps": K, "warmup": Wm,
+        "batched_img_s": round(B * K / (t_batch * 1e-3), 1),
+        "batched_ms_per_step": round(t_batch / K, 3),
+        "loop_eager_img_s": round(B * K / (t_loop * 1e-3), 1),
+        "loop_graph_img_s": round(B * K / (t_loop_graph * 1e-3), 1),
+        "psnr_batched_mean": round(float(np.mean(psnr_b)), 4),
+        "psnr_max_abs_diff_vs_loop": round(float(np.max(np.abs(np.array(psnr_b)
+                                                               - np.array(psnr_l)))), 6),
+        "psnr_after_steps": Wm + K, "index_overflow": overflow,
+        "gpu_launches_per_step": 9, "peak_mem_gb": round(mem_gb, 2), "clocks": clocks.summary(),
+    }
+    res["speedup_vs_loop_eager"] = round(res["batched_img_s"] / res["loop_eager_img_s"], 3)
+    if not args.no_ref_cuda:
+        res["reference_loop"] = ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev,
+                                                  steps=args.ref_batch_steps)
+        if "img_s" in res["reference_loop"]:
+            res["speedup_vs_reference_loop"] = round(
+                res["batched_img_s"] / res["reference_loop"]["img_s"], 2)
+    return res
+
+
+def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2):
+    """The reference's plain fit iteration per image (its CUDA extension, tiled arm, through
+    render_cuda_exact; pixel MSE; torch.optim.Adam over its parameter groups; log-scale clamp),
+    looped over the images; img/s over `steps` timed passes after one warm-up pass."""
+    try:
+        sys.path.insert(0, str(REPO / "baseline"))
+        from build_ref_cuda import load_reference_extension
+        cuda_render = load_reference_extension()
+        from structsplat.gaussians import GaussianField
+    except Exception as exc:
+        return {"unavailable": str(exc)[:200]}
+    names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
+    runs = []
+    for b, f in enumerate(fields_np):
+        g = GaussianField(*[torch.tensor(getattr(f, k), device=dev) for k in names])
+        g.trainable()
+        groups = g.parameter_groups(5e-2, 3e-2, 1e-2, 3e-2, 1e-2)
+        runs.append((g, torch.optim.Adam(groups), targets[b], sizes[b]))
+
+    def one_pass():
+        for g, opt, tgt, (H, W) in runs:
+            img = cuda_render.render_cuda_exact(g.means, g.conics(), g.colors, g.radii(3.0), H, W,
+                                                opacities=g.opacity_values(), tiled=True)
+            d = img - tgt
+            loss = (d * d).mean(dim=2).mean()
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            with torch.no_grad():
+                g.log_scales.clamp_(max=math.log(max(H, W)))
+                g.log_scales.clamp_(min=math.log(0.35))
+    one_pass()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        one_pass()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    return {"img_s": round(len(runs) * steps / (ms * 1e-3), 2), "steps": steps,
+            "ms_per_pass": round(ms / steps, 2), "arm": "cuda_tiled"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -327,6 +489,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-fit measurement")
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--ref-batch-steps", type=int, default=2)
+    ap.add_argument("--batched-only", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only replay the captured step (for ncu launch lists)")
     args = ap.parse_args()
@@ -364,8 +530,14 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(
             seconds=120))
+    workload = None
+    if world == 1 and (args.batched_only or not args.no_batched) and not args.profile:
+        workload = batched_workload()  # spawn pool before the first CUDA call
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
+    if args.batched_only:
+        print(json.dumps({"batched": run_batched(args, dev, workload)}), flush=True)
+        return
     res = run_ours(args, rank, world, dev)
     if res is None:
         return
@@ -416,6 +588,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline(host)
         if world == 1 and not args.no_ref_cuda:
             line["reference_cuda_ms"] = ref_cuda_baseline(host, dev)
+        if workload is not None:
+            line["batched"] = run_batched(args, dev, workload)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
