@@ -238,6 +238,35 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
                        double adam_eps, float log_scale_lo, const float* log_scale_hi,
                        int* step_state, ss_stream_t stream);
 
+/* ---------------------------------------------------------------- placement
+ * Density-weighted placement of a field from the structure tensor (density.py, init.py).
+ * All images are (H,W) row-major; the workspace (ss_placement_workspace_bytes) holds a copy of
+ * the cdf and CUB's temporary storage.
+ *
+ * ss_density_from_energy: density.py:16-29.  energy (H,W) f32 -> density (H,W) f64 pmf;
+ * ref_dev points to the energy reference (a device double, e.g. stats_dev[0] of
+ * ss_structure_tensor). */
+int ss_placement_workspace_bytes(int height, int width, size_t* bytes);
+int ss_density_from_energy(const float* energy, int height, int width, double base,
+                           double power, const double* ref_dev, double* density, void* workspace,
+                           size_t workspace_bytes, ss_stream_t stream);
+/* sample_candidates (density.py:133-153) for given uniforms: uniforms (3n) f64 hold the n draws
+ * of rng.choice followed by the (n,2) jitter block, exactly as the reference's numpy Generator
+ * draws them.  points (n,2) f64 (x, y); pixel_index (n) int64 optional. */
+int ss_sample_candidates(const double* density, int height, int width, const double* uniforms,
+                         int64_t n, double* points, int64_t* pixel_index, void* workspace,
+                         size_t workspace_bytes, ss_stream_t stream);
+/* Field initialisation at the sampled points for the density_random sampler (init.py:626-631,
+ * 778-847 with scale_mode spacing, orientation tensor, colour bilinear, no scale cap, no
+ * opacity): writes means (n,2), log_scales (n,2), rotations (n), colors (n,3) f32.
+ * density_points is the n of _radius_map (the requested Gaussian count). */
+int ss_place_gaussians(const double* points, int64_t n, const double* density,
+                       const float* across_edge_angle, const float* coherence,
+                       const float* image, int height, int width, int anisotropic,
+                       double max_axis_ratio, double coherence_power, double init_scale_mult,
+                       int64_t density_points, float* means, float* log_scales,
+                       float* rotations, float* colors, ss_stream_t stream);
+
 /* ---------------------------------------------------------------- reference-shaped calls
  * One-call equivalents of the reference extension's entry points, taking its tensor
  * contract (render_ext.cpp:89-137).  They pack records into `workspace` (size from

@@ -79,6 +79,11 @@ SIGNATURES = {
                         _vp, _vp],
     "ss_fit_adam_update": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _vp, _f32, _pp, _pp, _pp, _dp,
                            _f64, _f64, _f64, _f32, _vp, _vp, _vp],
+    "ss_placement_workspace_bytes": [_int, _int, _szp],
+    "ss_density_from_energy": [_vp, _int, _int, _f64, _f64, _vp, _vp, _vp, ctypes.c_size_t, _vp],
+    "ss_sample_candidates": [_vp, _int, _int, _vp, _i64, _vp, _vp, _vp, ctypes.c_size_t, _vp],
+    "ss_place_gaussians": [_vp, _i64, _vp, _vp, _vp, _vp, _int, _int, _int, _f64, _f64, _f64,
+                           _i64, _vp, _vp, _vp, _vp, _vp],
     "ss_structure_tensor_workspace_bytes": [_int, _int, _int, _szp],
     "ss_structure_tensor": [_vp, _int, _int, _int, _vp, _int, _vp, _int, _int, _int, _f64, _f64,
                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],

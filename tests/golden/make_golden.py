@@ -128,16 +128,49 @@ def structure_case(ref, name, img, **cfg):
         energy=t.energy, label=t.label, energy_ref=t.energy_ref)
 
 
+def placement_cases(ref, make_target):
+    """density_from_energy, sample_candidates and build_field (density_random) fixtures."""
+    scfg = ref.config.StructureTensorConfig(grad_sigma=1.0, tensor_sigma=2.0)
+    img = make_target(40, 48, seed=12)
+    t = ref.structure_tensor.compute(img, scfg)
+    for k, (base, power) in enumerate(((0.05, 1.0), (0.2, 2.0), (0.0, 0.5), (0.1, 1.7))):
+        d = ref.density.density_from_energy(t.energy, base, power, t.energy_ref)
+        np.savez_compressed(HERE / f"pl_density_{k}.npz", energy=t.energy, ref=t.energy_ref,
+                            base=base, power=power, density=d)
+    d = ref.density.density_from_energy(np.zeros((6, 7), np.float32), 0.0, 1.0, 1.0)
+    np.savez_compressed(HERE / "pl_density_flat.npz", energy=np.zeros((6, 7), np.float32),
+                        ref=1.0, base=0.0, power=1.0, density=d)
+    d = ref.density.density_from_energy(t.energy, 0.05, 1.0, t.energy_ref)
+    for seed, n in ((3, 500), (4, 3000)):
+        pts = ref.density.sample_candidates(d, n, np.random.default_rng(seed))
+        np.savez_compressed(HERE / f"pl_sample_{seed}.npz", density=d, n=n, seed=seed,
+                            points=pts)
+    for strategy, n, seed in (("aniso_onedge", 800, 5), ("iso_blue_noise", 600, 6)):
+        icfg = ref.config.InitConfig(strategy=strategy, sampling_mode="density_random",
+                                     num_gaussians=n, seed=seed)
+        g = ref.init.build_field(img, icfg, scfg)
+        np.savez_compressed(
+            HERE / f"pl_field_{strategy}.npz", img=img, n=n, seed=seed,
+            anisotropic=int(strategy == "aniso_onedge"), energy=t.energy,
+            energy_ref=t.energy_ref, angle=t.across_edge_angle, coherence=t.coherence,
+            density=d, means=g.means.detach().numpy(), log_scales=g.log_scales.detach().numpy(),
+            rotations=g.rotations.detach().numpy(), colors=g.colors.detach().numpy())
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-src", default="/root/reference/src")
+    ap.add_argument("--only", choices=["placement"], default=None,
+                    help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
     sys.path.insert(0, args.reference_src)
     sys.path.insert(0, str(REPO))
     import torch
     import structsplat.config
     import structsplat.cuda_render
+    import structsplat.density
     import structsplat.gaussians
+    import structsplat.init
     import structsplat.render
     import structsplat.structure_tensor
 
@@ -146,11 +179,19 @@ def main() -> None:
     class Ref:
         config = structsplat.config
         cuda_render = structsplat.cuda_render
+        density = structsplat.density
         gaussians = structsplat.gaussians
+        init = structsplat.init
         render = structsplat.render
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "placement":
+        for old in HERE.glob("pl_*.npz"):
+            old.unlink()
+        placement_cases(Ref, make_target)
+        print("wrote", len(list(HERE.glob("pl_*.npz"))), "placement fixtures")
+        return
     for old in HERE.glob("*.npz"):
         old.unlink()
 
@@ -234,6 +275,7 @@ def main() -> None:
     structure_case(Ref, "synthetic_rgb_rho2", tgt, grad_sigma=1.0, tensor_sigma=2.0,
                    color_space="rgb")
     structure_case(Ref, "tiny_5x3", make_target(5, 3, seed=4), grad_sigma=1.0, tensor_sigma=2.0)
+    placement_cases(Ref, make_target)
     print("wrote", len(list(HERE.glob("*.npz"))), "fixtures")
 
 
