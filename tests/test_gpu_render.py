@@ -224,3 +224,28 @@ def test_render_tile_sizes_agree(name):
     assert torch.equal(outs[0][0], outs[1][0])
     for a, b in zip(outs[0][1], outs[1][1]):
         assert rel_err(a, b) <= 1e-5
+
+
+@pytest.mark.parametrize("normalize", [True, False])
+def test_gpu_gradients_on_the_finite_difference_case(normalize):
+    """GPU RS-parameter gradients vs the float64 gradient that tests/test_fd_gradients.py pins
+    to central differences (64x64, 256 Gaussians, step 1e-4)."""
+    require_cuda()
+    from oracle import field_ref, render_ref
+    from structsplat_b200.synthetic import make_field
+    names = ("means", "log_scales", "rotations", "colors", "opacity_logits")
+    f = make_field(64, 64, 256, seed=3)
+    G = np.random.default_rng(5).normal(size=(64, 64, 3))
+    p64 = {k: torch.tensor(getattr(f, k), dtype=torch.float64).requires_grad_(True) for k in names}
+    img64 = render_ref.render(p64["means"], field_ref.conics(p64["log_scales"], p64["rotations"]),
+                              p64["colors"], field_ref.radii(p64["log_scales"], p64["rotations"], 3.0),
+                              64, 64, opacities=torch.sigmoid(p64["opacity_logits"]),
+                              normalize=normalize)
+    g64 = torch.autograd.grad((img64 * torch.tensor(G)).sum(), [p64[k] for k in names])
+    leaves = [torch.tensor(getattr(f, k), device="cuda").requires_grad_(True) for k in names]
+    img = render_gaussians(*leaves[:4], 64, 64, opacity_logits=leaves[4], normalize=normalize)
+    g32 = torch.autograd.grad(img, leaves, torch.tensor(G, dtype=torch.float32, device="cuda"))
+    for k, a, b in zip(names, g32, g64):
+        err = rel_err(a, b)
+        print(f"{k}: rel err vs float64 {err:.2e}")
+        assert err <= GRAD_TOL, k
