@@ -451,7 +451,9 @@ def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2):
     names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
     runs = []
     for b, f in enumerate(fields_np):
-        g = GaussianField(*[torch.tensor(getattr(f, k), device=dev) for k in names])
+        vals = [f[k] if isinstance(f, dict) else getattr(f, k) for k in names]
+        vals = [None if v is None else torch.as_tensor(v, device=dev).clone() for v in vals]
+        g = GaussianField(*vals)
         g.trainable()
         groups = g.parameter_groups(5e-2, 3e-2, 1e-2, 3e-2, 1e-2)
         runs.append((g, torch.optim.Adam(groups), targets[b], sizes[b]))
@@ -481,6 +483,106 @@ def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2):
             "ms_per_pass": round(ms / steps, 2), "arm": "cuda_tiled"}
 
 
+def run_stress(args, dev):
+    """C3: 2048² target, 1M heavy-tailed Gaussians (30% elongated along the structure tensor),
+    the whole deterministic Adam fit iteration captured in one CUDA graph."""
+    from structsplat_b200 import structure_tensor as st
+    from structsplat_b200.batch import Batch, FitPlan, FitSettings, GraphStep, psnr_from_mse
+    from structsplat_b200.synthetic import make_stress_field, make_target
+    H = W = 2048
+    N = 1_000_000
+    names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
+    target_np = make_target(H, W, seed=31)
+    target = torch.tensor(target_np, device=dev)
+    tensor = st.compute(target, st.StructureTensorConfig(grad_sigma=1.0, tensor_sigma=3.0))
+    along = (tensor.across_edge_angle + math.pi / 2.0).cpu().numpy()
+    f = make_stress_field(H, W, N, seed=32, along_edge_angle=along)
+    params = {k: torch.tensor(getattr(f, k), device=dev) for k in names}
+    settings = FitSettings(deterministic=True)
+    batch = Batch([(H, W)], [N], device=dev)
+    plan = FitPlan(batch, params, target.reshape(-1, 3).contiguous(), settings)
+    counts = (plan.offsets[1:] - plan.offsets[:-1]).to(torch.int64)
+    entries = int(plan.offsets[-1].item())
+    _, loss0 = plan.render()
+    step = GraphStep(plan)
+    for _ in range(args.warmup):
+        step.replay()
+    K = args.stress_steps
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clocks:
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(K):
+            step.replay()
+        e.record()
+        torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / K
+    status = int(plan.status.item())
+    _, loss1 = plan.render()
+    return {"workload": "2048x2048 target, 1M Gaussians, ln-sigma std 1.2, 30% elongated "
+                        "(aspect U[5,50]) along structure-tensor orientation (sigma 1, rho 3); "
+                        "deterministic two-pass backward; Adam fit iteration in one CUDA graph",
+            "ms_per_step": round(ms, 3), "steps": K, "warmup": args.warmup,
+            "tile_entries": entries, "tile_list_max": int(counts.max()),
+            "tile_list_median": float(counts.float().median()),
+            "psnr_start": round(psnr_from_mse(float(loss0[0, 1])), 3),
+            "psnr_end": round(psnr_from_mse(float(loss1[0, 1])), 3),
+            "steps_done": args.warmup + K, "status": status,
+            "peak_mem_gb": round(torch.cuda.max_memory_allocated(dev) / 1e9, 2),
+            "clocks": clocks.summary()}
+
+
+def run_e2e_fit(args, dev):
+    """C5: 1920x1080 target (60 polygons); structure tensor -> density -> 2M Gaussians placed by
+    the seeded sampler -> Adam fit on MSE; time to PSNR thresholds, graph vs plain launches."""
+    from structsplat_b200.batch import Batch, FitPlan, FitSettings, GraphStep, psnr_from_mse
+    from structsplat_b200.placement import place_field
+    from structsplat_b200.synthetic import make_target
+    H, W, N = 1080, 1920, 2_000_000
+    target = torch.tensor(make_target(H, W, seed=51, n_polygons=60), device=dev)
+    thresholds = [float(t) for t in args.psnr_thresholds.split(",")]
+    out = {"workload": "1920x1080 target (60 polygons), 2M Gaussians placed from the structure "
+                       "tensor (sigma 1, rho 2; aniso_onedge, density_random), normalized MSE, "
+                       "Adam with the reference's per-group learning rates",
+           "steps": args.e2e_steps, "check_every": args.e2e_check}
+    for form in ("graph", "plain"):
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t_place = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        field, _, _ = place_field(target, N, strategy="aniso_onedge", seed=5)
+        t_place.record()
+        field["opacity_logits"] = None
+        batch = Batch([(H, W)], [N], device=dev)
+        plan = FitPlan(batch, field, target.reshape(-1, 3).contiguous(), FitSettings())
+        runner = GraphStep(plan).replay if form == "graph" else plan.step
+        torch.cuda.synchronize()
+        placement_ms = t0.elapsed_time(t_place)
+        reached, trace = {}, []
+        start = time.perf_counter()
+        for it in range(1, args.e2e_steps + 1):
+            runner()
+            if it % args.e2e_check == 0 or it == args.e2e_steps:
+                psnr = psnr_from_mse(float(plan.loss[0, 1]))  # syncs: the check is the timer
+                el = time.perf_counter() - start
+                trace.append([it, round(psnr, 3), round(el, 3)])
+                for t in thresholds:
+                    if psnr >= t and str(t) not in reached:
+                        reached[str(t)] = {"iter": it, "seconds": round(el, 3)}
+        total = time.perf_counter() - start
+        out[form] = {"placement_ms": round(placement_ms, 2), "fit_seconds": round(total, 3),
+                     "ms_per_step": round(1e3 * total / args.e2e_steps, 3),
+                     "time_to_psnr": reached, "trace": trace,
+                     "entries": int(plan.offsets[-1].item())}
+        if form == "plain" and not args.no_ref_cuda:
+            # the reference's own per-launch iteration on the same placed field
+            out["reference_cuda_tiled"] = ref_cuda_fit_loop(
+                [(H, W)], [N], [target], [{k: v for k, v in field.items()}], dev,
+                steps=args.ref_batch_steps)
+        del plan, runner
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -493,6 +595,13 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--ref-batch-steps", type=int, default=2)
     ap.add_argument("--batched-only", action="store_true")
+    ap.add_argument("--stress", action="store_true", help="run only the stress workload")
+    ap.add_argument("--stress-steps", type=int, default=20)
+    ap.add_argument("--e2e-fit", action="store_true",
+                    help="run only the placement + fit end-to-end workload")
+    ap.add_argument("--e2e-steps", type=int, default=2000)
+    ap.add_argument("--e2e-check", type=int, default=25)
+    ap.add_argument("--psnr-thresholds", default="30,33,35,36,37,38,39")
     ap.add_argument("--profile", action="store_true",
                     help="only replay the captured step (for ncu launch lists)")
     args = ap.parse_args()
@@ -530,6 +639,12 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(
             seconds=120))
+    if args.stress or args.e2e_fit:
+        dev = torch.device(f"cuda:{local}")
+        torch.cuda.set_device(dev)
+        key, fn = ("stress", run_stress) if args.stress else ("e2e_fit", run_e2e_fit)
+        print(json.dumps({key: fn(args, dev)}), flush=True)
+        return
     workload = None
     if world == 1 and (args.batched_only or not args.no_batched) and not args.profile:
         workload = batched_workload()  # spawn pool before the first CUDA call

@@ -162,6 +162,13 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
                       int tile_size, int normalize, float eps, float fade_tail, float* out,
                       float* den, uint32_t* status, ss_stream_t stream);
 
+/* Launch tuning (process-wide, used by the autotuner): warps per backward CTA for a render
+ * tile size — 4 or 8 for tile 16, 8 or 16 for tile 32, 0 restores the default (8 / 16).
+ * Results do not depend on it.  ss_get_backward_warps returns the value in effect (-1 for an
+ * unsupported tile size). */
+int ss_set_backward_warps(int tile_size, int warps);
+int ss_get_backward_warps(int tile_size);
+
 /* Workspace of ss_render_backward: per-Gaussian moment accumulators (36 B per Gaussian) or,
  * deterministic, per-entry partials (48 B per entry of capacity); height and width are unused. */
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,

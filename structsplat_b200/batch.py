@@ -309,7 +309,7 @@ class GraphStep:
 
 def fit_batch(fields, targets, iters: int = 100, settings: FitSettings | None = None,
               graph: bool = True, log_every: int = 0, check_every: int = 50,
-              tile_size: int = RENDER_TILE):
+              tile_size: int = RENDER_TILE, tune: bool = False):
     """Fit B independent fields to B targets (H_b, W_b, 3) in one batch.
 
     ``fields`` is a list of dicts of CUDA float32 tensors (the five ``PARAM_NAMES``; opacity
@@ -318,16 +318,23 @@ def fit_batch(fields, targets, iters: int = 100, settings: FitSettings | None = 
     plan.  Every ``check_every`` steps the host reads the index status; if the tile list
     outgrew its capacity the plan is rebuilt with more room (in deterministic mode the steps
     since the last check are replayed from a snapshot, so the result never depends on it).
+    ``tune=True`` lets the autotuner pick the tile size and backward warps for this workload
+    (``autotune.tune_fit``) instead of ``tile_size``.
     """
     settings = settings or FitSettings()
     sizes = [(int(t.shape[0]), int(t.shape[1])) for t in targets]
     counts = [int(f["means"].shape[0]) for f in fields]
-    batch = Batch(sizes, counts, tile_size=tile_size, device=targets[0].device)
     params = Batch.concat_fields(fields)
-    target = batch.concat_images(targets)
+    target = torch.cat([t.reshape(-1, 3) for t in targets]).contiguous()
+    tuned = None
+    if tune:
+        from .autotune import tune_fit
+        tuned = tune_fit(sizes, counts, params, target, settings)
+        tile_size = tuned.tile_size
+    batch = Batch(sizes, counts, tile_size=tile_size, device=targets[0].device)
     plan = FitPlan(batch, params, target, settings)
     runner = GraphStep(plan) if graph else None
-    history = {"iter": [], "psnr": [], "replans": 0}
+    history = {"iter": [], "psnr": [], "replans": 0, "tuned": tuned}
     snap = plan.state() if settings.deterministic else None
     done = 0
     while done < iters:

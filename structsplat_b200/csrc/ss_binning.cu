@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __re
   }
 }
 
-constexpr int kBigSortCtas = 32;
+constexpr int kBigSortCtas = 296;  // 2 per SM: long lists are common under heavy-tailed fields
 
 // Opts tile_sort_big_kernel into its dynamic shared memory once per device.
 int allow_big_sort_smem() {

@@ -26,6 +26,8 @@
 // per-Gaussian accumulators (fast mode), or stored per (tile, Gaussian) entry and summed per
 // Gaussian in ascending tile order by a second kernel (deterministic mode).  A per-Gaussian
 // epilogue applies o, a, b, c once.
+#include <atomic>
+
 #include "ss_common.cuh"
 
 namespace ss {
@@ -38,7 +40,6 @@ template <int TS>
 struct Tiling {
   static constexpr int kWarps = (TS / 8) * (TS / 8);  // forward: one 8x8 block per warp
   static constexpr int kFwdThreads = 32 * kWarps;
-  static constexpr int kBwdThreads = TS == 16 ? 256 : 512;
   // backward whole-list stage: what fits in 48 KB of static shared memory beside the pixels
   static constexpr int kBwdStageAll = TS == 16 ? 512 : 448;
 };
@@ -305,15 +306,19 @@ __device__ __forceinline__ int moment_of_lane(int lane) {
 
 // Backward of one tile.  PIXGRAD: the per-pixel inputs come ready-made from the fit forward
 // (pixel_grad); otherwise they are formed from grad_out, out and den.
-template <int TS, bool FADE, bool DETERMINISTIC, bool PIXGRAD>
-__global__ void __launch_bounds__(Tiling<TS>::kBwdThreads, TS == 16 ? 4 : 2)
+template <int TS, int NT>
+struct BackwardOccupancy {  // CTAs per SM the register budget is planned for
+  static constexpr int kBlocks = TS == 16 ? (NT == 128 ? 6 : 4) : (NT == 256 ? 4 : 2);
+};
+
+template <int TS, int NT, bool FADE, bool DETERMINISTIC, bool PIXGRAD>
+__global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec,
                     int64_t n, const float* __restrict__ den, const float* __restrict__ out,
                     const float4* __restrict__ pixel_grad, const int32_t* __restrict__ gids,
                     int64_t cap, const int32_t* __restrict__ offsets, Frames frames,
                     int normalize, float eps, float tail, float* __restrict__ moments,
                     float* __restrict__ partials, uint32_t* status) {
-  constexpr int NT = Tiling<TS>::kBwdThreads;
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
   __shared__ __align__(16) float4 stage[kStageMax][4];
   __shared__ float4 pix[TS * TS + 1];  // the last entry is a zero pixel for masked slots
@@ -533,24 +538,44 @@ void launch_forward(int loss_kind, unsigned T, cudaStream_t s, const Splat* rec,
 #undef SS_FWD
 }
 
-template <int TS, bool PIXGRAD>
-void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float* grad_out,
-                     const Splat* rec, int64_t n, const float* den, const float* out,
-                     const float4* pixel_grad, const int32_t* gids, int64_t cap,
-                     const int32_t* offsets, const Frames& f, int normalize, float eps,
-                     float tail, float* ws, uint32_t* status) {
-  constexpr int NT = Tiling<TS>::kBwdThreads;
+// Warps per backward CTA: a process-wide tuning knob (0 = the default of the tile size).
+std::atomic<int> g_backward_warps[2] = {{0}, {0}};
+
+template <int TS, int NT, bool PIXGRAD>
+void launch_backward_nt(unsigned T, cudaStream_t s, bool deterministic, const float* grad_out,
+                        const Splat* rec, int64_t n, const float* den, const float* out,
+                        const float4* pixel_grad, const int32_t* gids, int64_t cap,
+                        const int32_t* offsets, const Frames& f, int normalize, float eps,
+                        float tail, float* ws, uint32_t* status) {
   const bool fade = tail > 0.0f;
 #define SS_BWD(FADE, DET)                                                                     \
-  backward_kernel<TS, FADE, DET, PIXGRAD><<<T, NT, 0, s>>>(grad_out, rec, n, den, out,       \
-                                                           pixel_grad, gids, cap, offsets, f, \
-                                                           normalize, eps, tail, ws, ws, status)
+  backward_kernel<TS, NT, FADE, DET, PIXGRAD><<<T, NT, 0, s>>>(                              \
+      grad_out, rec, n, den, out, pixel_grad, gids, cap, offsets, f, normalize, eps, tail, ws, \
+      ws, status)
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
     if (fade) SS_BWD(true, false); else SS_BWD(false, false);
   }
 #undef SS_BWD
+}
+
+template <int TS, bool PIXGRAD>
+void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float* grad_out,
+                     const Splat* rec, int64_t n, const float* den, const float* out,
+                     const float4* pixel_grad, const int32_t* gids, int64_t cap,
+                     const int32_t* offsets, const Frames& f, int normalize, float eps,
+                     float tail, float* ws, uint32_t* status) {
+  const int warps = g_backward_warps[TS == 16 ? 0 : 1].load(std::memory_order_relaxed);
+  constexpr int kSmall = TS == 16 ? 128 : 256, kLarge = TS == 16 ? 256 : 512;
+  if (warps * 32 == kSmall)
+    launch_backward_nt<TS, kSmall, PIXGRAD>(T, s, deterministic, grad_out, rec, n, den, out,
+                                            pixel_grad, gids, cap, offsets, f, normalize, eps,
+                                            tail, ws, status);
+  else
+    launch_backward_nt<TS, kLarge, PIXGRAD>(T, s, deterministic, grad_out, rec, n, den, out,
+                                            pixel_grad, gids, cap, offsets, f, normalize, eps,
+                                            tail, ws, status);
 }
 
 // Forward over any tile set; loss_kind selects the plain render or a fit forward.
@@ -694,6 +719,23 @@ int ss_batch_render_forward(const ss_batch* batch, const void* records, int64_t 
   return render_forward(f, batch->tile_size, batch->tiles, records, n, tile_gids, gid_capacity,
                         tile_offsets, normalize, eps, fade_tail, kNoLoss, nullptr, 0.f, nullptr,
                         out, den, nullptr, as_stream(stream));
+}
+
+int ss_set_backward_warps(int tile_size, int warps) {
+  if (tile_size != 16 && tile_size != 32)
+    return fail(SS_ERR_UNSUPPORTED, "render tile_size must be 16 or 32, got %d", tile_size);
+  const int small = tile_size == 16 ? 4 : 8, large = tile_size == 16 ? 8 : 16;
+  if (warps != 0 && warps != small && warps != large)
+    return fail(SS_ERR_INVALID_ARGUMENT, "backward warps for tile %d must be 0, %d or %d",
+                tile_size, small, large);
+  g_backward_warps[tile_size == 16 ? 0 : 1].store(warps, std::memory_order_relaxed);
+  return SS_OK;
+}
+
+int ss_get_backward_warps(int tile_size) {
+  if (tile_size != 16 && tile_size != 32) return -1;
+  const int w = g_backward_warps[tile_size == 16 ? 0 : 1].load(std::memory_order_relaxed);
+  return w ? w : (tile_size == 16 ? 8 : 16);
 }
 
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,

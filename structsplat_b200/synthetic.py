@@ -86,3 +86,26 @@ def make_field(H: int, W: int, n: int, seed: int, log_sigma_mean: float = math.l
     colors = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
     logits = rng.normal(0.0, 1.0, n).astype(np.float32)
     return FieldArrays(means, log_scales, rotations, colors, logits)
+
+
+def make_stress_field(H: int, W: int, n: int, seed: int, along_edge_angle: np.ndarray,
+                      log_sigma_std: float = 1.2, elongated_frac: float = 0.3,
+                      aspect_range=(5.0, 50.0)) -> FieldArrays:
+    """Heavy-tailed stress field: σ = exp(N(ln 2, 1.2)) per Gaussian, and a fraction of
+    elongated Gaussians (aspect ratio U[5, 50], same area) aligned with ``along_edge_angle``
+    (H, W) read at the pixel nearest their mean; the rest as ``make_field``.  The heavy tail
+    gives tile lists from a few entries to ~10⁴."""
+    f = make_field(H, W, n, seed, log_sigma_std=log_sigma_std)
+    rng = np.random.default_rng(seed + 7919)
+    sigma = rng.normal(math.log(2.0), log_sigma_std, n).astype(np.float32)
+    f.log_scales[:, 0] = sigma
+    f.log_scales[:, 1] = sigma
+    elong = rng.random(n) < elongated_frac
+    k = int(elong.sum())
+    half_log_ar = 0.5 * np.log(rng.uniform(aspect_range[0], aspect_range[1], k)).astype(np.float32)
+    f.log_scales[elong, 0] += half_log_ar
+    f.log_scales[elong, 1] -= half_log_ar
+    xi = np.clip(np.round(f.means[elong, 0]).astype(int), 0, W - 1)
+    yi = np.clip(np.round(f.means[elong, 1]).astype(int), 0, H - 1)
+    f.rotations[elong] = np.asarray(along_edge_angle, np.float32)[yi, xi]
+    return f

@@ -130,3 +130,14 @@ def test_batch_validation_without_gpu(lib):
                       None, ctypes.c_float(0.0), ptrs, ptrs, ptrs, lrs, 0.9, 0.999, 1e-8,
                       ctypes.c_float(-1.0), None, None, None)
     assert rc == 1 and "null" in msg
+
+
+def test_backward_warps_knob_validation(lib):
+    rc, msg = _status(lib, "ss_set_backward_warps", 8, 4)
+    assert rc == 4 and "tile_size" in msg
+    rc, msg = _status(lib, "ss_set_backward_warps", 32, 12)
+    assert rc == 1 and "0, 8 or 16" in msg
+    assert lib.ss_get_backward_warps(16) == 8 and lib.ss_get_backward_warps(32) == 16
+    assert lib.ss_set_backward_warps(32, 8) == 0 and lib.ss_get_backward_warps(32) == 8
+    assert lib.ss_set_backward_warps(32, 0) == 0 and lib.ss_get_backward_warps(32) == 16
+    assert lib.ss_get_backward_warps(7) == -1
