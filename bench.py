@@ -35,6 +35,7 @@ sys.path.insert(0, str(REPO))
 METRIC = "fwd+bwd ms/iter (1024², 100k Gaussians); batched fit img/s vs plain kernel"
 WORKLOAD = {"H": 1024, "W": 1024, "N": 100_000, "seed": 0, "mode": "normalized"}
 PAIR_SLOTS_FWD, PAIR_SLOTS_BWD = 14, 40   # FP32 issue slots per in-rectangle pair (reference)
+BACKWARD_DRAM_BYTES = 40_239_360 + 2_560  # one backward_kernel launch at this workload (ncu)
 SM_COUNT, FP32_LANES = 148, 128
 
 
@@ -181,7 +182,8 @@ def run_ours(args, rank, world, dev):
 
     # ---- dominant kernels alone, CUDA events on the launching stream ----
     kt = {}
-    for name, fn in (("forward", plan.render), ("backward", lambda: plan.backward(grad_out, params)),
+    for name, fn in (("forward", plan.render), ("backward_kernel", lambda: plan.backward_tiles(grad_out)),
+                     ("backward", lambda: plan.backward(grad_out, params)),
                      ("binning", lambda: (plan.count(), plan.fill())),
                      ("project", lambda: plan.project(params))):
         for _ in range(3):
@@ -666,7 +668,7 @@ def main():
         f_mhz = peaks.get("sm_max_mhz") or 1965.0
         peak_slots = SM_COUNT * FP32_LANES * f_mhz * 1e6 / 1e9   # Gslot/s
         kt = res["kernels_ms"]
-        bwd_ach = P * PAIR_SLOTS_BWD / (kt["backward"] * 1e-3) / 1e9
+        bwd_ach = P * PAIR_SLOTS_BWD / (kt["backward_kernel"] * 1e-3) / 1e9
         fwd_ach = P * PAIR_SLOTS_FWD / (kt["forward"] * 1e-3) / 1e9
         t_bound_ms = P * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (peak_slots * 1e9) * 1e3
         line = {
@@ -685,7 +687,10 @@ def main():
             "roofline": {"bound": "fp32", "kernel": "backward_kernel",
                          "achieved": round(bwd_ach, 1), "peak": round(peak_slots, 1),
                          "unit": "Gslot/s", "frac": round(bwd_ach / peak_slots, 4),
-                         "traffic": None,
+                         "traffic": BACKWARD_DRAM_BYTES,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                           "backward_kernel launch, ncu --set full "
+                                           "(profiles/backward_kernel_1024x1024_100k.md)",
                          "work": f"{PAIR_SLOTS_BWD} FP32 issue slots per in-rectangle pair x "
                                  f"{P} pairs per launch",
                          "peak_source": "148 SMs x 128 FP32 lanes x sm_max_mhz of "

@@ -274,6 +274,23 @@ int ss_place_gaussians(const double* points, int64_t n, const double* density,
                        int64_t density_points, float* means, float* log_scales,
                        float* rotations, float* colors, ss_stream_t stream);
 
+/* ---------------------------------------------------------------- render backward, staged
+ * ss_render_backward split in two, for callers that accumulate several renders' moments before
+ * finalising (or time the tile kernel alone).  _moments runs only the tile kernel: in fast mode
+ * it ADDS into per-Gaussian moments (zero the workspace first), in deterministic mode it writes
+ * the per-entry partials.  _finalize turns them into the four gradient outputs. */
+int ss_render_backward_moments(const float* grad_out, const void* records, int64_t n,
+                               const float* den, const float* out, const int32_t* tile_gids,
+                               int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                               int width, int tile_size, int normalize, float eps,
+                               float fade_tail, int deterministic, void* workspace,
+                               size_t workspace_bytes, uint32_t* status, ss_stream_t stream);
+int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* tile_gids,
+                                int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                                int width, int tile_size, int has_opacity, int deterministic,
+                                const void* workspace, float* grad_means, float* grad_conics,
+                                float* grad_colors, float* grad_opacities, ss_stream_t stream);
+
 /* ---------------------------------------------------------------- reference-shaped calls
  * One-call equivalents of the reference extension's entry points, taking its tensor
  * contract (render_ext.cpp:89-137).  They pack records into `workspace` (size from

@@ -765,6 +765,54 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
                          workspace, workspace_bytes, status, as_stream(stream));
 }
 
+int ss_render_backward_moments(const float* grad_out, const void* records, int64_t n,
+                               const float* den, const float* out, const int32_t* tile_gids,
+                               int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                               int width, int tile_size, int normalize, float eps,
+                               float fade_tail, int deterministic, void* workspace,
+                               size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, eps);
+  if (rc) return rc;
+  if (n == 0 || (int64_t)height * width == 0) return SS_OK;
+  if (!grad_out || !records || !den || !out || !tile_offsets)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
+  if (workspace_bytes < need || !workspace)
+    return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+                workspace_bytes, need);
+  const int64_t T = (int64_t)((width + tile_size - 1) / tile_size) *
+                    ((height + tile_size - 1) / tile_size);
+  return render_backward_tiles(single_frame(height, width, tile_size), tile_size, T, grad_out,
+                               records, n, den, out, nullptr, tile_gids, gid_capacity,
+                               tile_offsets, normalize, eps, fade_tail, deterministic,
+                               static_cast<float*>(workspace), status, as_stream(stream));
+}
+
+int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* tile_gids,
+                                int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                                int width, int tile_size, int has_opacity, int deterministic,
+                                const void* workspace, float* grad_means, float* grad_conics,
+                                float* grad_colors, float* grad_opacities, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, 1.0f);
+  if (rc) return rc;
+  if (n == 0) return SS_OK;
+  if (!records || !workspace || !grad_means || !grad_conics || !grad_colors ||
+      (has_opacity && !grad_opacities) || (deterministic && !tile_offsets))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const Splat* rec = static_cast<const Splat*>(records);
+  const float* ws = static_cast<const float*>(workspace);
+  const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
+  cudaStream_t s = as_stream(stream);
+  if (deterministic)
+    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, tile_gids, gid_capacity, tile_offsets, single_frame(height, width, tile_size),
+        tile_size, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
+  else
+    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
+  return check_launch("backward finalize");
+}
+
 int ss_batch_render_backward(const ss_batch* batch, const float* grad_out, const void* records,
                              int64_t n, const float* den, const float* out,
                              const int32_t* tile_gids, int64_t gid_capacity,

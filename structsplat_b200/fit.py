@@ -131,6 +131,14 @@ class RenderPlan:
                      _p(self.g_rotations), _p(self.g_logits if self.has_opacity else None),
                      _stream())
 
+    def backward_tiles(self, grad_out):
+        """Only the backward tile kernel (fast mode: adds into the moments), for timing."""
+        _native.call("ss_render_backward_moments", _p(grad_out), _p(self.records), self.n,
+                     _p(self.den), _p(self.image), _p(self.gids), self.capacity,
+                     _p(self.offsets), self.H, self.W, self.tile_size, int(self.normalize),
+                     float(self.eps), float(self.tail), int(self.deterministic), _p(self.bwd_ws),
+                     self.bwd_ws_bytes, _p(self.status), _stream())
+
     def forward(self, params):
         self.status.zero_()
         self.project(params)

@@ -85,3 +85,30 @@ def test_graph_fit_matches_eager_fit_and_improves_psnr():
     assert h_graph["psnr"][-1] > h_graph["psnr"][0]
     assert abs(h_graph["psnr"][-1] - h_eager["psnr"][-1]) <= 0.01
     assert not h_graph["overflowed"]
+
+
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_staged_backward_equals_one_call_backward(deterministic):
+    require_cuda()
+    from structsplat_b200 import _native
+    from structsplat_b200.render import _p, _stream
+    H, W = 80, 72
+    params = _field(H, W, 500, seed=8)
+    grad_out = torch.randn(H, W, 3, device="cuda", generator=torch.Generator("cuda").manual_seed(9))
+    plan = RenderPlan.for_field(params, H, W, deterministic=deterministic)
+    plan.forward(params)
+    plan.backward(grad_out, params)
+    want = [plan.g_means.clone(), plan.g_conics.clone(), plan.g_colors.clone(),
+            plan.g_opac.clone()]
+    plan.bwd_ws.zero_()
+    plan.backward_tiles(grad_out)
+    got = [torch.empty_like(t) for t in want]
+    _native.call("ss_render_backward_finalize", _p(plan.records), plan.n, _p(plan.gids),
+                 plan.capacity, _p(plan.offsets), H, W, plan.tile_size, 1, int(deterministic),
+                 _p(plan.bwd_ws), _p(got[0]), _p(got[1]), _p(got[2]), _p(got[3]), _stream())
+    torch.cuda.synchronize()
+    for a, b in zip(got, want):
+        if deterministic:
+            assert torch.equal(a, b)
+        else:
+            assert rel_err(a, b) <= 1e-5
