@@ -1,20 +1,21 @@
 // Tiled forward and backward of the clipped-support normalized / additive renderer.
 //
 // Both kernels run one CTA per TS x TS tile (TS = 16 or 32) and stage the tile's Gaussian list
-// 64 records at a time into shared memory with cp.async, double-buffered, so the L2 gather of
-// the next chunk overlaps the math on the current one.
+// into shared memory with cp.async: whole when it fits (one barrier per tile), otherwise 64
+// records at a time, double-buffered, so the L2 gather of the next chunk overlaps the math on
+// the current one.
 //
 // Forward (render_ext.cu:349-431 contract): each warp owns an 8x8 pixel block (two pixels per
-// lane, rows r and r+4).  For every staged chunk a warp builds, with two ballots, the mask of
-// the Gaussians whose support rectangle touches its block and walks only those; a lane masks
-// its own pixels with the in-rectangle test.  The weight is 2^(qa dx^2 + qb dx dy + qc dy^2)
+// lane, rows r and r+4).  For every 32 staged records a warp builds, with one ballot, the mask
+// of the Gaussians whose support rectangle touches its block and walks only those, in
+// ascending id; a lane masks its own pixels with the in-rectangle test.  The weight is 2^(qa dx^2 + qb dx dy + qc dy^2)
 // on the SFU.  The epilogue writes den raw and out = num / (den + eps) or num.
 //
 // Backward (render_ext.cu:696-847 contract): a prologue turns grad_out, out and den into the
-// per-pixel (dnum_r, dnum_g, dnum_b, dden) of the tile in shared memory.  Work is then
-// Gaussian-major: one warp per staged Gaussian walks exactly the pixels of its support
-// rectangle inside the tile — lane (c, s) takes columns c, c+8, … and the s-th quarter of the
-// rows — and accumulates nine moments
+// per-pixel (dnum_r, dnum_g, dnum_b, dden) of the tile in shared memory (the fit path hands
+// them over ready-made).  Work is then Gaussian-major: one warp per staged Gaussian walks
+// exactly the pixels of its support rectangle inside the tile — lane (c, s) takes columns c,
+// c+8, … and the s-th quarter of the rows — and accumulates nine moments
 //   R_k = Σ base·dnum_k,  G = Σ base·dw,  S1 = Σ t dx,  S2 = Σ t dy,  S3 = Σ t dx²,
 //   S4 = Σ t dx dy,  S5 = Σ t dy²,     dw = dnum·c + dden,  t = raw·dw (0 where the fade clamps)
 // from which
@@ -104,11 +105,13 @@ constexpr int kStageAll = 512;
 // entry (q >> 2) for q = threadIdx.x, threadIdx.x + NT, …
 template <int NT>
 __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
-                                            const TileList& L, int64_t k0, int m) {
+                                            const TileList& L, int64_t k0, int m,
+                                            int* gid_dst = nullptr) {
   for (int q = threadIdx.x; q < 4 * m; q += NT) {
     const int slot = q >> 2, piece = q & 3;
     const int g = L.gid(k0 + slot);
     cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
+    if (gid_dst && piece == 0) gid_dst[slot] = g;  // the backward's atomics need the id
   }
 }
 
@@ -321,19 +324,19 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
                     float* __restrict__ partials, uint32_t* status) {
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
   __shared__ __align__(16) float4 stage[kStageMax][4];
-  __shared__ float4 pix[TS * TS + 1];  // the last entry is a zero pixel for masked slots
-  __shared__ int next_entry;
+  __shared__ float4 pix[TS * TS];
+  __shared__ int stage_gid[kStageMax];
   const int tile = blockIdx.x;
   const Frame fr = frame_of_tile(frames, tile, n);
   const int local = tile - fr.first_tile;
   const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
   const int H = fr.H, W = fr.W;
-  for (int q = threadIdx.x; q <= TS * TS; q += NT) {
+  for (int q = threadIdx.x; q < TS * TS; q += NT) {
     const int x = tx0 + (q % TS), y = ty0 + (q / TS);
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (PIXGRAD) {
-      if (q < TS * TS && x < W && y < H) v = pixel_grad[fr.pixel_base + (int64_t)y * W + x];
-    } else if (q < TS * TS && x < W && y < H) {
+      if (x < W && y < H) v = pixel_grad[fr.pixel_base + (int64_t)y * W + x];
+    } else if (x < W && y < H) {
       const int64_t p = fr.pixel_base + (int64_t)y * W + x;
       const float gr = grad_out[3 * p], gg = grad_out[3 * p + 1], gb = grad_out[3 * p + 2];
       v = make_float4(gr, gg, gb, 0.f);
@@ -355,7 +358,9 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
     return;
   }
-  auto work = [&](const float4(*st)[4], int j, int64_t k0) {
+  // One staged Gaussian (entry k0 + j, id gsm[j]) on the whole warp.  Lanes whose column or
+  // rows fall outside the rectangle skip the loops (divergent but exact: they add nothing).
+  auto work = [&](const float4(*st)[4], int j, int64_t k0, const int* gsm) {
     const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
     const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
     const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
@@ -369,33 +374,34 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
     for (int pass = 0; pass < passes; ++pass) {
       const int cx = cx0 + col_slot + 8 * pass;
-      const bool col_ok = cx < cx1;
-      const float dx = (float)(tx0 + cx) - p0.x;
-      const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
-      float tc = 0.f, uc = 0.f;
-      float dy = (float)(ty0 + ry0) - p0.y;
-      int pidx = ry0 * TS + cx;
-      for (int k = 0; k < seg_rows; ++k, dy += 1.0f, pidx += TS) {
-        const bool ok = col_ok && k < rows;
-        const float4 g = pix[ok ? pidx : TS * TS];
-        const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
-        const float raw = fast_exp2(ok ? e : -INFINITY);
-        const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-        const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
-        acc[0] = fmaf(base_w, g.x, acc[0]);
-        acc[1] = fmaf(base_w, g.y, acc[1]);
-        acc[2] = fmaf(base_w, g.z, acc[2]);
-        acc[3] = fmaf(base_w, dw, acc[3]);
-        const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
-        const float u = t * dy;
-        tc += t;
-        uc += u;
-        acc[8] = fmaf(u, dy, acc[8]);
+      if (cx < cx1 && rows > 0) {
+        const float dx = (float)(tx0 + cx) - p0.x;
+        const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+        float tc = 0.f, uc = 0.f;
+        float dy = (float)(ty0 + ry0) - p0.y;
+        int pidx = ry0 * TS + cx;
+#pragma unroll 1
+        for (int k = 0; k < rows; ++k, dy += 1.0f, pidx += TS) {
+          const float4 g = pix[pidx];
+          const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
+          const float raw = fast_exp2(e);
+          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
+          acc[0] = fmaf(base_w, g.x, acc[0]);
+          acc[1] = fmaf(base_w, g.y, acc[1]);
+          acc[2] = fmaf(base_w, g.z, acc[2]);
+          acc[3] = fmaf(base_w, dw, acc[3]);
+          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+          const float u = t * dy;
+          tc += t;
+          uc += u;
+          acc[8] = fmaf(u, dy, acc[8]);
+        }
+        acc[4] = fmaf(dx, tc, acc[4]);
+        acc[5] += uc;
+        acc[6] = fmaf(dx * dx, tc, acc[6]);
+        acc[7] = fmaf(dx, uc, acc[7]);
       }
-      acc[4] = fmaf(dx, tc, acc[4]);
-      acc[5] += uc;
-      acc[6] = fmaf(dx * dx, tc, acc[6]);
-      acc[7] = fmaf(dx, uc, acc[7]);
     }
     const float total = reduce_scatter9(acc, lane);
     if (my_moment >= 0) {
@@ -403,39 +409,35 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       if (DETERMINISTIC) {
         partials[entry * kPartialFloats + my_moment] = total;
       } else {
-        atomicAdd(moments + (int64_t)my_moment * n + L.gid(k0 + j), total);
+        atomicAdd(moments + (int64_t)my_moment * n + gsm[j], total);
       }
     }
   };
   if (L.count <= kStageMax) {
-    // whole list staged once; warps take Gaussians from a shared counter (load balancing)
-    if (threadIdx.x == 0) next_entry = 0;
-    stage_range<NT>(stage, rec, L, 0, (int)L.count);
+    // whole list staged once; warp w takes entries w, w + warps, … (a static split measured
+    // faster than taking them from a shared counter)
+    stage_range<NT>(stage, rec, L, 0, (int)L.count, stage_gid);
     cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     const int count = (int)L.count;
-    for (;;) {
-      int j = 0;
-      if (lane == 0) j = atomicAdd(&next_entry, 1);
-      j = __shfl_sync(0xffffffffu, j, 0);
-      if (j >= count) break;
-      work(stage, j, 0);
-    }
+    for (int j = warp; j < count; j += NT / 32) work(stage, j, 0, stage_gid);
   } else {
     float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
     const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
-    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0));
+    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0), stage_gid);
     cp_async_commit();
     for (int c = 0; c < nchunks; ++c) {
       const int64_t k0 = (int64_t)c * kChunk;
       if (c + 1 < nchunks)
-        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
+        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk),
+                        stage_gid + ((c + 1) & 1) * kChunk);
       cp_async_commit();
       cp_async_wait_one();
       __syncthreads();
       const int m = chunk_len(L.count, k0);
-      for (int j = warp; j < m; j += NT / 32) work(buf[c & 1], j, k0);
+      for (int j = warp; j < m; j += NT / 32)
+        work(buf[c & 1], j, k0, stage_gid + (c & 1) * kChunk);
       __syncthreads();
     }
   }
