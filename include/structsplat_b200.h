@@ -278,9 +278,14 @@ int ss_place_gaussians(const double* points, int64_t n, const double* density,
  * ss_render_backward split in two, for callers that accumulate several renders' moments before
  * finalising (or time the tile kernel alone).  _moments runs only the tile kernel: in fast mode
  * it ADDS into per-Gaussian moments (zero the workspace first), in deterministic mode it writes
- * the per-entry partials.  _finalize turns them into the four gradient outputs. */
-int ss_render_backward_moments(const float* grad_out, const void* records, int64_t n,
-                               const float* den, const float* out, const int32_t* tile_gids,
+ * the per-entry partials.  Its per-pixel input is either grad_out with out and den (the plain
+ * render's gradient), or, when pixel_grad is given, (P,4) f32 per-pixel gradients with respect
+ * to the accumulated colour numerator and weight sum (grad_out, out, den, normalize and eps are
+ * then unused): (0, 0, 0, g) differentiates sum(g * den), the raw weight map.
+ * _finalize turns them into the four gradient outputs. */
+int ss_render_backward_moments(const float* grad_out, const float* pixel_grad,
+                               const void* records, int64_t n, const float* den,
+                               const float* out, const int32_t* tile_gids,
                                int64_t gid_capacity, const int32_t* tile_offsets, int height,
                                int width, int tile_size, int normalize, float eps,
                                float fade_tail, int deterministic, void* workspace,
@@ -290,6 +295,13 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
                                 int width, int tile_size, int has_opacity, int deterministic,
                                 const void* workspace, float* grad_means, float* grad_conics,
                                 float* grad_colors, float* grad_opacities, ss_stream_t stream);
+
+/* ---------------------------------------------------------------- per-Gaussian passes
+ * gaussian_activity (render.py:417-442): activity[g] = sum over the pixels of g's clipped
+ * support rectangle of max(exp(-q/2) - fade_tail, 0) (opacity-free), from packed records.
+ * lanes_per_gaussian: 8 (fields of small Gaussians) or 32.  Deterministic. */
+int ss_gaussian_activity(const void* records, int64_t n, float fade_tail, int lanes_per_gaussian,
+                         float* activity, ss_stream_t stream);
 
 /* ---------------------------------------------------------------- reference-shaped calls
  * One-call equivalents of the reference extension's entry points, taking its tensor

@@ -120,7 +120,6 @@ template <bool FADE>
 __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int sx0, int sy0,
                                               int lane, int px, int py0, float fx, float fy0,
                                               float tail, float (&acc0)[4], float (&acc1)[4]) {
-  const int py1 = py0 + 4;
   for (int base = 0; base < m; base += 32) {
     unsigned hits = hit_mask(st + base, m - base, sx0, sy0, lane, 0);
     while (hits) {
@@ -129,9 +128,11 @@ __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int 
       const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
       const float4 p0 = st[j][0], p1 = st[j][1];
       const float cb = st[j][2].x;
-      const bool inx = px >= r.x && px < r.z;
-      const bool in0 = inx && py0 >= r.y && py0 < r.w;
-      const bool in1 = inx && py1 >= r.y && py1 < r.w;
+      // half-open range tests as one unsigned compare each: x in [x0, x1) <=> x - x0 < x1 - x0
+      const unsigned ry = (unsigned)(py0 - r.y), rh = (unsigned)(r.w - r.y);
+      const bool inx = (unsigned)(px - r.x) < (unsigned)(r.z - r.x);
+      const bool in0 = inx && ry < rh;
+      const bool in1 = inx && ry + 4u < rh;
       const float dx = fx - p0.x, dy0 = fy0 - p0.y, dy1 = dy0 + 4.0f;
       const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
       const float raw0 = fast_exp2(fmaf(dy0, fmaf(p1.x, dy0, bdx), adx2));
@@ -767,8 +768,9 @@ int ss_render_backward(const float* grad_out, const void* records, int64_t n, co
                          workspace, workspace_bytes, status, as_stream(stream));
 }
 
-int ss_render_backward_moments(const float* grad_out, const void* records, int64_t n,
-                               const float* den, const float* out, const int32_t* tile_gids,
+int ss_render_backward_moments(const float* grad_out, const float* pixel_grad,
+                               const void* records, int64_t n, const float* den,
+                               const float* out, const int32_t* tile_gids,
                                int64_t gid_capacity, const int32_t* tile_offsets, int height,
                                int width, int tile_size, int normalize, float eps,
                                float fade_tail, int deterministic, void* workspace,
@@ -776,18 +778,22 @@ int ss_render_backward_moments(const float* grad_out, const void* records, int64
   int rc = check_render_args(n, height, width, tile_size, eps);
   if (rc) return rc;
   if (n == 0 || (int64_t)height * width == 0) return SS_OK;
-  if (!grad_out || !records || !den || !out || !tile_offsets)
-    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (!records || !tile_offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (!pixel_grad && (!grad_out || !den || !out))
+    return fail(SS_ERR_INVALID_ARGUMENT, "need grad_out, out and den, or pixel_grad");
+  if (pixel_grad && reinterpret_cast<uintptr_t>(pixel_grad) % 16)
+    return fail(SS_ERR_INVALID_ARGUMENT, "pixel_grad must be 16-byte aligned");
   const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
   if (workspace_bytes < need || !workspace)
     return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
                 workspace_bytes, need);
   const int64_t T = (int64_t)((width + tile_size - 1) / tile_size) *
                     ((height + tile_size - 1) / tile_size);
-  return render_backward_tiles(single_frame(height, width, tile_size), tile_size, T, grad_out,
-                               records, n, den, out, nullptr, tile_gids, gid_capacity,
-                               tile_offsets, normalize, eps, fade_tail, deterministic,
-                               static_cast<float*>(workspace), status, as_stream(stream));
+  return render_backward_tiles(single_frame(height, width, tile_size), tile_size, T,
+                               pixel_grad ? nullptr : grad_out, records, n, den, out,
+                               pixel_grad, tile_gids, gid_capacity, tile_offsets, normalize, eps,
+                               fade_tail, deterministic, static_cast<float*>(workspace), status,
+                               as_stream(stream));
 }
 
 int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* tile_gids,

@@ -133,7 +133,7 @@ class RenderPlan:
 
     def backward_tiles(self, grad_out):
         """Only the backward tile kernel (fast mode: adds into the moments), for timing."""
-        _native.call("ss_render_backward_moments", _p(grad_out), _p(self.records), self.n,
+        _native.call("ss_render_backward_moments", _p(grad_out), None, _p(self.records), self.n,
                      _p(self.den), _p(self.image), _p(self.gids), self.capacity,
                      _p(self.offsets), self.H, self.W, self.tile_size, int(self.normalize),
                      float(self.eps), float(self.tail), int(self.deterministic), _p(self.bwd_ws),

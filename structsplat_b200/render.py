@@ -322,3 +322,116 @@ def render_field(means, conics, colors, radii, H: int, W: int, chunk: int = 4096
                        normalize=normalize, eps=eps, support_fade=support_fade,
                        sigma_cutoff=sigma_cutoff, support_fade_alpha=support_fade_alpha,
                        deterministic=deterministic)
+
+
+# ---------------------------------------------------------------- passes reusing the pair loop
+
+def gaussian_activity(means, conics, radii, H: int, W: int, chunk: int = 4096,
+                      support_fade: bool = False, sigma_cutoff: float = 3.0,
+                      support_fade_alpha: float | None = None) -> torch.Tensor:
+    """Each Gaussian's summed unnormalised weight over the image (render.py:417-442).
+
+    Opacity-free, like the reference's pruning helper; ``chunk`` is accepted for signature
+    compatibility (there is no chunking here).  Deterministic.
+    """
+    del chunk
+    if not means.is_cuda:
+        raise RuntimeError("StructSplat B200 renderer requires CUDA tensors; pass device='cuda'.")
+    n = means.shape[0]
+    alpha = resolve_fade_alpha(support_fade, support_fade_alpha)
+    tail = fade_tail(sigma_cutoff, alpha)
+    means = means.detach().contiguous().to(torch.float32)
+    conics = conics.detach().contiguous().to(torch.float32)
+    rec = pack_records(means, conics, conics, radii.contiguous(), None, H, W)
+    act = torch.empty(n, device=means.device, dtype=torch.float32)
+    if n:
+        r = radii.detach()
+        mean_side = float((2 * r + 1).to(torch.float32).mean()) if n else 0.0
+        lanes = 8 if mean_side * mean_side <= 96 else 32
+        _native.call("ss_gaussian_activity", _p(rec), n, float(tail), lanes, _p(act), _stream())
+    return act
+
+
+@torch.no_grad()
+def render_cuda_exact_with_coverage(means, conics, colors, radii, H: int, W: int,
+                                    opacities=None, eps: float = DEFAULT_EPS,
+                                    support_fade: bool = False, sigma_cutoff: float = 3.0,
+                                    tile_size: int = RENDER_TILE):
+    """Normalized RGB and the raw coverage (opacity-weighted weight sum, no ε) from one
+    forward (cuda_render.py:229-253); inference only."""
+    if not means.is_cuda:
+        raise RuntimeError("joint CUDA rendering requires CUDA tensors")
+    if any(t.dtype != torch.float32 for t in (means, conics, colors)):
+        raise RuntimeError("joint CUDA rendering requires float32 tensors")
+    eps = validate_eps(eps)
+    _check_shapes(means, conics, colors, radii, opacities)
+    if opacities is not None and opacities.numel() == 0:
+        opacities = None
+    n = means.shape[0]
+    alpha = resolve_fade_alpha(support_fade, None)
+    tail = fade_tail(sigma_cutoff, alpha)
+    rec = pack_records(means.contiguous(), conics.contiguous(), colors.contiguous(),
+                       radii.contiguous(), None if opacities is None else opacities.contiguous(),
+                       H, W)
+    index = index_from_records(rec, n, H, W, tile_size, alpha >= 1.0, sigma_cutoff)
+    return _forward(rec, n, index, H, W, True, eps, tail, means.device)
+
+
+class _RawWeightMap(Function):
+    """den(p) = Σ_i o_i · visible_weight_i(p) over each Gaussian's clipped support, flattened to
+    (H·W,), differentiable w.r.t. means, conics and opacities (fit.py:338-367)."""
+
+    @staticmethod
+    def forward(ctx, means, conics, radii, opacities, H, W, tail, cull, sigma_cutoff, tile_size):
+        n = means.shape[0]
+        means, conics = means.contiguous(), conics.contiguous()
+        has_op = opacities is not None
+        rec = pack_records(means, conics, conics, radii.contiguous(),
+                           opacities.contiguous() if has_op else None, H, W)
+        index = index_from_records(rec, n, H, W, tile_size, cull, sigma_cutoff)
+        _, den = _forward(rec, n, index, H, W, False, 1.0, tail, means.device)
+        ctx.save_for_backward(rec, index.gids, index.offsets, index.status)
+        ctx.meta = (n, H, W, tile_size, tail, has_op)
+        return den.view(-1)
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, grad_den):
+        rec, gids, offsets, status = ctx.saved_tensors
+        n, H, W, ts, tail, has_op = ctx.meta
+        if n == 0 or H * W == 0:
+            return (None,) * 10
+        dev = grad_den.device
+        pixel_grad = torch.zeros(H * W, 4, device=dev, dtype=torch.float32)
+        pixel_grad[:, 3] = grad_den.reshape(-1).to(torch.float32)
+        cap = int(gids.numel())
+        ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n, cap, H, W, 0)
+        ws = torch.zeros(max(ws_bytes // 4, 4), device=dev, dtype=torch.float32)
+        _native.call("ss_render_backward_moments", None, _p(pixel_grad), _p(rec), n, None, None,
+                     _p(gids), cap, _p(offsets), H, W, ts, 0, 1.0, float(tail), 0, _p(ws),
+                     ws_bytes, _p(status), _stream())
+        g_means = torch.empty(n, 2, device=dev)
+        g_conics = torch.empty(n, 3, device=dev)
+        g_colors = torch.empty(n, 3, device=dev)
+        g_opac = torch.empty(n, device=dev) if has_op else None
+        _native.call("ss_render_backward_finalize", _p(rec), n, _p(gids), cap, _p(offsets), H, W,
+                     ts, int(has_op), 0, _p(ws), _p(g_means), _p(g_conics), _p(g_colors),
+                     _p(g_opac), _stream())
+        need = ctx.needs_input_grad
+        return (g_means if need[0] else None, g_conics if need[1] else None, None,
+                g_opac if (has_op and need[3]) else None) + (None,) * 6
+
+
+def raw_weight_map(means, conics, radii, H: int, W: int, opacities=None,
+                   sigma_cutoff: float = 3.0, support_fade: bool = False,
+                   support_fade_alpha: float | None = None, tile_size: int = RENDER_TILE):
+    """Differentiable (H·W,) raw opacity-weighted weight sum Σ_i o_i G_i(p) — the accumulation
+    behind the reference's mask and coverage losses (``_raw_weight_map_field``, fit.py:338-367),
+    with the renderer's support window and fade."""
+    _check_cuda_f32(means, conics, conics)
+    if opacities is not None and opacities.numel() == 0:
+        opacities = None
+    alpha = resolve_fade_alpha(support_fade, support_fade_alpha)
+    tail = fade_tail(sigma_cutoff, alpha)
+    return _RawWeightMap.apply(means, conics, radii, opacities, int(H), int(W), tail,
+                               alpha >= 1.0, float(sigma_cutoff), int(tile_size))

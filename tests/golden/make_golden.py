@@ -157,10 +157,36 @@ def placement_cases(ref, make_target):
             rotations=g.rotations.detach().numpy(), colors=g.colors.detach().numpy())
 
 
+def passes_cases(ref):
+    """gaussian_activity and _raw_weight_map_field fixtures (render.py:417-442, fit.py:338-367)."""
+    import torch
+    H, W = 30, 34
+    for name, alpha, seed in (("plain", 0.0, 61), ("fade", 1.0, 62), ("frac", 0.5, 63)):
+        g = _field(ref, seed, 40, H, W, 0.6, 5.0, 4.0, opac_range=(0.2, 1.0))
+        conics = g.conics()
+        radii = g.radii(3.0)
+        act = ref.render.gaussian_activity(g.means.detach(), conics.detach(), radii, H, W,
+                                           support_fade=alpha > 0, support_fade_alpha=alpha)
+        cfg = ref.config.FitConfig(support_fade=alpha > 0)
+        g.trainable()
+        den = ref.fit._raw_weight_map_field(g, cfg, H, W, support_fade_alpha=alpha)
+        G = torch.as_tensor(np.random.default_rng(seed).normal(size=H * W), dtype=den.dtype)
+        params = [g.means, g.log_scales, g.rotations, g.opacities]
+        grads = torch.autograd.grad((den * G).sum(), params)
+        np.savez_compressed(
+            HERE / f"pass_{name}.npz", H=H, W=W, fade_alpha=alpha,
+            means=g.means.detach().numpy(), log_scales=g.log_scales.detach().numpy(),
+            rotations=g.rotations.detach().numpy(), opacity_logits=g.opacities.detach().numpy(),
+            conics=conics.detach().numpy(), radii=radii.numpy(), activity=act.numpy(),
+            den=den.detach().numpy(), G=G.numpy(),
+            **{f"g_{k}": v.numpy() for k, v in zip(
+                ("means", "log_scales", "rotations", "opacity_logits"), grads)})
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-src", default="/root/reference/src")
-    ap.add_argument("--only", choices=["placement"], default=None,
+    ap.add_argument("--only", choices=["placement", "passes"], default=None,
                     help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
     sys.path.insert(0, args.reference_src)
@@ -169,6 +195,7 @@ def main() -> None:
     import structsplat.config
     import structsplat.cuda_render
     import structsplat.density
+    import structsplat.fit
     import structsplat.gaussians
     import structsplat.init
     import structsplat.render
@@ -180,12 +207,19 @@ def main() -> None:
         config = structsplat.config
         cuda_render = structsplat.cuda_render
         density = structsplat.density
+        fit = structsplat.fit
         gaussians = structsplat.gaussians
         init = structsplat.init
         render = structsplat.render
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "passes":
+        for old in HERE.glob("pass_*.npz"):
+            old.unlink()
+        passes_cases(Ref)
+        print("wrote", len(list(HERE.glob("pass_*.npz"))), "pass fixtures")
+        return
     if args.only == "placement":
         for old in HERE.glob("pl_*.npz"):
             old.unlink()
@@ -276,6 +310,7 @@ def main() -> None:
                    color_space="rgb")
     structure_case(Ref, "tiny_5x3", make_target(5, 3, seed=4), grad_sigma=1.0, tensor_sigma=2.0)
     placement_cases(Ref, make_target)
+    passes_cases(Ref)
     print("wrote", len(list(HERE.glob("*.npz"))), "fixtures")
 
 
