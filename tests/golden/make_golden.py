@@ -183,10 +183,51 @@ def passes_cases(ref):
                 ("means", "log_scales", "rotations", "opacity_logits"), grads)})
 
 
+def fit_case(ref, make_field, make_target):
+    """The plain fit of the CPU benchmark case (256², 4,096 Gaussians, 100 Adam steps at lr 1e-2,
+    pixel MSE, normalized renderer) with the reference's own modules: render_field, the field's
+    parameter groups in torch.optim.Adam, and the post-step log-scale clamp (fit.py:3033,
+    3359-3366).  Records the PSNR of the pre-step render every 10 steps and after the last."""
+    import math
+    import torch
+    H = W = 256
+    f = make_field(H, W, 4096, seed=71)
+    target = torch.as_tensor(make_target(H, W, seed=72))
+    g = ref.gaussians.GaussianField(*[torch.as_tensor(getattr(f, k)).clone() for k in
+                                      ("means", "log_scales", "rotations", "colors",
+                                       "opacity_logits")]).trainable()
+    opt = torch.optim.Adam(g.parameter_groups(1e-2, 1e-2, 1e-2, 1e-2, 1e-2))
+    lo, hi = math.log(0.35), math.log(max(H, W))
+    psnr = []
+
+    def render():
+        return ref.render.render_field(g.means, g.conics(), g.colors, g.radii(3.0), H, W,
+                                       mode="normalized", opacities=g.opacity_values())
+    for it in range(100):
+        img = render()
+        loss = ((img - target) ** 2).mean(dim=2).mean()
+        if it % 10 == 0:
+            psnr.append(10 * math.log10(1.0 / float(((img.detach() - target) ** 2).mean())))
+        opt.zero_grad(set_to_none=True)
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            g.log_scales.clamp_(max=hi)
+            g.log_scales.clamp_(min=lo)
+    with torch.no_grad():
+        img = render()
+    psnr.append(10 * math.log10(1.0 / float(((img - target) ** 2).mean())))
+    np.savez_compressed(HERE / "fit_plain_256_4096.npz", seed_field=71, seed_target=72,
+                        psnr=np.array(psnr), **{k: getattr(g, a).detach().numpy() for k, a in (
+                            ("means", "means"), ("log_scales", "log_scales"),
+                            ("rotations", "rotations"), ("colors", "colors"),
+                            ("opacity_logits", "opacities"))})
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-src", default="/root/reference/src")
-    ap.add_argument("--only", choices=["placement", "passes"], default=None,
+    ap.add_argument("--only", choices=["placement", "passes", "fit"], default=None,
                     help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
     sys.path.insert(0, args.reference_src)
@@ -214,6 +255,10 @@ def main() -> None:
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "fit":
+        fit_case(Ref, make_field, make_target)
+        print("wrote the fit fixture")
+        return
     if args.only == "passes":
         for old in HERE.glob("pass_*.npz"):
             old.unlink()
@@ -311,6 +356,7 @@ def main() -> None:
     structure_case(Ref, "tiny_5x3", make_target(5, 3, seed=4), grad_sigma=1.0, tensor_sigma=2.0)
     placement_cases(Ref, make_target)
     passes_cases(Ref)
+    fit_case(Ref, make_field, make_target)
     print("wrote", len(list(HERE.glob("*.npz"))), "fixtures")
 
 

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import math
 
+import numpy as np
 import pytest
 import torch
 
@@ -260,3 +261,31 @@ def test_fit_forward_loss_gradient_matches_autograd(loss):
     assert abs(float(plan.loss[0, 0]) - lval) <= 1e-5 * abs(lval)
     mse = float(((image.view(H, W, 3) - target) ** 2).mean())
     assert abs(float(plan.loss[0, 1]) - mse) <= 1e-5 * mse
+
+
+@pytest.mark.parametrize("deterministic", [True, False])
+def test_plain_fit_reaches_the_reference_psnr_trajectory(deterministic):
+    """The CPU benchmark's plain fit (256², 4,096 Gaussians, 100 Adam steps at lr 1e-2, pixel
+    MSE) run by the reference itself (fixture fit_plain_256_4096): every 10 steps our fused,
+    graph-free iteration matches its PSNR within 0.01 dB."""
+    require_cuda()
+    from conftest import golden
+    z = golden("fit_plain_256_4096.npz")
+    H = W = 256
+    target = torch.tensor(make_target(H, W, seed=int(z["seed_target"])), device="cuda")
+    field = _field(H, W, 4096, seed=int(z["seed_field"]))
+    batch = Batch([(H, W)], [4096])
+    s = FitSettings.uniform_lr(1e-2, deterministic=deterministic)
+    plan = FitPlan(batch, Batch.concat_fields([field]), batch.concat_images([target]), s)
+    psnr = []
+    for it in range(100):
+        if it % 10 == 0:
+            _, loss = plan.render()
+            psnr.append(10 * math.log10(1.0 / float(loss[0, 1])))
+        plan.step()
+    _, loss = plan.render()
+    psnr.append(10 * math.log10(1.0 / float(loss[0, 1])))
+    assert not plan.overflowed()
+    diff = np.abs(np.array(psnr) - z["psnr"])
+    print("PSNR", np.round(psnr, 4).tolist(), "max |diff| dB", float(diff.max()))
+    assert diff.max() <= 0.01
