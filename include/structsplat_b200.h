@@ -303,6 +303,36 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
 int ss_gaussian_activity(const void* records, int64_t n, float fade_tail, int lanes_per_gaussian,
                          float* activity, ss_stream_t stream);
 
+/* ---------------------------------------------------------------- SSPL1 field decode
+ * The integer streams of an SSPL1 container (codec.py:235-391), inflated on the host (zlib /
+ * PNG), in device memory; the header's JSON fields are copied into this struct.  Values are
+ * 1, 2 or 4 bytes each by bit depth, little-endian; means may be byte-planar.  Layout: means
+ * (x for all Gaussians, then y), scales likewise, rotation, colours (r, g, b planes), opacity
+ * (optional, probabilities).  Morton-ordered means and delta colours are modular deltas. */
+typedef struct ss_sspl1_streams {
+  int64_t n;
+  const uint8_t* means;
+  int means_bits, means_byte_planar, morton;
+  double means_lo[2], means_hi[2];
+  const uint8_t* scales;
+  int scale_bits;
+  double scale_lo[2], scale_hi[2];
+  const uint8_t* rotations;
+  int rot_bits, rot_circular;
+  const uint8_t* colors;
+  int color_bits, color_delta;
+  double color_lo[3], color_hi[3];
+  const uint8_t* opacities;  /* NULL: the container has no opacity stream */
+  int opacity_bits;
+} ss_sspl1_streams;
+int ss_sspl1_workspace_bytes(int64_t n, size_t* bytes);
+/* Writes means (n,2), log_scales (n,2), rotations (n), colors (n,3) and, with an opacity
+ * stream, opacity logits (n), all f32, bit-identical to the reference's decode except the
+ * logit (log of a float32 ratio, within 2 ulp). */
+int ss_sspl1_dequantize(const ss_sspl1_streams* streams, float* means, float* log_scales,
+                        float* rotations, float* colors, float* opacity_logits, void* workspace,
+                        size_t workspace_bytes, ss_stream_t stream);
+
 /* ---------------------------------------------------------------- reference-shaped calls
  * One-call equivalents of the reference extension's entry points, taking its tensor
  * contract (render_ext.cpp:89-137).  They pack records into `workspace` (size from

@@ -28,6 +28,18 @@ class SsBatch(ctypes.Structure):
                 ("gaussian_image", _vp), ("tile_image", _vp)]
 
 
+class SsSspl1Streams(ctypes.Structure):
+    """``ss_sspl1_streams`` of the C header."""
+    _fields_ = [("n", ctypes.c_int64), ("means", _vp), ("means_bits", ctypes.c_int),
+                ("means_byte_planar", ctypes.c_int), ("morton", ctypes.c_int),
+                ("means_lo", _f64 * 2), ("means_hi", _f64 * 2), ("scales", _vp),
+                ("scale_bits", ctypes.c_int), ("scale_lo", _f64 * 2), ("scale_hi", _f64 * 2),
+                ("rotations", _vp), ("rot_bits", ctypes.c_int), ("rot_circular", ctypes.c_int),
+                ("colors", _vp), ("color_bits", ctypes.c_int), ("color_delta", ctypes.c_int),
+                ("color_lo", _f64 * 3), ("color_hi", _f64 * 3), ("opacities", _vp),
+                ("opacity_bits", ctypes.c_int)]
+
+
 _bp = ctypes.POINTER(SsBatch)
 _pp = ctypes.POINTER(_vp)
 _dp = ctypes.POINTER(_f64)
@@ -91,6 +103,9 @@ SIGNATURES = {
     "ss_sample_candidates": [_vp, _int, _int, _vp, _i64, _vp, _vp, _vp, ctypes.c_size_t, _vp],
     "ss_place_gaussians": [_vp, _i64, _vp, _vp, _vp, _vp, _int, _int, _int, _f64, _f64, _f64,
                            _i64, _vp, _vp, _vp, _vp, _vp],
+    "ss_sspl1_workspace_bytes": [_i64, _szp],
+    "ss_sspl1_dequantize": [ctypes.POINTER(SsSspl1Streams), _vp, _vp, _vp, _vp, _vp, _vp,
+                            ctypes.c_size_t, _vp],
     "ss_structure_tensor_workspace_bytes": [_int, _int, _int, _szp],
     "ss_structure_tensor": [_vp, _int, _int, _int, _vp, _int, _vp, _int, _int, _int, _f64, _f64,
                             _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp],

@@ -224,15 +224,50 @@ def fit_case(ref, make_field, make_target):
                             ("opacity_logits", "opacities"))})
 
 
+def codec_cases(ref, make_field, make_target):
+    """SSPL1 containers written by the reference's codec.encode, with its decode and
+    decode_and_render results (codec.py:235-500)."""
+    import torch
+    H, W = 48, 64
+    cases = [
+        ("default_opacity", dict(), True, False),
+        ("plain_noopacity", dict(morton_reorder=False, color_delta=False,
+                                 means_byte_planar=False, rot_circular=False, bits_means=12,
+                                 bits_scales=10, bits_rot=9, bits_colors=7), False, False),
+        ("png_alpha", dict(stream_codec="png", bits_opacity=6), True, True),
+    ]
+    for k, (name, kw, with_opacity, with_alpha) in enumerate(cases):
+        f = make_field(H, W, 400, seed=81 + k)
+        g = ref.gaussians.GaussianField(
+            torch.as_tensor(f.means), torch.as_tensor(f.log_scales), torch.as_tensor(f.rotations),
+            torch.as_tensor(f.colors),
+            torch.as_tensor(f.opacity_logits) if with_opacity else None)
+        alpha = make_target(H, W, seed=90 + k)[..., 0] if with_alpha else None
+        blob = ref.codec.encode(g, H, W, ref.codec.CodecConfig(**kw), alpha=alpha)
+        d = ref.codec.decode(blob)
+        img = ref.codec.decode_and_render(blob)
+        out = dict(blob=np.frombuffer(blob, dtype=np.uint8), H=H, W=W,
+                   means=d.means.numpy(), log_scales=d.log_scales.numpy(),
+                   rotations=d.rotations.numpy(), colors=d.colors.numpy(),
+                   image=img.detach().numpy())
+        if d.opacities is not None:
+            out["opacity_logits"] = d.opacities.numpy()
+        a = ref.codec.decode_alpha(blob)
+        if a is not None:
+            out["alpha"] = a
+        np.savez_compressed(HERE / f"codec_{name}.npz", **out)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-src", default="/root/reference/src")
-    ap.add_argument("--only", choices=["placement", "passes", "fit"], default=None,
+    ap.add_argument("--only", choices=["placement", "passes", "fit", "codec"], default=None,
                     help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
     sys.path.insert(0, args.reference_src)
     sys.path.insert(0, str(REPO))
     import torch
+    import structsplat.codec
     import structsplat.config
     import structsplat.cuda_render
     import structsplat.density
@@ -245,6 +280,7 @@ def main() -> None:
     from structsplat_b200.synthetic import make_field, make_target
 
     class Ref:
+        codec = structsplat.codec
         config = structsplat.config
         cuda_render = structsplat.cuda_render
         density = structsplat.density
@@ -255,6 +291,12 @@ def main() -> None:
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "codec":
+        for old in HERE.glob("codec_*.npz"):
+            old.unlink()
+        codec_cases(Ref, make_field, make_target)
+        print("wrote", len(list(HERE.glob("codec_*.npz"))), "codec fixtures")
+        return
     if args.only == "fit":
         fit_case(Ref, make_field, make_target)
         print("wrote the fit fixture")
@@ -357,6 +399,7 @@ def main() -> None:
     placement_cases(Ref, make_target)
     passes_cases(Ref)
     fit_case(Ref, make_field, make_target)
+    codec_cases(Ref, make_field, make_target)
     print("wrote", len(list(HERE.glob("*.npz"))), "fixtures")
 
 

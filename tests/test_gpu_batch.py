@@ -196,7 +196,8 @@ def test_graph_fit_equals_eager_fit_and_counts_steps():
     for k in PARAM_NAMES:
         assert torch.equal(a[k], b[k]), k
     assert int(ha["plan"].step_state[0]) == 25
-    assert ha["final_psnr"] == hb["final_psnr"]
+    # the per-image loss is summed with float atomics (any order): equal to float rounding
+    assert abs(ha["final_psnr"][0] - hb["final_psnr"][0]) <= 1e-4
 
 
 def test_fit_replans_when_the_index_outgrows_its_capacity():

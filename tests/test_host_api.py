@@ -105,3 +105,13 @@ def test_shape_validation_happens_before_launch():
     m, c, col, r = _cpu_field()
     with pytest.raises(RuntimeError, match="requires CUDA tensors"):
         R.build_tile_index(m, c, r, 8, 8, 4)
+
+
+def test_codec_header_rejects_non_containers():
+    import pytest as _pytest
+    from structsplat_b200 import codec
+    with _pytest.raises(ValueError):
+        codec.blob_header(b"NOPE0" + b"\x00" * 8)
+    from conftest import golden
+    h = codec.blob_header(golden("codec_default_opacity.npz")["blob"].tobytes())
+    assert h["n"] == 400 and h["H"] == 48 and h["W"] == 64 and h["has_opacity"]
