@@ -35,7 +35,7 @@ sys.path.insert(0, str(REPO))
 METRIC = "fwd+bwd ms/iter (1024², 100k Gaussians); batched fit img/s vs plain kernel"
 WORKLOAD = {"H": 1024, "W": 1024, "N": 100_000, "seed": 0, "mode": "normalized"}
 PAIR_SLOTS_FWD, PAIR_SLOTS_BWD = 14, 40   # FP32 issue slots per in-rectangle pair (reference)
-BACKWARD_DRAM_BYTES = 40_239_360 + 2_560  # one backward_kernel launch at this workload (ncu)
+BACKWARD_DRAM_BYTES = 40_236_288 + 512  # one backward_kernel launch at this workload (ncu)
 SM_COUNT, FP32_LANES = 148, 128
 
 
@@ -505,6 +505,8 @@ def run_stress(args, dev):
     plan = FitPlan(batch, params, target.reshape(-1, 3).contiguous(), settings)
     counts = (plan.offsets[1:] - plan.offsets[:-1]).to(torch.int64)
     entries = int(plan.offsets[-1].item())
+    host = {"log_scales": f.log_scales, "rotations": f.rotations, "means": f.means}
+    pairs = pair_count(host, {"H": H, "W": W})
     _, loss0 = plan.render()
     step = GraphStep(plan)
     for _ in range(args.warmup):
@@ -525,6 +527,10 @@ def run_stress(args, dev):
                         "(aspect U[5,50]) along structure-tensor orientation (sigma 1, rho 3); "
                         "deterministic two-pass backward; Adam fit iteration in one CUDA graph",
             "ms_per_step": round(ms, 3), "steps": K, "warmup": args.warmup,
+            "pairs": pairs, "gpairs_per_s": round(pairs / (ms * 1e-3) / 1e9, 2),
+            "step_roofline_frac": round(pairs * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (
+                SM_COUNT * FP32_LANES * (measured_peaks().get("sm_max_mhz") or 1965.0) * 1e6)
+                / (ms * 1e-3), 4),
             "tile_entries": entries, "tile_list_max": int(counts.max()),
             "tile_list_median": float(counts.float().median()),
             "psnr_start": round(psnr_from_mse(float(loss0[0, 1])), 3),
