@@ -331,21 +331,25 @@ def _batch_target(args):
     return make_target(H, W, seed=seed)
 
 
-def batched_workload(images=BATCH_IMAGES, seed=BATCH_SEED):
+def batched_workload(images=BATCH_IMAGES, seed=BATCH_SEED, rank=0, world=1):
     """The batched-fit workload: image sizes drawn uniformly from BATCH_SIZES, 0.1 Gaussians per
-    pixel, seeded targets and fields (targets built in a spawn pool: no fork after CUDA init)."""
+    pixel, seeded targets and fields (targets built in a spawn pool: no fork after CUDA init).
+    With several ranks each builds only its share of the images (``shard_images``)."""
     import multiprocessing as mp
     from concurrent.futures import ProcessPoolExecutor
+    from structsplat_b200.replicas import shard_images
     from structsplat_b200.synthetic import make_field
     rng = np.random.default_rng(seed)
-    sizes = [BATCH_SIZES[int(k)] for k in rng.integers(0, len(BATCH_SIZES), images)]
+    all_sizes = [BATCH_SIZES[int(k)] for k in rng.integers(0, len(BATCH_SIZES), images)]
+    mine = shard_images(all_sizes, rank, world)
+    sizes = [all_sizes[b] for b in mine]
     counts = [int(round(BATCH_DENSITY * h * w)) for h, w in sizes]
-    jobs = [(h, w, seed * 1000 + 2 * b) for b, (h, w) in enumerate(sizes)]
+    jobs = [(h, w, seed * 1000 + 2 * b) for b, (h, w) in zip(mine, sizes)]
     with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
                              mp_context=mp.get_context("spawn")) as pool:
         targets = list(pool.map(_batch_target, jobs))
     fields = [make_field(h, w, n, seed=seed * 1000 + 2 * b + 1)
-              for b, ((h, w), n) in enumerate(zip(sizes, counts))]
+              for b, (h, w), n in zip(mine, sizes, counts)]
     return sizes, counts, targets, fields
 
 
@@ -413,24 +417,33 @@ def run_batched(args, dev, workload):
     t_loop_graph = timed(lambda: [g.replay() for g in graphs], K)
     del graphs, plans
 
+    # ranks fit disjoint shares of the images: the job is as slow as its slowest rank
+    from structsplat_b200.replicas import max_over_ranks, sum_over_ranks
+    t_batch, t_loop, t_loop_graph, dpsnr = max_over_ranks(
+        [t_batch, t_loop, t_loop_graph,
+         float(np.max(np.abs(np.array(psnr_b) - np.array(psnr_l))))], device=dev)
+    B_all, px_all, g_all, e_all, psum = sum_over_ranks(
+        [B, batch.pixels, batch.n, entries, float(np.sum(psnr_b))], device=dev)
+    B_all = int(B_all)
     res = {
-        "workload": f"{B} images, sizes uniform over {{256x256, 512x512, 768x512, 1024x1024, "
+        "workload": f"{B_all} images, sizes uniform over {{256x256, 512x512, 768x512, 1024x1024, "
                     f"2048x1536}} (WxH), 0.1 Gaussians/px, seeded generator targets; "
                     f"normalized, pixel MSE, Adam (reference per-group lrs)",
-        "images": B, "pixels": int(batch.pixels), "gaussians": int(batch.n),
-        "tile_entries": entries, "steps": K, "warmup": Wm,
-        "batched_img_s": round(B * K / (t_batch * 1e-3), 1),
+        "images": B_all, "pixels": int(px_all), "gaussians": int(g_all),
+        "tile_entries": int(e_all), "steps": K, "warmup": Wm,
+        "scaling": "strong (the images are split across ranks)",
+        "batched_img_s": round(B_all * K / (t_batch * 1e-3), 1),
         "batched_ms_per_step": round(t_batch / K, 3),
-        "loop_eager_img_s": round(B * K / (t_loop * 1e-3), 1),
-        "loop_graph_img_s": round(B * K / (t_loop_graph * 1e-3), 1),
-        "psnr_batched_mean": round(float(np.mean(psnr_b)), 4),
-        "psnr_max_abs_diff_vs_loop": round(float(np.max(np.abs(np.array(psnr_b)
-                                                               - np.array(psnr_l)))), 6),
+        "loop_eager_img_s": round(B_all * K / (t_loop * 1e-3), 1),
+        "loop_graph_img_s": round(B_all * K / (t_loop_graph * 1e-3), 1),
+        "psnr_batched_mean": round(psum / max(B_all, 1), 4),
+        "psnr_max_abs_diff_vs_loop": round(dpsnr, 6),
         "psnr_after_steps": Wm + K, "index_overflow": overflow,
         "gpu_launches_per_step": 9, "peak_mem_gb": round(mem_gb, 2), "clocks": clocks.summary(),
     }
     res["speedup_vs_loop_eager"] = round(res["batched_img_s"] / res["loop_eager_img_s"], 3)
-    if not args.no_ref_cuda:
+    world = torch.distributed.get_world_size() if torch.distributed.is_initialized() else 1
+    if not args.no_ref_cuda and world == 1:
         res["reference_loop"] = ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev,
                                                   steps=args.ref_batch_steps)
         if "img_s" in res["reference_loop"]:
@@ -654,16 +667,23 @@ def main():
         print(json.dumps({key: fn(args, dev)}), flush=True)
         return
     workload = None
-    if world == 1 and (args.batched_only or not args.no_batched) and not args.profile:
-        workload = batched_workload()  # spawn pool before the first CUDA call
+    if (args.batched_only or not args.no_batched) and not args.profile:
+        # spawn pool before the first CUDA call; each rank builds its share of the images
+        workload = batched_workload(rank=rank, world=world)
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
     if args.batched_only:
-        print(json.dumps({"batched": run_batched(args, dev, workload)}), flush=True)
+        batched = run_batched(args, dev, workload)
+        if rank == 0:
+            print(json.dumps({"batched": batched}), flush=True)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
         return
     res = run_ours(args, rank, world, dev)
     if res is None:
         return
+    batched = run_batched(args, dev, workload) if workload is not None else None
     host = res.pop("host")
     peaks = measured_peaks()
     P = pair_count(host) if rank == 0 else 0
@@ -714,8 +734,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline(host)
         if world == 1 and not args.no_ref_cuda:
             line["reference_cuda_ms"] = ref_cuda_baseline(host, dev)
-        if workload is not None:
-            line["batched"] = run_batched(args, dev, workload)
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
