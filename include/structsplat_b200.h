@@ -163,7 +163,7 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
                       float* den, uint32_t* status, ss_stream_t stream);
 
 /* Launch tuning (process-wide, used by the autotuner): warps per backward CTA for a render
- * tile size — 4 or 8 for tile 16, 8 or 16 for tile 32, 0 restores the default (8 / 16).
+ * tile size — 4 or 8 for tile 16, 8 or 16 for tile 32, 0 restores the default (8 for both).
  * Results do not depend on it.  ss_get_backward_warps returns the value in effect (-1 for an
  * unsupported tile size). */
 int ss_set_backward_warps(int tile_size, int warps);

@@ -13,9 +13,11 @@
 //
 // Backward (render_ext.cu:696-847 contract): a prologue turns grad_out, out and den into the
 // per-pixel (dnum_r, dnum_g, dnum_b, dden) of the tile in shared memory (the fit path hands
-// them over ready-made).  Work is then Gaussian-major: one warp per staged Gaussian walks
-// exactly the pixels of its support rectangle inside the tile — lane (c, s) takes columns c,
-// c+8, … and the s-th quarter of the rows — and accumulates nine moments
+// them over ready-made).  Work is then Gaussian-major: four lanes own one staged Gaussian and
+// walk exactly the pixels of its support rectangle inside the tile — lane q takes columns q,
+// q+4, … and runs down each column — so a warp works on eight Gaussians at once.  A counting
+// sort orders the staged entries by their loop trip counts first, so the eight Gaussians of a
+// warp need nearly the same number of iterations.  Each Gaussian accumulates nine moments
 //   R_k = Σ base·dnum_k,  G = Σ base·dw,  S1 = Σ t dx,  S2 = Σ t dy,  S3 = Σ t dx²,
 //   S4 = Σ t dx dy,  S5 = Σ t dy²,     dw = dnum·c + dden,  t = raw·dw (0 where the fade clamps)
 // from which
@@ -23,10 +25,11 @@
 //   dL/dc = -o S5/2,  dL/dc_k = o R_k,  dL/do = G,
 // i.e. the reference's per-pixel formulas (render_ext.cu:785-818) summed over pixels.  Along a
 // column dx is constant, so S1, S3 and S4 fold into per-column products.  The moments are
-// reduce-scattered over the warp (one moment per lane) and added with one atomic per moment into
-// per-Gaussian accumulators (fast mode), or stored per (tile, Gaussian) entry and summed per
-// Gaussian in ascending tile order by a second kernel (deterministic mode).  A per-Gaussian
-// epilogue applies o, a, b, c once.
+// reduce-scattered over the four lanes and added with one atomic per moment into per-Gaussian
+// accumulators (fast mode), or stored per (tile, Gaussian) entry and summed per Gaussian in
+// ascending tile order by a second kernel (deterministic mode: every entry is computed by its
+// own four lanes in a fixed order, so the result does not depend on the scheduling).  A
+// per-Gaussian epilogue applies o, a, b, c once.
 #include <atomic>
 
 #include "ss_common.cuh"
@@ -285,31 +288,6 @@ __device__ __forceinline__ void scatter_level(const float (&v)[N], float (&w)[K]
   }
 }
 
-// Reduce-scatter of the nine moments over the 32 lanes of a warp: after the xor butterflies
-// 16, 8, 4, 2, 1 lane l holds the warp total of moment moment_of_lane(l) (or nothing, -1).
-__device__ __forceinline__ float reduce_scatter9(const float (&v)[kMoments], int lane) {
-  float a[5], b[3], c[2], d[1];
-  scatter_level<9, 5>(v, a, lane & 16, 16);  // 0-4 | 5-8
-  scatter_level<5, 3>(a, b, lane & 8, 8);    // 0-2 | 3-4
-  scatter_level<3, 2>(b, c, lane & 4, 4);    // 0-1 | 2
-  scatter_level<2, 1>(c, d, lane & 2, 2);    // 0   | 1
-  return d[0] + __shfl_xor_sync(0xffffffffu, d[0], 1);
-}
-
-// Which moment lane l holds after reduce_scatter9 (-1: none); only even lanes report.
-__device__ __forceinline__ int moment_of_lane(int lane) {
-  const int b16 = (lane >> 4) & 1, b8 = (lane >> 3) & 1, b4 = (lane >> 2) & 1,
-            b2 = (lane >> 1) & 1;
-  int slot;
-  if (!b8) slot = b4 ? (b2 ? -1 : 2) : b2;  // slots 0, 1, 2
-  else slot = b4 ? -1 : 3 + b2;              // slots 3, 4
-  if (slot < 0) return -1;
-  const int m = b16 ? 5 + slot : slot;
-  return (m < kMoments && (lane & 1) == 0) ? m : -1;
-}
-
-// Backward of one tile.  PIXGRAD: the per-pixel inputs come ready-made from the fit forward
-// (pixel_grad); otherwise they are formed from grad_out, out and den.
 template <int TS, int NT>
 struct BackwardOccupancy {  // CTAs per SM the register budget is planned for
   static constexpr int kBlocks = TS == 16 ? (NT == 128 ? 6 : 4) : (NT == 256 ? 4 : 2);
@@ -324,9 +302,12 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
                     int normalize, float eps, float tail, float* __restrict__ moments,
                     float* __restrict__ partials, uint32_t* status) {
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
+  constexpr int kHalf = kStageMax / 2;  // entries per chunk when a long list streams through
   __shared__ __align__(16) float4 stage[kStageMax][4];
   __shared__ float4 pix[TS * TS];
   __shared__ int stage_gid[kStageMax];
+  __shared__ int order[kStageMax];
+  __shared__ int class_count[64];
   const int tile = blockIdx.x;
   const Frame fr = frame_of_tile(frames, tile, n);
   const int local = tile - fr.first_tile;
@@ -352,93 +333,152 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     pix[q] = v;
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int my_moment = moment_of_lane(lane);
-  const int col_slot = lane & 7, row_seg = lane >> 3;
+  const int member = lane >> 2, quad = lane & 3;
   const TileList L = tile_list(gids, offsets, cap, fr, tile);
   if (DETERMINISTIC && L.direct) {
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
     return;
   }
-  // One staged Gaussian (entry k0 + j, id gsm[j]) on the whole warp.  Lanes whose column or
-  // rows fall outside the rectangle skip the loops (divergent but exact: they add nothing).
-  auto work = [&](const float4(*st)[4], int j, int64_t k0, const int* gsm) {
-    const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
-    const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
-    const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
-    const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
-    const int seg_rows = (cy1 - cy0 + 3) >> 2;
-    const int ry0 = cy0 + row_seg * seg_rows;
-    const int rows = max(min(seg_rows, cy1 - ry0), 0);
-    const int passes = (cx1 - cx0 + 7) >> 3;
+  // Order of the staged entries [0, m) by a counting sort into 64 cost classes (loop passes
+  // descending, then rows in fours descending), so the eight Gaussians of a warp have nearly the
+  // same loop trip counts and the heaviest groups start first.  The order within a class comes
+  // from shared-memory atomics and varies from run to run; no result depends on it (every
+  // entry's moments are computed by its own four lanes).
+  auto prepare = [&](const float4(*st)[4], int m, int* ord) {
+    constexpr int kPer = (kStageMax + NT - 1) / NT;  // entries per thread
+    int code[kPer];
+    if (threadIdx.x < 64) class_count[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int t = threadIdx.x + i * NT;
+      code[i] = -1;
+      if (t < m) {
+        const int4 r = *reinterpret_cast<const int4*>(&st[t][3]);
+        const int w = min(r.z - tx0, TS) - max(r.x - tx0, 0);
+        const int h = min(r.w - ty0, TS) - max(r.y - ty0, 0);
+        const int passes = w > 0 && h > 0 ? min((w + 3) >> 2, 8) : 0;
+        const int hb = h > 0 ? min((h - 1) >> 2, 7) : 0;
+        const int cls = passes > 0 ? (8 - passes) * 8 + (7 - hb) : 63;
+        code[i] = (cls << 16) | atomicAdd(&class_count[cls], 1);
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of the 64 class counts
+      const int c0 = class_count[2 * lane], c1 = class_count[2 * lane + 1];
+      int x = c0 + c1;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      const int excl = x - c0 - c1;
+      class_count[2 * lane] = excl;
+      class_count[2 * lane + 1] = excl + c0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kPer; ++i)
+      if (code[i] >= 0) ord[class_count[code[i] >> 16] + (code[i] & 0xffff)] = threadIdx.x + i * NT;
+    __syncthreads();
+  };
+  // Group g of the sorted entries: member k of the warp takes entry ord[8 g + k] with its four
+  // lanes; lane (k, q) walks columns q, q+4, … of the rectangle, each over all its rows.
+  auto work_group = [&](const float4(*st)[4], const int* ord, const int* gsm, int m, int g,
+                        int64_t k0) {
+    const int slot = g * 8 + member;
+    const bool active = slot < m;
+    const int j = active ? ord[slot] : 0;
     float acc[kMoments];
 #pragma unroll
     for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
-    for (int pass = 0; pass < passes; ++pass) {
-      const int cx = cx0 + col_slot + 8 * pass;
-      if (cx < cx1 && rows > 0) {
-        const float dx = (float)(tx0 + cx) - p0.x;
-        const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
-        float tc = 0.f, uc = 0.f;
-        float dy = (float)(ty0 + ry0) - p0.y;
-        int pidx = ry0 * TS + cx;
+    if (active) {
+      const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
+      const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+      const int cx0 = max(r.x - tx0, 0), cx1 = min(r.z - tx0, TS);
+      const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
+      const int rows = cy1 - cy0;
+      const int passes = (cx1 - cx0 + 3) >> 2;
+      const float dy0 = (float)(ty0 + cy0) - p0.y;
+      for (int pass = 0; pass < passes; ++pass) {
+        const int cx = cx0 + quad + 4 * pass;
+        if (cx < cx1 && rows > 0) {
+          const float dx = (float)(tx0 + cx) - p0.x;
+          const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+          float tc = 0.f, uc = 0.f;
+          float dy = dy0;
+          int pidx = cy0 * TS + cx;
 #pragma unroll 1
-        for (int k = 0; k < rows; ++k, dy += 1.0f, pidx += TS) {
-          const float4 g = pix[pidx];
-          const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
-          const float raw = fast_exp2(e);
-          const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
-          const float dw = fmaf(g.x, p1.z, fmaf(g.y, p1.w, fmaf(g.z, p2.x, g.w)));
-          acc[0] = fmaf(base_w, g.x, acc[0]);
-          acc[1] = fmaf(base_w, g.y, acc[1]);
-          acc[2] = fmaf(base_w, g.z, acc[2]);
-          acc[3] = fmaf(base_w, dw, acc[3]);
-          const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
-          const float u = t * dy;
-          tc += t;
-          uc += u;
-          acc[8] = fmaf(u, dy, acc[8]);
+          for (int k = 0; k < rows; ++k, dy += 1.0f, pidx += TS) {
+            const float4 gp = pix[pidx];
+            const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
+            const float raw = fast_exp2(e);
+            const float base_w = FADE ? fmaxf(raw - tail, 0.0f) : raw;
+            const float dw = fmaf(gp.x, p1.z, fmaf(gp.y, p1.w, fmaf(gp.z, p2.x, gp.w)));
+            acc[0] = fmaf(base_w, gp.x, acc[0]);
+            acc[1] = fmaf(base_w, gp.y, acc[1]);
+            acc[2] = fmaf(base_w, gp.z, acc[2]);
+            acc[3] = fmaf(base_w, dw, acc[3]);
+            const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
+            const float u = t * dy;
+            tc += t;
+            uc += u;
+            acc[8] = fmaf(u, dy, acc[8]);
+          }
+          acc[4] = fmaf(dx, tc, acc[4]);
+          acc[5] += uc;
+          acc[6] = fmaf(dx * dx, tc, acc[6]);
+          acc[7] = fmaf(dx, uc, acc[7]);
         }
-        acc[4] = fmaf(dx, tc, acc[4]);
-        acc[5] += uc;
-        acc[6] = fmaf(dx * dx, tc, acc[6]);
-        acc[7] = fmaf(dx, uc, acc[7]);
       }
     }
-    const float total = reduce_scatter9(acc, lane);
-    if (my_moment >= 0) {
-      const int64_t entry = L.first + k0 + j;
-      if (DETERMINISTIC) {
-        partials[entry * kPartialFloats + my_moment] = total;
-      } else {
-        atomicAdd(moments + (int64_t)my_moment * n + gsm[j], total);
+    // reduce-scatter over the member's four lanes: lane q ends with moments
+    // (q&2 ? 5 : 0) + (q&1 ? 3 : 0) + s for s < (q&1 ? 2 : 3), those below 9
+    float a[5], b[3];
+    scatter_level<9, 5>(acc, a, lane & 2, 2);
+    scatter_level<5, 3>(a, b, lane & 1, 1);
+    if (active) {
+      const int base = ((quad & 2) ? 5 : 0) + ((quad & 1) ? 3 : 0);
+      const int cnt = (quad & 1) ? 2 : 3;
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        const int mo = base + s;
+        if (s < cnt && mo < kMoments) {
+          if (DETERMINISTIC)
+            partials[(L.first + k0 + j) * kPartialFloats + mo] = b[s];
+          else
+            atomicAdd(moments + (int64_t)mo * n + gsm[j], b[s]);
+        }
       }
     }
   };
+  auto run = [&](const float4(*st)[4], int m, int* ord, const int* gsm, int64_t k0) {
+    prepare(st, m, ord);
+    const int groups = (m + 7) >> 3;
+    for (int g = warp; g < groups; g += NT / 32) work_group(st, ord, gsm, m, g, k0);
+  };
   if (L.count <= kStageMax) {
-    // whole list staged once; warp w takes entries w, w + warps, … (a static split measured
-    // faster than taking them from a shared counter)
     stage_range<NT>(stage, rec, L, 0, (int)L.count, stage_gid);
     cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    const int count = (int)L.count;
-    for (int j = warp; j < count; j += NT / 32) work(stage, j, 0, stage_gid);
+    run(stage, (int)L.count, order, stage_gid, 0);
   } else {
-    float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
-    const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
-    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0), stage_gid);
+    float4(*buf)[kHalf][4] = reinterpret_cast<float4(*)[kHalf][4]>(stage);
+    const int64_t count = L.count;
+    const int nchunks = (int)((count + kHalf - 1) / kHalf);
+    auto len = [&](int64_t k0) { return (int)(count - k0 < kHalf ? count - k0 : kHalf); };
+    stage_range<NT>(buf[0], rec, L, 0, len(0), stage_gid);
     cp_async_commit();
     for (int c = 0; c < nchunks; ++c) {
-      const int64_t k0 = (int64_t)c * kChunk;
+      const int64_t k0 = (int64_t)c * kHalf;
       if (c + 1 < nchunks)
-        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk),
-                        stage_gid + ((c + 1) & 1) * kChunk);
+        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kHalf, len(k0 + kHalf),
+                        stage_gid + ((c + 1) & 1) * kHalf);
       cp_async_commit();
       cp_async_wait_one();
       __syncthreads();
-      const int m = chunk_len(L.count, k0);
-      for (int j = warp; j < m; j += NT / 32)
-        work(buf[c & 1], j, k0, stage_gid + (c & 1) * kChunk);
+      run(buf[c & 1], len(k0), order + (c & 1) * kHalf, stage_gid + (c & 1) * kHalf, k0);
       __syncthreads();
     }
   }
@@ -571,7 +611,7 @@ void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float
                      float tail, float* ws, uint32_t* status) {
   const int warps = g_backward_warps[TS == 16 ? 0 : 1].load(std::memory_order_relaxed);
   constexpr int kSmall = TS == 16 ? 128 : 256, kLarge = TS == 16 ? 256 : 512;
-  if (warps * 32 == kSmall)
+  if (warps * 32 == kSmall || (TS == 32 && warps == 0))  // tile 32: 8 warps unless asked
     launch_backward_nt<TS, kSmall, PIXGRAD>(T, s, deterministic, grad_out, rec, n, den, out,
                                             pixel_grad, gids, cap, offsets, f, normalize, eps,
                                             tail, ws, status);
@@ -738,7 +778,7 @@ int ss_set_backward_warps(int tile_size, int warps) {
 int ss_get_backward_warps(int tile_size) {
   if (tile_size != 16 && tile_size != 32) return -1;
   const int w = g_backward_warps[tile_size == 16 ? 0 : 1].load(std::memory_order_relaxed);
-  return w ? w : (tile_size == 16 ? 8 : 16);
+  return w ? w : 8;
 }
 
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,

@@ -137,7 +137,7 @@ def test_backward_warps_knob_validation(lib):
     assert rc == 4 and "tile_size" in msg
     rc, msg = _status(lib, "ss_set_backward_warps", 32, 12)
     assert rc == 1 and "0, 8 or 16" in msg
-    assert lib.ss_get_backward_warps(16) == 8 and lib.ss_get_backward_warps(32) == 16
-    assert lib.ss_set_backward_warps(32, 8) == 0 and lib.ss_get_backward_warps(32) == 8
-    assert lib.ss_set_backward_warps(32, 0) == 0 and lib.ss_get_backward_warps(32) == 16
+    assert lib.ss_get_backward_warps(16) == 8 and lib.ss_get_backward_warps(32) == 8
+    assert lib.ss_set_backward_warps(32, 16) == 0 and lib.ss_get_backward_warps(32) == 16
+    assert lib.ss_set_backward_warps(32, 0) == 0 and lib.ss_get_backward_warps(32) == 8
     assert lib.ss_get_backward_warps(7) == -1

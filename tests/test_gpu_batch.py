@@ -164,8 +164,14 @@ def test_fused_fit_step_follows_eager_torch_adam(iters):
     ref = _torch_fit(field, target, iters, settings)
     mine = {k: v.clone() for k, v in field.items()}
     fit_batch([mine], [target], iters=iters, settings=settings, graph=False)
+    # Adam moves each element by about lr * m / (sqrt(v) + eps) per step: where a gradient is
+    # near eps (1e-8) that ratio, and so the step, swings with the last bits of the gradient.
+    # The bar is therefore a fraction of the group's learning rate per element.
+    lrs = dict(zip(PARAM_NAMES, settings.lrs()))
     for k in PARAM_NAMES:
-        assert rel_err(mine[k], ref[k]) <= 1e-5, k
+        dev = float((mine[k] - ref[k]).abs().max()) / lrs[k]
+        assert dev <= 2e-3, (k, dev)
+        assert rel_err(mine[k], ref[k]) <= 5e-5, k
 
 
 def test_batched_fit_matches_single_image_fits():
