@@ -222,9 +222,11 @@ def run_ours(args, rank, world, dev):
 
 
 KERNELS_PER_CALL = {
-    # kernels of this library launched by each entry point (CUB's scan is two kernels)
-    "ss_project_rs": 1, "ss_pack_splats": 1, "ss_tile_index_count": 4, "ss_tile_index_fill": 3,
-    "ss_render_forward": 1, "ss_render_backward": 1, "ss_project_rs_backward": 1,
+    # kernels of this library launched by each entry point (the index count's scan is one
+    # single-CTA kernel up to 16k tiles)
+    "ss_project_rs": 1, "ss_pack_splats": 1, "ss_tile_index_count": 2, "ss_tile_index_fill": 3,
+    "ss_render_forward": 1, "ss_render_backward": 2, "ss_project_rs_backward": 1,
+    "ss_render_backward_moments": 1, "ss_render_backward_finalize_rs": 1,
 }
 
 

@@ -296,6 +296,18 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
                                 const void* workspace, float* grad_means, float* grad_conics,
                                 float* grad_colors, float* grad_opacities, ss_stream_t stream);
 
+/* _finalize straight to the RS field parameters (the epilogue followed by
+ * ss_project_rs_backward, in one pass): grad_means (n,2), grad_log_scales (n,2),
+ * grad_rotations (n), grad_colors (n,3) and, with opacity logits, grad_opacity_logits (n). */
+int ss_render_backward_finalize_rs(const void* records, int64_t n, const int32_t* tile_gids,
+                                   int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                                   int width, int tile_size, int deterministic,
+                                   const void* workspace, const float* log_scales,
+                                   const float* rotations, const float* opacity_logits,
+                                   float dilation, float* grad_means, float* grad_log_scales,
+                                   float* grad_rotations, float* grad_colors,
+                                   float* grad_opacity_logits, ss_stream_t stream);
+
 /* ---------------------------------------------------------------- per-Gaussian passes
  * gaussian_activity (render.py:417-442): activity[g] = sum over the pixels of g's clipped
  * support rectangle of max(exp(-q/2) - fade_tail, 0) (opacity-free), from packed records.

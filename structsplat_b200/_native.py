@@ -69,6 +69,8 @@ SIGNATURES = {
                            _vp],
     "ss_render_backward_moments": [_vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _int,
                                    _int, _int, _f32, _f32, _int, _vp, ctypes.c_size_t, _vp, _vp],
+    "ss_render_backward_finalize_rs": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _vp,
+                                       _vp, _vp, _vp, _f32, _vp, _vp, _vp, _vp, _vp, _vp],
     "ss_gaussian_activity": [_vp, _i64, _f32, _int, _vp, _vp],
     "ss_render_backward_finalize": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _int, _vp,
                                     _vp, _vp, _vp, _vp, _vp],

@@ -5,7 +5,8 @@
 // ascending Gaussian id, which is the order the reference's stable radix sort leaves and makes
 // every downstream sum deterministic.  No sort over all pairs is needed: per-tile counts come
 // from atomics, a device-wide scan gives the offsets, the fill claims slots with per-tile atomic
-// cursors, and a per-tile bitonic sort in shared memory restores ascending ids.
+// cursors, and a per-tile bitonic sort in shared memory restores ascending ids.  The scan is one
+// single-CTA kernel for up to 16,384 tiles and CUB's device scan beyond.
 #include <climits>
 
 #include <cub/device/device_scan.cuh>
@@ -227,6 +228,58 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
     if (pos[k] >= 0 && pos[k] < cap) gids[pos[k]] = owner;
 }
 
+// Offsets of small tile sets in one launch: a single CTA scans up to kSingleScanMax per-tile
+// counts (each thread a contiguous run of kScanPerThread, then a block scan of the run totals)
+// and writes the int64 and the int32 offsets.  Larger tile sets use CUB's device scan.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPerThread = 16;
+constexpr int64_t kSingleScanMax = (int64_t)kScanThreads * kScanPerThread;
+
+__global__ void __launch_bounds__(kScanThreads)
+    single_scan_kernel(const int* __restrict__ tile_count, int64_t items,
+                       long long* __restrict__ off64, int32_t* __restrict__ off32) {
+  __shared__ long long warp_total[kScanThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t base = (int64_t)tid * kScanPerThread;
+  long long run[kScanPerThread];
+  long long sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    const int64_t idx = base + k;
+    run[k] = sum;
+    sum += idx < items ? tile_count[idx * kCounterStride] : 0;
+  }
+  long long incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_total[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const long long v = warp_total[lane];
+    long long w = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    warp_total[lane] = w - v;  // exclusive prefix of the warp totals
+  }
+  __syncthreads();
+  const long long prefix = warp_total[warp] + (incl - sum);
+#pragma unroll
+  for (int k = 0; k < kScanPerThread; ++k) {
+    const int64_t idx = base + k;
+    if (idx < items) {
+      const long long o = prefix + run[k];
+      off64[idx] = o;
+      off32[idx] = (int32_t)(o < 2147483647LL ? o : 2147483647LL);
+    }
+  }
+}
+
 // Ascending sort of buf[0..len) using a bitonic network over the next power of two in which
 // every comparator puts the smaller key first; positions >= len act as +inf and never move.
 template <typename Sync>
@@ -413,6 +466,12 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
                                                            w.tile_count);
     if ((rc = check_launch("tile_count"))) return rc;
   }
+  (void)status;
+  if (T + 1 <= kSingleScanMax) {
+    single_scan_kernel<<<1, kScanThreads, 0, s>>>(w.tile_count, T + 1, w.offsets64,
+                                                  tile_offsets);
+    return check_launch("tile_offsets scan");
+  }
   size_t sb = w.scan_bytes;
   cudaError_t e = cub::DeviceScan::ExclusiveScan(w.scan_temp, sb, counter_iter(w.tile_count),
                                                  w.offsets64,
@@ -423,7 +482,6 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
   tile_fill_kernel<false><<<(int)((T + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
       rec, 0, ts, frames, cutoff2, T, w.offsets64, w.tile_count, tile_offsets, nullptr,
       INT64_MAX, w.big_count, nullptr);
-  (void)status;
   return check_launch("tile_offsets");
 }
 

@@ -535,6 +535,43 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
   write_gradients(rec, g, acc, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
+// Per-Gaussian epilogue straight to the RS field parameters: moments (fast) or the sum of the
+// entry partials (deterministic) -> render-input gradients -> the RS chain rule, the same
+// arithmetic as the backward epilogue followed by ss_project_rs_backward, in one pass.
+template <bool DETERMINISTIC>
+__global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n, Frames frames,
+                                   int ts, const float* __restrict__ ws,
+                                   const int32_t* __restrict__ gids, int64_t cap,
+                                   const int32_t* __restrict__ offsets,
+                                   const float* __restrict__ log_scales,
+                                   const float* __restrict__ rotations,
+                                   const float* __restrict__ logits, float dilation,
+                                   float* __restrict__ g_means, float* __restrict__ g_ls,
+                                   float* __restrict__ g_rot, float* __restrict__ g_colors,
+                                   float* __restrict__ g_logits) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  float m[kMoments];
+  if (DETERMINISTIC) {
+    sum_partials(rec, g, n, ts, frames, gids, cap, offsets, ws, m);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kMoments; ++k) m[k] = ws[k * n + g];
+  }
+  const float4 p1 = reinterpret_cast<const float4*>(rec + g)[1];
+  const float4 p2 = reinterpret_cast<const float4*>(rec + g)[2];
+  const float op = p1.y, a = p2.y, b = p2.z, c = p2.w;
+  g_means[2 * g] = op * (a * m[4] + b * m[5]);
+  g_means[2 * g + 1] = op * (b * m[4] + c * m[5]);
+  g_colors[3 * g] = op * m[0];
+  g_colors[3 * g + 1] = op * m[1];
+  g_colors[3 * g + 2] = op * m[2];
+  rs_conic_chain(log_scales[2 * g], log_scales[2 * g + 1], rotations[g], dilation,
+                 -0.5f * op * m[6], -op * m[7], -0.5f * op * m[8], g_ls[2 * g], g_ls[2 * g + 1],
+                 g_rot[g]);
+  if (logits && g_logits) g_logits[g] = logit_chain(logits[g], m[3]);
+}
+
 int check_render_args(int64_t n, int H, int W, int ts, float eps) {
   if (n < 0 || H < 0 || W < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
   if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
@@ -859,6 +896,39 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
     finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
         rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
   return check_launch("backward finalize");
+}
+
+int ss_render_backward_finalize_rs(const void* records, int64_t n, const int32_t* tile_gids,
+                                   int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                                   int width, int tile_size, int deterministic,
+                                   const void* workspace, const float* log_scales,
+                                   const float* rotations, const float* opacity_logits,
+                                   float dilation, float* grad_means, float* grad_log_scales,
+                                   float* grad_rotations, float* grad_colors,
+                                   float* grad_opacity_logits, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, 1.0f);
+  if (rc) return rc;
+  if (n == 0) return SS_OK;
+  if (!records || !workspace || !log_scales || !rotations || !grad_means || !grad_log_scales ||
+      !grad_rotations || !grad_colors || (opacity_logits && !grad_opacity_logits) ||
+      (deterministic && !tile_offsets))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  const Splat* rec = static_cast<const Splat*>(records);
+  const float* ws = static_cast<const float*>(workspace);
+  const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
+  const Frames f = single_frame(height, width, tile_size);
+  cudaStream_t s = as_stream(stream);
+  if (deterministic)
+    finalize_rs_kernel<true><<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, f, tile_size, ws, tile_gids, gid_capacity, tile_offsets, log_scales, rotations,
+        opacity_logits, dilation, grad_means, grad_log_scales, grad_rotations, grad_colors,
+        grad_opacity_logits);
+  else
+    finalize_rs_kernel<false><<<gblocks, kEpilogueThreads, 0, s>>>(
+        rec, n, f, tile_size, ws, tile_gids, gid_capacity, tile_offsets, log_scales, rotations,
+        opacity_logits, dilation, grad_means, grad_log_scales, grad_rotations, grad_colors,
+        grad_opacity_logits);
+  return check_launch("backward finalize rs");
 }
 
 int ss_batch_render_backward(const ss_batch* batch, const float* grad_out, const void* records,

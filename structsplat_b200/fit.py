@@ -115,8 +115,25 @@ class RenderPlan:
                          _p(self.den), _p(self.status), _stream())
 
     def backward(self, grad_out, params):
+        """Gradients w.r.t. the RS parameters: the backward tile kernel into moments (fast) or
+        entry partials (deterministic), then one per-Gaussian pass through the RS chain rule."""
         if not self.n:
             return
+        if not self.deterministic:
+            self.bwd_ws.zero_()
+        self.backward_tiles(grad_out)
+        _native.call("ss_render_backward_finalize_rs", _p(self.records), self.n, _p(self.gids),
+                     self.capacity, _p(self.offsets), self.H, self.W, self.tile_size,
+                     int(self.deterministic), _p(self.bwd_ws), _p(params["log_scales"]),
+                     _p(params["rotations"]),
+                     _p(params.get("opacity_logits") if self.has_opacity else None),
+                     float(self.dilation), _p(self.g_means), _p(self.g_log_scales),
+                     _p(self.g_rotations), _p(self.g_colors),
+                     _p(self.g_logits if self.has_opacity else None), _stream())
+
+    def render_input_grads(self, grad_out):
+        """Gradients w.r.t. the render inputs (means, conics, colours, opacities) into
+        g_means / g_conics / g_colors / g_opac, through the one-call ss_render_backward."""
         _native.call("ss_render_backward", _p(grad_out), _p(self.records), self.n, _p(self.den),
                      _p(self.image), _p(self.gids), self.capacity, _p(self.offsets), self.H,
                      self.W, self.tile_size, int(self.normalize), float(self.eps),
@@ -124,12 +141,7 @@ class RenderPlan:
                      _p(self.g_conics), _p(self.g_colors), _p(self.g_opac),
                      int(self.deterministic), _p(self.bwd_ws), self.bwd_ws_bytes,
                      _p(self.status), _stream())
-        _native.call("ss_project_rs_backward", _p(params["log_scales"]), _p(params["rotations"]),
-                     _p(params.get("opacity_logits") if self.has_opacity else None), self.n,
-                     float(self.dilation), _p(self.g_conics),
-                     _p(self.g_opac if self.has_opacity else None), _p(self.g_log_scales),
-                     _p(self.g_rotations), _p(self.g_logits if self.has_opacity else None),
-                     _stream())
+        return self.g_means, self.g_conics, self.g_colors, self.g_opac
 
     def backward_tiles(self, grad_out):
         """Only the backward tile kernel (fast mode: adds into the moments), for timing."""

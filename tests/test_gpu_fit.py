@@ -97,9 +97,7 @@ def test_staged_backward_equals_one_call_backward(deterministic):
     grad_out = torch.randn(H, W, 3, device="cuda", generator=torch.Generator("cuda").manual_seed(9))
     plan = RenderPlan.for_field(params, H, W, deterministic=deterministic)
     plan.forward(params)
-    plan.backward(grad_out, params)
-    want = [plan.g_means.clone(), plan.g_conics.clone(), plan.g_colors.clone(),
-            plan.g_opac.clone()]
+    want = [t.clone() for t in plan.render_input_grads(grad_out)]
     plan.bwd_ws.zero_()
     plan.backward_tiles(grad_out)
     got = [torch.empty_like(t) for t in want]
