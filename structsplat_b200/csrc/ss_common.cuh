@@ -231,36 +231,99 @@ __device__ __forceinline__ Frame frame_of_gaussian(const Frames& f, int64_t g, i
 constexpr int kMoments = 9;
 constexpr int kPartialFloats = 12;
 
-// Deterministic second pass for Gaussian g: sums its per-entry moment partials over the tiles
-// of its support rectangle in ascending tile order, each entry found by binary search in the
-// tile's ascending list.  Tiles whose list was truncated by the capacity contribute nothing (the
-// backward reports them).
-__device__ __forceinline__ void sum_partials(const Splat* rec, int64_t g, int64_t n, int ts,
-                                             const Frames& frames, const int32_t* gids,
-                                             int64_t cap, const int32_t* offsets,
-                                             const float* partials, float (&acc)[kMoments]) {
+// Deterministic-mode workspace.  The backward writes one partial (nine moments, padded to 12
+// floats) per tile-list entry; the entries are then ordered by Gaussian with a stable radix sort
+// of their ids, so Gaussian g's entries are order[seg[g] .. seg[n + g]) in ascending tile order
+// and its moments are summed in that fixed order, whatever the schedule of the backward.
+//   partials  cap x 12 floats       keys_in / keys   cap uint32 (ids; n marks unused slots)
+//   order_in / order  cap int32      seg              2n int32 (segment begin, end)
+//   temp      the radix sort's scratch
+struct EntryOrder {
+  float* partials;
+  uint32_t* keys_in;
+  uint32_t* keys;
+  int32_t* order_in;
+  int32_t* order;
+  int32_t* seg;
+  void* temp;
+  size_t fixed_bytes;  // bytes before temp
+};
+
+__host__ __device__ inline size_t align_up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+__host__ __device__ inline EntryOrder entry_order_layout(void* ws, int64_t n, int64_t cap) {
+  size_t off[7];
+  const size_t bytes[6] = {(size_t)cap * kPartialFloats * sizeof(float), (size_t)cap * 4,
+                           (size_t)cap * 4, (size_t)cap * 4, (size_t)cap * 4, (size_t)2 * n * 4};
+  off[0] = 0;
+  for (int k = 0; k < 6; ++k) off[k + 1] = off[k] + align_up256(bytes[k]);
+  char* p = static_cast<char*>(ws);
+  EntryOrder e;
+  e.partials = reinterpret_cast<float*>(p + off[0]);
+  e.keys_in = reinterpret_cast<uint32_t*>(p + off[1]);
+  e.keys = reinterpret_cast<uint32_t*>(p + off[2]);
+  e.order_in = reinterpret_cast<int32_t*>(p + off[3]);
+  e.order = reinterpret_cast<int32_t*>(p + off[4]);
+  e.seg = reinterpret_cast<int32_t*>(p + off[5]);
+  e.temp = p + off[6];
+  e.fixed_bytes = off[6];
+  return e;
+}
+
+__host__ __device__ inline size_t entry_order_fixed_bytes(int64_t n, int64_t cap) {
+  return align_up256((size_t)cap * kPartialFloats * sizeof(float)) +
+         4 * align_up256((size_t)cap * 4) + align_up256((size_t)2 * n * 4);
+}
+
+// Segments up to this many entries are summed by their own lane; longer ones by the warp.
+constexpr int kLaneSegment = 32;
+
+__device__ __forceinline__ void add_partial(const float* partials, int32_t e,
+                                            float (&acc)[kMoments]) {
+  const float4* pp = reinterpret_cast<const float4*>(partials + (int64_t)e * kPartialFloats);
+  const float4 u = pp[0], v = pp[1];
+  const float w = partials[(int64_t)e * kPartialFloats + 8];
+  acc[0] += u.x; acc[1] += u.y; acc[2] += u.z; acc[3] += u.w;
+  acc[4] += v.x; acc[5] += v.y; acc[6] += v.z; acc[7] += v.w;
+  acc[8] += w;
+}
+
+// Sum of Gaussian g's entry partials in its fixed entry order.  Warp-collective: every lane of
+// the warp calls it (active = false for a lane without a Gaussian).  A segment of at most
+// kLaneSegment entries is summed serially by its lane; a longer one by the whole warp (lane l
+// takes entries l, l + 32, ..., then a butterfly over the lanes), so one huge Gaussian does not
+// serialise its warp.  The order depends only on the segment's length.
+__device__ __forceinline__ void sum_entry_partials(const float* __restrict__ partials,
+                                                   const int32_t* __restrict__ order,
+                                                   const int32_t* __restrict__ seg, int64_t n,
+                                                   int64_t g, bool active,
+                                                   float (&acc)[kMoments]) {
 #pragma unroll
   for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
-  const int4 r = reinterpret_cast<const int4*>(rec + g)[3];
-  if (!(r.z > r.x && r.w > r.y)) return;
-  const Frame fr = frame_of_gaussian(frames, g, n);
-  const int gx0 = r.x / ts, gx1 = (r.z - 1) / ts, gy0 = r.y / ts, gy1 = (r.w - 1) / ts;
-  for (int gy = gy0; gy <= gy1; ++gy) {
-    for (int gx = gx0; gx <= gx1; ++gx) {
-      const int t = fr.first_tile + gy * fr.tiles_x + gx;
-      int64_t lo = offsets[t], hi = offsets[t + 1];
-      if (hi > cap) continue;
-      const int64_t end = hi;
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (gids[mid] < g) lo = mid + 1; else hi = mid;
-      }
-      if (lo < end && gids[lo] == g) {
-        const float* pp = partials + lo * kPartialFloats;
+  int beg = 0, end = 0;
+  if (active) {
+    beg = seg[g];
+    end = seg[n + g];
+  }
+  if (end - beg <= kLaneSegment)
+    for (int i = beg; i < end; ++i) add_partial(partials, order[i], acc);
+  const int lane = threadIdx.x & 31;
+  unsigned big = __ballot_sync(0xffffffffu, end - beg > kLaneSegment);
+  while (big) {
+    const int src = __ffs(big) - 1;
+    big &= big - 1;
+    const int b = __shfl_sync(0xffffffffu, beg, src), e = __shfl_sync(0xffffffffu, end, src);
+    float t[kMoments];
 #pragma unroll
-        for (int k = 0; k < kMoments; ++k) acc[k] += pp[k];
-      }
-    }
+    for (int k = 0; k < kMoments; ++k) t[k] = 0.f;
+    for (int i = b + lane; i < e; i += 32) add_partial(partials, order[i], t);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+    if (lane == src)
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) acc[k] = t[k];
   }
 }
 

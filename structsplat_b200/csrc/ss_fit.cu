@@ -48,19 +48,17 @@ __device__ __forceinline__ float adam(float p, float g, float& m, float& v, floa
 
 template <bool DETERMINISTIC>
 __global__ void __launch_bounds__(kThreads)
-    fit_update_kernel(const Splat* __restrict__ rec, int64_t n, Frames frames, int ts,
+    fit_update_kernel(const Splat* __restrict__ rec, int64_t n, Frames frames,
                       float* __restrict__ moments, const float* __restrict__ partials,
-                      const int32_t* __restrict__ gids, int64_t cap,
-                      const int32_t* __restrict__ offsets, FieldPtrs field, FieldPtrs exp_avg,
-                      FieldPtrs exp_avg_sq, AdamHyper h, const float* __restrict__ log_hi,
-                      int* __restrict__ step_state) {
+                      const int32_t* __restrict__ order, const int32_t* __restrict__ seg,
+                      FieldPtrs field, FieldPtrs exp_avg, FieldPtrs exp_avg_sq, AdamHyper h,
+                      const float* __restrict__ log_hi, int* __restrict__ step_state) {
   const int t = step_state[0] + 1;
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  float m[kMoments];
+  if (DETERMINISTIC) sum_entry_partials(partials, order, seg, n, g, g < n, m);
   if (g < n) {
-    float m[kMoments];
-    if (DETERMINISTIC) {
-      sum_partials(rec, g, n, ts, frames, gids, cap, offsets, partials, m);
-    } else {
+    if (!DETERMINISTIC) {
 #pragma unroll
       for (int k = 0; k < kMoments; ++k) {
         m[k] = moments[k * n + g];
@@ -171,15 +169,16 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
   const Splat* rec = static_cast<const Splat*>(records);
   float* ws = static_cast<float*>(workspace);
   cudaStream_t s = as_stream(stream);
-  if (deterministic)
-    fit_update_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, f, batch->tile_size, nullptr, ws,
-                                                        tile_gids, gid_capacity, tile_offsets, p,
-                                                        m, v, h, log_scale_hi, step_state);
-  else
-    fit_update_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, f, batch->tile_size, ws,
-                                                         nullptr, tile_gids, gid_capacity,
-                                                         tile_offsets, p, m, v, h, log_scale_hi,
+  if (deterministic) {
+    const EntryOrder eo = entry_order_layout(workspace, n, gid_capacity);
+    fit_update_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, f, nullptr, eo.partials,
+                                                        eo.order, eo.seg, p, m, v, h,
+                                                        log_scale_hi, step_state);
+  } else {
+    fit_update_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, f, ws, nullptr, nullptr,
+                                                         nullptr, p, m, v, h, log_scale_hi,
                                                          step_state);
+  }
   return check_launch("fit_adam_update");
 }
 

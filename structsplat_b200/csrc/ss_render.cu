@@ -26,11 +26,14 @@
 // i.e. the reference's per-pixel formulas (render_ext.cu:785-818) summed over pixels.  Along a
 // column dx is constant, so S1, S3 and S4 fold into per-column products.  The moments are
 // reduce-scattered over the four lanes and added with one atomic per moment into per-Gaussian
-// accumulators (fast mode), or stored per (tile, Gaussian) entry and summed per Gaussian in
-// ascending tile order by a second kernel (deterministic mode: every entry is computed by its
-// own four lanes in a fixed order, so the result does not depend on the scheduling).  A
-// per-Gaussian epilogue applies o, a, b, c once.
+// accumulators (fast mode), or stored per (tile, Gaussian) entry, the entries ordered by
+// Gaussian with a stable radix sort, and summed per Gaussian in ascending tile order by a second
+// kernel (deterministic mode: every entry is computed by its own four lanes in a fixed order, so
+// the result does not depend on the scheduling).  A per-Gaussian epilogue applies o, a, b, c
+// once.
 #include <atomic>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "ss_common.cuh"
 
@@ -518,20 +521,20 @@ __global__ void finalize_moments_kernel(const Splat* __restrict__ rec, int64_t n
   write_gradients(rec, g, m, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
-// Deterministic second pass: per-Gaussian sum of the per-entry partials (sum_partials), then
-// the per-Gaussian factors.
+// Deterministic second pass: per-Gaussian sum of the entry partials in the fixed entry order
+// (sum_entry_partials), then the per-Gaussian factors.
 __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
-                                       const int32_t* __restrict__ gids, int64_t cap,
-                                       const int32_t* __restrict__ offsets, Frames frames,
-                                       int ts, const float* __restrict__ partials,
-                                       int has_opacity, float* __restrict__ g_means,
+                                       const float* __restrict__ partials,
+                                       const int32_t* __restrict__ order,
+                                       const int32_t* __restrict__ seg, int has_opacity,
+                                       float* __restrict__ g_means,
                                        float* __restrict__ g_conics,
                                        float* __restrict__ g_colors,
                                        float* __restrict__ g_opac) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n) return;
   float acc[kMoments];
-  sum_partials(rec, g, n, ts, frames, gids, cap, offsets, partials, acc);
+  sum_entry_partials(partials, order, seg, n, g, g < n, acc);
+  if (g >= n) return;
   write_gradients(rec, g, acc, has_opacity, g_means, g_conics, g_colors, g_opac);
 }
 
@@ -539,10 +542,10 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
 // entry partials (deterministic) -> render-input gradients -> the RS chain rule, the same
 // arithmetic as the backward epilogue followed by ss_project_rs_backward, in one pass.
 template <bool DETERMINISTIC>
-__global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n, Frames frames,
-                                   int ts, const float* __restrict__ ws,
-                                   const int32_t* __restrict__ gids, int64_t cap,
-                                   const int32_t* __restrict__ offsets,
+__global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n,
+                                   const float* __restrict__ ws,
+                                   const int32_t* __restrict__ order,
+                                   const int32_t* __restrict__ seg,
                                    const float* __restrict__ log_scales,
                                    const float* __restrict__ rotations,
                                    const float* __restrict__ logits, float dilation,
@@ -550,11 +553,10 @@ __global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n, Fra
                                    float* __restrict__ g_rot, float* __restrict__ g_colors,
                                    float* __restrict__ g_logits) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n) return;
   float m[kMoments];
-  if (DETERMINISTIC) {
-    sum_partials(rec, g, n, ts, frames, gids, cap, offsets, ws, m);
-  } else {
+  if (DETERMINISTIC) sum_entry_partials(ws, order, seg, n, g, g < n, m);
+  if (g >= n) return;
+  if (!DETERMINISTIC) {
 #pragma unroll
     for (int k = 0; k < kMoments; ++k) m[k] = ws[k * n + g];
   }
@@ -570,6 +572,75 @@ __global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n, Fra
                  -0.5f * op * m[6], -op * m[7], -0.5f * op * m[8], g_ls[2 * g], g_ls[2 * g + 1],
                  g_rot[g]);
   if (logits && g_logits) g_logits[g] = logit_chain(logits[g], m[3]);
+}
+
+// Deterministic mode, after the backward: the entries of the tile lists ordered by Gaussian.
+// Keys are the entry ids (n for slots past the filled part of the index); a stable radix sort
+// keeps each Gaussian's entries in ascending tile order; the segment kernel records where each
+// Gaussian's run begins and ends (Gaussians without entries keep the empty run 0..0).
+__global__ void entry_keys_kernel(const int32_t* __restrict__ gids,
+                                  const int32_t* __restrict__ offsets, int64_t T, int64_t cap,
+                                  int64_t n, uint32_t* __restrict__ keys,
+                                  int32_t* __restrict__ order) {
+  const int64_t last = offsets[T];
+  const int64_t total = last < cap ? last : cap;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cap; e += stride) {
+    const int32_t id = e < total ? gids[e] : -1;
+    keys[e] = (id >= 0 && id < n) ? (uint32_t)id : (uint32_t)n;
+    order[e] = (int32_t)e;
+  }
+}
+
+__global__ void entry_segments_kernel(const uint32_t* __restrict__ keys, int64_t cap, int64_t n,
+                                      int32_t* __restrict__ seg) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
+    const uint32_t k = keys[i];
+    if (k >= (uint64_t)n) continue;
+    if (i == 0 || keys[i - 1] != k) seg[k] = (int32_t)i;
+    if (i + 1 == cap || keys[i + 1] != k) seg[n + k] = (int32_t)(i + 1);
+  }
+}
+
+int key_bits(int64_t n) {
+  int b = 1;
+  while (b < 32 && ((int64_t)1 << b) <= n) ++b;
+  return b;  // keys 0..n fit in b bits
+}
+
+size_t sort_temp_bytes(int64_t n, int64_t cap) {
+  size_t b = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (const uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (const int32_t*)nullptr, (int32_t*)nullptr,
+                                  (int)(cap > 0 ? cap : 1), 0, key_bits(n));
+  return b;
+}
+
+int clear_entry_segments(void* ws, int64_t n, int64_t cap, cudaStream_t s) {
+  const EntryOrder eo = entry_order_layout(ws, n, cap);
+  cudaMemsetAsync(eo.seg, 0, sizeof(int32_t) * 2 * n, s);
+  return check_launch("entry segments zero-fill");
+}
+
+int order_entries(const int32_t* gids, const int32_t* offsets, int64_t T, int64_t cap,
+                  int64_t n, void* ws, cudaStream_t s) {
+  int rc;
+  if ((rc = clear_entry_segments(ws, n, cap, s))) return rc;
+  if (cap == 0) return SS_OK;
+  const EntryOrder eo = entry_order_layout(ws, n, cap);
+  const int64_t want = (cap + kEpilogueThreads - 1) / kEpilogueThreads;
+  const unsigned blocks = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+  entry_keys_kernel<<<blocks, kEpilogueThreads, 0, s>>>(gids, offsets, T, cap, n, eo.keys_in,
+                                                         eo.order_in);
+  if ((rc = check_launch("entry keys"))) return rc;
+  size_t tb = sort_temp_bytes(n, cap);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(eo.temp, tb, eo.keys_in, eo.keys, eo.order_in,
+                                                  eo.order, (int)cap, 0, key_bits(n), s);
+  if (e != cudaSuccess)
+    return fail(SS_ERR_CUDA, "entry order sort: %s", cudaGetErrorString(e));
+  entry_segments_kernel<<<blocks, kEpilogueThreads, 0, s>>>(eo.keys, cap, n, eo.seg);
+  return check_launch("entry segments");
 }
 
 int check_render_args(int64_t n, int H, int W, int ts, float eps) {
@@ -684,8 +755,11 @@ int render_backward_tiles(const Frames& f, int ts, int64_t T, const float* grad_
                           const float* pixel_grad, const int32_t* gids, int64_t cap,
                           const int32_t* offsets, int normalize, float eps, float tail,
                           int deterministic, float* ws, uint32_t* status, cudaStream_t s) {
-  if (T == 0 || n == 0) return SS_OK;
+  if (n == 0) return SS_OK;
+  if (T == 0) return deterministic ? clear_entry_segments(ws, n, cap, s) : SS_OK;
   if (T > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "too many tiles");
+  if (deterministic && cap > (int64_t)INT32_MAX)
+    return fail(SS_ERR_INVALID_ARGUMENT, "deterministic backward needs capacity < 2^31");
   const Splat* rec = static_cast<const Splat*>(records);
   const float4* pg = reinterpret_cast<const float4*>(pixel_grad);
   if (pixel_grad) {
@@ -703,11 +777,13 @@ int render_backward_tiles(const Frames& f, int ts, int64_t T, const float* grad_
       launch_backward<32, false>((unsigned)T, s, deterministic, grad_out, rec, n, den, out, pg,
                                  gids, cap, offsets, f, normalize, eps, tail, ws, status);
   }
-  return check_launch("render_backward");
+  int rc = check_launch("render_backward");
+  if (rc || !deterministic) return rc;
+  return order_entries(gids, offsets, T, cap, n, ws, s);
 }
 
 size_t backward_ws_bytes(int64_t n, int64_t cap, int deterministic) {
-  return deterministic ? (size_t)cap * kPartialFloats * sizeof(float)
+  return deterministic ? entry_order_fixed_bytes(n, cap) + align_up256(sort_temp_bytes(n, cap))
                        : (size_t)n * kMoments * sizeof(float);
 }
 
@@ -746,11 +822,12 @@ int render_backward(const Frames& f, int ts, int64_t T, int64_t npx, const float
     return rc;
   const Splat* rec = static_cast<const Splat*>(records);
   const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
-  if (deterministic)
+  if (deterministic) {
+    const EntryOrder eo = entry_order_layout(ws, n, cap);
     reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, gids, cap, offsets, f, ts, ws, has_opacity, grad_means, grad_conics,
+        rec, n, eo.partials, eo.order, eo.seg, has_opacity, grad_means, grad_conics,
         grad_colors, grad_opacities);
-  else
+  } else
     finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
         rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
   return check_launch("backward epilogue");
@@ -854,13 +931,20 @@ int ss_render_backward_moments(const float* grad_out, const float* pixel_grad,
                                size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
   int rc = check_render_args(n, height, width, tile_size, eps);
   if (rc) return rc;
-  if (n == 0 || (int64_t)height * width == 0) return SS_OK;
+  if (n == 0) return SS_OK;
+  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
+  if ((int64_t)height * width == 0) {  // nothing rendered; the finalize sums no entries
+    if (!deterministic) return SS_OK;
+    if (workspace_bytes < need || !workspace)
+      return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+                  workspace_bytes, need);
+    return clear_entry_segments(workspace, n, gid_capacity, as_stream(stream));
+  }
   if (!records || !tile_offsets) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (!pixel_grad && (!grad_out || !den || !out))
     return fail(SS_ERR_INVALID_ARGUMENT, "need grad_out, out and den, or pixel_grad");
   if (pixel_grad && reinterpret_cast<uintptr_t>(pixel_grad) % 16)
     return fail(SS_ERR_INVALID_ARGUMENT, "pixel_grad must be 16-byte aligned");
-  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
   if (workspace_bytes < need || !workspace)
     return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
                 workspace_bytes, need);
@@ -888,11 +972,12 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
   const float* ws = static_cast<const float*>(workspace);
   const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
   cudaStream_t s = as_stream(stream);
-  if (deterministic)
+  if (deterministic) {
+    const EntryOrder eo = entry_order_layout(const_cast<float*>(ws), n, gid_capacity);
     reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, tile_gids, gid_capacity, tile_offsets, single_frame(height, width, tile_size),
-        tile_size, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
-  else
+        rec, n, eo.partials, eo.order, eo.seg, has_opacity, grad_means, grad_conics,
+        grad_colors, grad_opacities);
+  } else
     finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
         rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
   return check_launch("backward finalize");
@@ -916,18 +1001,17 @@ int ss_render_backward_finalize_rs(const void* records, int64_t n, const int32_t
   const Splat* rec = static_cast<const Splat*>(records);
   const float* ws = static_cast<const float*>(workspace);
   const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
-  const Frames f = single_frame(height, width, tile_size);
   cudaStream_t s = as_stream(stream);
-  if (deterministic)
+  if (deterministic) {
+    const EntryOrder eo = entry_order_layout(const_cast<float*>(ws), n, gid_capacity);
     finalize_rs_kernel<true><<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, f, tile_size, ws, tile_gids, gid_capacity, tile_offsets, log_scales, rotations,
-        opacity_logits, dilation, grad_means, grad_log_scales, grad_rotations, grad_colors,
-        grad_opacity_logits);
-  else
+        rec, n, eo.partials, eo.order, eo.seg, log_scales, rotations, opacity_logits, dilation,
+        grad_means, grad_log_scales, grad_rotations, grad_colors, grad_opacity_logits);
+  } else {
     finalize_rs_kernel<false><<<gblocks, kEpilogueThreads, 0, s>>>(
-        rec, n, f, tile_size, ws, tile_gids, gid_capacity, tile_offsets, log_scales, rotations,
-        opacity_logits, dilation, grad_means, grad_log_scales, grad_rotations, grad_colors,
-        grad_opacity_logits);
+        rec, n, ws, nullptr, nullptr, log_scales, rotations, opacity_logits, dilation,
+        grad_means, grad_log_scales, grad_rotations, grad_colors, grad_opacity_logits);
+  }
   return check_launch("backward finalize rs");
 }
 
@@ -988,9 +1072,16 @@ int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
   Frames f;
   int rc = check_batch_render(batch, n, 1.0f, &f);
   if (rc) return rc;
-  if (n == 0 || batch->pixels == 0) return SS_OK;
-  if (!records || !tile_offsets || !pixel_grad) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
+  if (n == 0) return SS_OK;
   const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
+  if (batch->pixels == 0) {  // nothing rendered; the update sums no entries
+    if (!deterministic) return SS_OK;
+    if (workspace_bytes < need || !workspace)
+      return fail(SS_ERR_INVALID_ARGUMENT, "fit backward workspace too small (%zu < %zu)",
+                  workspace_bytes, need);
+    return clear_entry_segments(workspace, n, gid_capacity, as_stream(stream));
+  }
+  if (!records || !tile_offsets || !pixel_grad) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (workspace_bytes < need || !workspace)
     return fail(SS_ERR_INVALID_ARGUMENT, "fit backward workspace too small (%zu < %zu)",
                 workspace_bytes, need);

@@ -79,7 +79,10 @@ def test_argument_validation_without_gpu(lib):
     assert rc == 1 and "central gradients" in msg
     rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 16, 16, 1,
                       ctypes.byref(size))
-    assert rc == 0 and size.value == 100 * 48
+    # 12-float partials, two key and two order arrays per entry, begin/end per Gaussian (each
+    # 256-byte aligned), then the radix sort's scratch (queried from CUB; none without a GPU)
+    fixed = 4864 + 4 * 512 + 256
+    assert rc == 0 and size.value >= fixed and size.value % 256 == 0
     rc, msg = _status(lib, "ss_render_backward_workspace_bytes", 10, 100, 16, 16, 0,
                       ctypes.byref(size))
     assert rc == 0 and size.value == 10 * 36
@@ -123,7 +126,10 @@ def test_batch_validation_without_gpu(lib):
                       None, None, None, None, None, None)
     assert rc == 1 and "loss_kind" in msg
     rc, msg = _status(lib, "ss_fit_backward_workspace_bytes", 10, 100, 1, ctypes.byref(size))
-    assert rc == 0 and size.value == 100 * 48
+    # 12-float partials, two key and two order arrays per entry, begin/end per Gaussian (each
+    # 256-byte aligned), then the radix sort's scratch (queried from CUB; none without a GPU)
+    fixed = 4864 + 4 * 512 + 256
+    assert rc == 0 and size.value >= fixed and size.value % 256 == 0
     lrs = (ctypes.c_double * 5)(*([1e-2] * 5))
     ptrs = (ctypes.c_void_p * 5)()
     rc, msg = _status(lib, "ss_fit_adam_update", ctypes.byref(b), None, 10, None, 0, None, 0,
