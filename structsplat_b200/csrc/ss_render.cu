@@ -311,6 +311,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   __shared__ int stage_gid[kStageMax];
   __shared__ int order[kStageMax];
   __shared__ int class_count[64];
+  __shared__ int next_group;  // the next group a warp takes
   const int tile = blockIdx.x;
   const Frame fr = frame_of_tile(frames, tile, n);
   const int local = tile - fr.first_tile;
@@ -351,6 +352,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     constexpr int kPer = (kStageMax + NT - 1) / NT;  // entries per thread
     int code[kPer];
     if (threadIdx.x < 64) class_count[threadIdx.x] = 0;
+    if (threadIdx.x == 0) next_group = 0;
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < kPer; ++i) {
@@ -457,8 +459,16 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   };
   auto run = [&](const float4(*st)[4], int m, int* ord, const int* gsm, int64_t k0) {
     prepare(st, m, ord);
+    // Groups go to warps as they become free (heaviest first, by the class order), so the
+    // warps of a CTA finish close together instead of idling behind a round-robin share.
     const int groups = (m + 7) >> 3;
-    for (int g = warp; g < groups; g += NT / 32) work_group(st, ord, gsm, m, g, k0);
+    for (;;) {
+      int g = 0;
+      if (lane == 0) g = atomicAdd(&next_group, 1);
+      g = __shfl_sync(0xffffffffu, g, 0);
+      if (g >= groups) break;
+      work_group(st, ord, gsm, m, g, k0);
+    }
   };
   if (L.count <= kStageMax) {
     stage_range<NT>(stage, rec, L, 0, (int)L.count, stage_gid);
