@@ -317,32 +317,65 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   const int local = tile - fr.first_tile;
   const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
   const int H = fr.H, W = fr.W;
-  for (int q = threadIdx.x; q < TS * TS; q += NT) {
-    const int x = tx0 + (q % TS), y = ty0 + (q / TS);
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (PIXGRAD) {
-      if (x < W && y < H) v = pixel_grad[fr.pixel_base + (int64_t)y * W + x];
-    } else if (x < W && y < H) {
-      const int64_t p = fr.pixel_base + (int64_t)y * W + x;
-      const float gr = grad_out[3 * p], gg = grad_out[3 * p + 1], gb = grad_out[3 * p + 2];
-      v = make_float4(gr, gg, gb, 0.f);
-      if (normalize) {
-        const float denom = den[p] + eps;
-        v.x = gr / denom;
-        v.y = gg / denom;
-        v.z = gb / denom;
-        v.w = -(gr * out[3 * p] + gg * out[3 * p + 1] + gb * out[3 * p + 2]) / denom;
-      }
-    }
-    pix[q] = v;
-  }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int member = lane >> 2, quad = lane & 3;
   const TileList L = tile_list(gids, offsets, cap, fr, tile);
   if (DETERMINISTIC && L.direct) {
     if (threadIdx.x == 0) raise_status(status, SS_STATUS_DETERMINISTIC_TRUNCATED);
     return;
   }
+  // the first records' copies are in flight while the pixel inputs load
+  if (L.count <= kStageMax)
+    stage_range<NT>(stage, rec, L, 0, (int)L.count, stage_gid);
+  else
+    stage_range<NT>(stage, rec, L, 0, (int)(L.count < kHalf ? L.count : kHalf), stage_gid);
+  cp_async_commit();
+  // Per-pixel inputs of the tile: every load is issued before the first is used.
+  constexpr int kPx = TS * TS / NT;
+  static_assert(TS * TS % NT == 0, "pixels per thread");
+  {
+    float4 va[kPx];
+    float dn[kPx], o0[kPx], o1[kPx], o2[kPx];
+#pragma unroll
+    for (int i = 0; i < kPx; ++i) {
+      const int q = threadIdx.x + i * NT;
+      const int x = tx0 + (q % TS), y = ty0 + (q / TS);
+      va[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      dn[i] = 0.f;
+      o0[i] = o1[i] = o2[i] = 0.f;
+      if (x < W && y < H) {
+        const int64_t p = fr.pixel_base + (int64_t)y * W + x;
+        if (PIXGRAD) {
+          va[i] = pixel_grad[p];
+        } else {
+          va[i] = make_float4(grad_out[3 * p], grad_out[3 * p + 1], grad_out[3 * p + 2], 0.f);
+          if (normalize) {
+            dn[i] = den[p];
+            o0[i] = out[3 * p];
+            o1[i] = out[3 * p + 1];
+            o2[i] = out[3 * p + 2];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kPx; ++i) {
+      const int q = threadIdx.x + i * NT;
+      float4 v = va[i];
+      if (!PIXGRAD && normalize) {
+        const int x = tx0 + (q % TS), y = ty0 + (q / TS);
+        if (x < W && y < H) {
+          const float denom = dn[i] + eps;
+          const float gr = v.x, gg = v.y, gb = v.z;
+          v.x = gr / denom;
+          v.y = gg / denom;
+          v.z = gb / denom;
+          v.w = -(gr * o0[i] + gg * o1[i] + gb * o2[i]) / denom;
+        }
+      }
+      pix[q] = v;
+    }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int member = lane >> 2, quad = lane & 3;
   // Order of the staged entries [0, m) by a counting sort into 64 cost classes (loop passes
   // descending, then rows in fours descending), so the eight Gaussians of a warp have nearly the
   // same loop trip counts and the heaviest groups start first.  The order within a class comes
@@ -413,7 +446,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
           float tc = 0.f, uc = 0.f;
           float dy = dy0;
           int pidx = cy0 * TS + cx;
-#pragma unroll 1
+#pragma unroll 2
           for (int k = 0; k < rows; ++k, dy += 1.0f, pidx += TS) {
             const float4 gp = pix[pidx];
             const float e = fmaf(dy, fmaf(p1.x, dy, bdx), adx2);
@@ -423,13 +456,14 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
             acc[0] = fmaf(base_w, gp.x, acc[0]);
             acc[1] = fmaf(base_w, gp.y, acc[1]);
             acc[2] = fmaf(base_w, gp.z, acc[2]);
-            acc[3] = fmaf(base_w, dw, acc[3]);
+            if (FADE) acc[3] = fmaf(base_w, dw, acc[3]);
             const float t = (FADE && raw <= tail) ? 0.0f : raw * dw;
             const float u = t * dy;
             tc += t;
             uc += u;
             acc[8] = fmaf(u, dy, acc[8]);
           }
+          if (!FADE) acc[3] += tc;  // without the fade base_w = raw, so G's column sum is tc
           acc[4] = fmaf(dx, tc, acc[4]);
           acc[5] += uc;
           acc[6] = fmaf(dx * dx, tc, acc[6]);
@@ -471,8 +505,6 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     }
   };
   if (L.count <= kStageMax) {
-    stage_range<NT>(stage, rec, L, 0, (int)L.count, stage_gid);
-    cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     run(stage, (int)L.count, order, stage_gid, 0);
@@ -481,8 +513,6 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     const int64_t count = L.count;
     const int nchunks = (int)((count + kHalf - 1) / kHalf);
     auto len = [&](int64_t k0) { return (int)(count - k0 < kHalf ? count - k0 : kHalf); };
-    stage_range<NT>(buf[0], rec, L, 0, len(0), stage_gid);
-    cp_async_commit();
     for (int c = 0; c < nchunks; ++c) {
       const int64_t k0 = (int64_t)c * kHalf;
       if (c + 1 < nchunks)
