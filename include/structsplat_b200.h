@@ -217,8 +217,10 @@ int ss_fit_forward_loss(const ss_batch* batch, const void* records, int64_t n,
                         const float* target, int loss_kind, float charbonnier_eps,
                         float* pixel_grad, float* image, float* den, float* loss,
                         uint32_t* status, ss_stream_t stream);
-/* Workspace of ss_fit_backward: moments (36 B per Gaussian) or, deterministic, per-entry
- * partials (48 B per entry of capacity). */
+/* Workspace of ss_fit_backward and ss_fit_adam_update: moments (36 B per Gaussian) or,
+ * deterministic, per-entry partials and their by-Gaussian order (64 B per entry of capacity,
+ * 8 B per Gaussian and the radix sort's scratch), followed by the parameter gradients of the
+ * Adam step (36 B per Gaussian). */
 int ss_fit_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int deterministic,
                                     size_t* bytes);
 /* Render backward from pixel_grad into the workspace.  Fast mode adds into per-Gaussian

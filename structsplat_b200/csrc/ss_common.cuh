@@ -275,6 +275,34 @@ __host__ __device__ inline size_t entry_order_fixed_bytes(int64_t n, int64_t cap
          4 * align_up256((size_t)cap * 4) + align_up256((size_t)2 * n * 4);
 }
 
+// Fit workspace: the backward's part (above) followed by the parameter gradients of the Adam
+// step, five arrays shaped like the parameters (means 2n, log-scales 2n, rotations n, colours 3n,
+// opacity logits n), each 256-byte aligned.
+struct FitGrads {
+  float *means, *log_scales, *rotations, *colors, *logits;
+};
+__host__ __device__ inline size_t fit_grads_bytes(int64_t n) {
+  return 2 * align_up256((size_t)8 * n) + 2 * align_up256((size_t)4 * n) +
+         align_up256((size_t)12 * n);
+}
+__host__ __device__ inline FitGrads fit_grads_layout(void* base, int64_t n) {
+  char* p = static_cast<char*>(base);
+  FitGrads g;
+  g.means = reinterpret_cast<float*>(p);
+  p += align_up256((size_t)8 * n);
+  g.log_scales = reinterpret_cast<float*>(p);
+  p += align_up256((size_t)8 * n);
+  g.rotations = reinterpret_cast<float*>(p);
+  p += align_up256((size_t)4 * n);
+  g.colors = reinterpret_cast<float*>(p);
+  p += align_up256((size_t)12 * n);
+  g.logits = reinterpret_cast<float*>(p);
+  return g;
+}
+// Offset of the gradients in the fit workspace and its total size (ss_render.cu).
+size_t fit_grads_offset(int64_t n, int64_t cap, int deterministic);
+size_t fit_ws_bytes(int64_t n, int64_t cap, int deterministic);
+
 // Segments up to this many entries are summed by their own lane; longer ones by the warp.
 constexpr int kLaneSegment = 32;
 

@@ -1,8 +1,11 @@
-// Per-Gaussian update of a fit iteration: the render backward's summed moments become conic /
-// mean / colour / opacity gradients, the chain rule carries them to the RS field parameters
-// (gaussians.py:270-300), one Adam step updates every parameter, and the log-scales are clamped
-// as the reference's fit loop does after opt.step() (fit.py:3033, 3359-3366).  The moment
-// accumulators are zeroed for the next iteration.
+// Update of a fit iteration, in two passes.  Per Gaussian (fit_grad_kernel): the render
+// backward's summed moments become conic / mean / colour / opacity gradients and the chain rule
+// carries them to the RS field parameters (gaussians.py:270-300); the moment accumulators are
+// zeroed for the next iteration.  Per parameter element (adam_kernel): one Adam step over the
+// five parameter tensors as flat arrays, then the clamp of the log-scales that the reference's
+// fit loop applies after opt.step() (fit.py:3033, 3359-3366).  The gradients pass through the
+// fit workspace so the Adam pass streams four aligned arrays per tensor at full occupancy,
+// as torch's multi-tensor Adam does.
 //
 // Adam is torch.optim.Adam's multi-tensor step (no weight decay, no amsgrad), element by element:
 //   m <- lerp(m, g, 1 - beta1)            = m + (1 - beta1)(g - m)
@@ -12,8 +15,8 @@
 // scalars are, so the update reproduces the eager optimizer.
 //
 // The step count lives on the device (step_state[0]) so the update can be replayed from a CUDA
-// graph: every thread uses t = step_state[0] + 1 and the last CTA to finish stores t back
-// (step_state[1] counts finished CTAs and is reset by that CTA).
+// graph: every thread of the Adam pass uses t = step_state[0] + 1 and its last CTA to finish
+// stores t back (step_state[1] counts finished CTAs and is reset by that CTA).
 #include "ss_common.cuh"
 
 namespace ss {
@@ -46,71 +49,128 @@ __device__ __forceinline__ float adam(float p, float g, float& m, float& v, floa
   return fmaf(-step, m / denom, p);
 }
 
+// Per-Gaussian gradients of the five parameter groups: the summed moments (fast: the atomic
+// accumulators, read and zeroed; deterministic: the entry partials in their fixed order) become
+// render-input gradients, and the chain rule carries them to the RS parameters at their current
+// values.  Grid-stride, a warp's 32 consecutive Gaussians per round (the deterministic sum is
+// warp-collective).  The gradients go to tensors shaped like the parameters.
 template <bool DETERMINISTIC>
 __global__ void __launch_bounds__(kThreads)
-    fit_update_kernel(const Splat* __restrict__ rec, int64_t n, Frames frames,
-                      float* __restrict__ moments, const float* __restrict__ partials,
-                      const int32_t* __restrict__ order, const int32_t* __restrict__ seg,
-                      FieldPtrs field, FieldPtrs exp_avg, FieldPtrs exp_avg_sq, AdamHyper h,
-                      const float* __restrict__ log_hi, int* __restrict__ step_state) {
-  const int t = step_state[0] + 1;
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  float m[kMoments];
-  if (DETERMINISTIC) sum_entry_partials(partials, order, seg, n, g, g < n, m);
-  if (g < n) {
+    fit_grad_kernel(const Splat* __restrict__ rec, int64_t n, float* __restrict__ moments,
+                    const float* __restrict__ partials, const int32_t* __restrict__ order,
+                    const int32_t* __restrict__ seg, const float* __restrict__ log_scales,
+                    const float* __restrict__ rotations, const float* __restrict__ logits,
+                    float dilation, FieldPtrs grad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n;
+       base += stride) {
+    const int64_t g = base + lane;
+    const bool active = g < n;
+    float m[kMoments];
+    if (DETERMINISTIC) sum_entry_partials(partials, order, seg, n, g, active, m);
+    if (!active) continue;
     if (!DETERMINISTIC) {
 #pragma unroll
-      for (int k = 0; k < kMoments; ++k) {
-        m[k] = moments[k * n + g];
-        moments[k * n + g] = 0.0f;
-      }
+      for (int k = 0; k < kMoments; ++k) m[k] = moments[k * n + g];
     }
     const float4 p1 = reinterpret_cast<const float4*>(rec + g)[1];
     const float4 p2 = reinterpret_cast<const float4*>(rec + g)[2];
-    const float op = p1.y, a = p2.y, b = p2.z, c = p2.w;
-    // gradients w.r.t. the render inputs (the same arithmetic as the plain backward epilogue)
-    const float gm0 = op * (a * m[4] + b * m[5]), gm1 = op * (b * m[4] + c * m[5]);
-    const float ga = -0.5f * op * m[6], gb = -op * m[7], gc = -0.5f * op * m[8];
-    const float gcol[3] = {op * m[0], op * m[1], op * m[2]};
-    // chain rule to log-scales, rotation and the logit
-    float gls0, gls1, grot;
-    rs_conic_chain(field.log_scales[2 * g], field.log_scales[2 * g + 1], field.rotations[g],
-                   h.dilation, ga, gb, gc, gls0, gls1, grot);
-    AdamStep st;
-    st.w1 = (float)(1.0 - h.beta1);
-    st.b2 = (float)h.beta2;
-    st.s2 = (float)(1.0 - h.beta2);
-    st.bc2s = (float)sqrt(1.0 - pow(h.beta2, (double)t));
-    st.eps = h.eps;
-    st.bc1 = 1.0 - pow(h.beta1, (double)t);
-    float pm, pv;
-#define SS_ADAM(PTR, IDX, GRAD, GROUP)                                                   \
-  pm = exp_avg.PTR[IDX];                                                                 \
-  pv = exp_avg_sq.PTR[IDX];                                                              \
-  field.PTR[IDX] = adam(field.PTR[IDX], GRAD, pm, pv, (float)(h.lr[GROUP] / st.bc1), st); \
-  exp_avg.PTR[IDX] = pm;                                                                 \
-  exp_avg_sq.PTR[IDX] = pv
-    if (field.logits) {  // before the update: the chain rule needs the current logit
-      const float glogit = logit_chain(field.logits[g], m[3]);
-      SS_ADAM(logits, g, glogit, 4);
-    }
-    SS_ADAM(means, 2 * g, gm0, 0);
-    SS_ADAM(means, 2 * g + 1, gm1, 0);
-    SS_ADAM(log_scales, 2 * g, gls0, 1);
-    SS_ADAM(log_scales, 2 * g + 1, gls1, 1);
-    SS_ADAM(rotations, g, grot, 2);
-    SS_ADAM(colors, 3 * g, gcol[0], 3);
-    SS_ADAM(colors, 3 * g + 1, gcol[1], 3);
-    SS_ADAM(colors, 3 * g + 2, gcol[2], 3);
-#undef SS_ADAM
-    // clamp_(max=hi) then clamp_(min=lo), NaN passing through as in torch
-    const float hi = log_hi[frames.image ? frames.gauss_image[g] : 0];
+    const float ls0 = log_scales[2 * g], ls1 = log_scales[2 * g + 1];
+    const float th = rotations[g];
+    const float lg = logits ? logits[g] : 0.f;
+    if (!DETERMINISTIC) {
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      float x = field.log_scales[2 * g + k];
-      x = x > hi ? hi : x;
-      x = x < h.log_lo ? h.log_lo : x;
-      field.log_scales[2 * g + k] = x;
+      for (int k = 0; k < kMoments; ++k) moments[k * n + g] = 0.0f;
+    }
+    const float op = p1.y, a = p2.y, b = p2.z, c = p2.w;
+    // the same arithmetic as the plain backward epilogue, then the RS chain rule
+    float gls0, gls1, grot;
+    rs_conic_chain(ls0, ls1, th, dilation, -0.5f * op * m[6], -op * m[7], -0.5f * op * m[8],
+                   gls0, gls1, grot);
+    grad.means[2 * g] = op * (a * m[4] + b * m[5]);
+    grad.means[2 * g + 1] = op * (b * m[4] + c * m[5]);
+    grad.log_scales[2 * g] = gls0;
+    grad.log_scales[2 * g + 1] = gls1;
+    grad.rotations[g] = grot;
+    grad.colors[3 * g] = op * m[0];
+    grad.colors[3 * g + 1] = op * m[1];
+    grad.colors[3 * g + 2] = op * m[2];
+    if (logits) grad.logits[g] = logit_chain(lg, m[3]);
+  }
+}
+
+// One parameter tensor of the Adam step: parameters, both moments, gradient and length; its
+// position in AdamTensors is its learning-rate group.
+struct AdamTensor {
+  float *p, *m, *v;
+  const float* g;
+  int64_t len;
+};
+struct AdamTensors {
+  AdamTensor t[5];  // means, log_scales, rotations, colors, opacity logits (len 0 if absent)
+};
+
+__device__ __forceinline__ float clamp_log_scale(float x, float hi, float lo) {
+  x = x > hi ? hi : x;  // clamp_(max=hi) then clamp_(min=lo), NaN passing through as in torch
+  return x < lo ? lo : x;
+}
+
+// The Adam step over the five tensors as flat arrays (four elements per access where every
+// pointer allows it), each block taking a grid-stride share of every tensor; log-scales are
+// clamped to [log_lo, log_hi[image]] after the step.  The step-dependent factors are formed
+// once per thread; the last block to finish advances the device step count.
+__global__ void __launch_bounds__(kThreads)
+    adam_kernel(AdamTensors ts, AdamHyper h, Frames frames, const float* __restrict__ log_hi,
+                int* __restrict__ step_state) {
+  const int t = step_state[0] + 1;
+  AdamStep st;
+  st.w1 = (float)(1.0 - h.beta1);
+  st.b2 = (float)h.beta2;
+  st.s2 = (float)(1.0 - h.beta2);
+  st.bc2s = (float)sqrt(1.0 - pow(h.beta2, (double)t));
+  st.eps = h.eps;
+  st.bc1 = 1.0 - pow(h.beta1, (double)t);
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  auto hi_of = [&](int64_t e) {  // log-scale element e belongs to Gaussian e / 2
+    return log_hi[frames.image ? frames.gauss_image[e >> 1] : 0];
+  };
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    const AdamTensor T = ts.t[k];
+    const float step = (float)(h.lr[k] / st.bc1);
+    const bool vec = ((reinterpret_cast<uintptr_t>(T.p) | reinterpret_cast<uintptr_t>(T.m) |
+                       reinterpret_cast<uintptr_t>(T.v) | reinterpret_cast<uintptr_t>(T.g)) &
+                      15) == 0;
+    const int64_t n4 = vec ? T.len / 4 : 0;
+    for (int64_t i = tid; i < n4; i += stride) {
+      float4 p = reinterpret_cast<float4*>(T.p)[i];
+      float4 m = reinterpret_cast<float4*>(T.m)[i];
+      float4 v = reinterpret_cast<float4*>(T.v)[i];
+      const float4 g = reinterpret_cast<const float4*>(T.g)[i];
+      p.x = adam(p.x, g.x, m.x, v.x, step, st);
+      p.y = adam(p.y, g.y, m.y, v.y, step, st);
+      p.z = adam(p.z, g.z, m.z, v.z, step, st);
+      p.w = adam(p.w, g.w, m.w, v.w, step, st);
+      if (k == 1) {
+        const float h0 = hi_of(4 * i), h1 = hi_of(4 * i + 2);
+        p.x = clamp_log_scale(p.x, h0, h.log_lo);
+        p.y = clamp_log_scale(p.y, h0, h.log_lo);
+        p.z = clamp_log_scale(p.z, h1, h.log_lo);
+        p.w = clamp_log_scale(p.w, h1, h.log_lo);
+      }
+      reinterpret_cast<float4*>(T.p)[i] = p;
+      reinterpret_cast<float4*>(T.m)[i] = m;
+      reinterpret_cast<float4*>(T.v)[i] = v;
+    }
+    for (int64_t e = 4 * n4 + tid; e < T.len; e += stride) {
+      float m = T.m[e], v = T.v[e];
+      float p = adam(T.p[e], T.g[e], m, v, step, st);
+      if (k == 1) p = clamp_log_scale(p, hi_of(e), h.log_lo);
+      T.p[e] = p;
+      T.m[e] = m;
+      T.v[e] = v;
     }
   }
   __syncthreads();
@@ -123,7 +183,6 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
 }
-
 }  // namespace
 }  // namespace ss
 
@@ -156,8 +215,6 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
   if (!(beta1 >= 0.0 && beta1 < 1.0 && beta2 >= 0.0 && beta2 < 1.0))
     return fail(SS_ERR_INVALID_ARGUMENT, "Adam betas must lie in [0, 1)");
   FieldPtrs p{params[0], params[1], params[2], params[3], params[4]};
-  FieldPtrs m{exp_avg[0], exp_avg[1], exp_avg[2], exp_avg[3], exp_avg[4]};
-  FieldPtrs v{exp_avg_sq[0], exp_avg_sq[1], exp_avg_sq[2], exp_avg_sq[3], exp_avg_sq[4]};
   AdamHyper h;
   for (int k = 0; k < 5; ++k) h.lr[k] = lrs[k];
   h.beta1 = beta1;
@@ -165,21 +222,44 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
   h.eps = (float)adam_eps;
   h.log_lo = log_scale_lo;
   h.dilation = dilation;
-  const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const Splat* rec = static_cast<const Splat*>(records);
   float* ws = static_cast<float*>(workspace);
+  const FitGrads fg = fit_grads_layout(
+      static_cast<char*>(workspace) + fit_grads_offset(n, gid_capacity, deterministic), n);
+  const FieldPtrs gp{fg.means, fg.log_scales, fg.rotations, fg.colors, p.logits ? fg.logits : nullptr};
   cudaStream_t s = as_stream(stream);
+  // gradients: a grid of at most 8 blocks per SM, grid-stride beyond that
+  const int64_t want = (n + kThreads - 1) / kThreads, cap_blocks = (int64_t)sms * 8;
+  const unsigned blocks = (unsigned)(want < cap_blocks ? want : cap_blocks);
   if (deterministic) {
     const EntryOrder eo = entry_order_layout(workspace, n, gid_capacity);
-    fit_update_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, f, nullptr, eo.partials,
-                                                        eo.order, eo.seg, p, m, v, h,
-                                                        log_scale_hi, step_state);
+    fit_grad_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, nullptr, eo.partials, eo.order,
+                                                      eo.seg, p.log_scales, p.rotations,
+                                                      p.logits, dilation, gp);
   } else {
-    fit_update_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, f, ws, nullptr, nullptr,
-                                                         nullptr, p, m, v, h, log_scale_hi,
-                                                         step_state);
+    fit_grad_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ws, nullptr, nullptr, nullptr,
+                                                       p.log_scales, p.rotations, p.logits,
+                                                       dilation, gp);
   }
-  return check_launch("fit_adam_update");
+  if ((rc = check_launch("fit gradients"))) return rc;
+  // the Adam step over the five tensors as flat arrays
+  AdamTensors ts;
+  const int64_t lens[5] = {2 * n, 2 * n, n, 3 * n, p.logits ? n : 0};
+  float* gptr[5] = {fg.means, fg.log_scales, fg.rotations, fg.colors, fg.logits};
+  for (int k = 0; k < 5; ++k) {
+    ts.t[k].p = params[k];
+    ts.t[k].m = exp_avg[k];
+    ts.t[k].v = exp_avg_sq[k];
+    ts.t[k].g = gptr[k];
+    ts.t[k].len = lens[k];
+  }
+  const int64_t want4 = (3 * n / 4 + kThreads - 1) / kThreads + 1;
+  const unsigned ablocks = (unsigned)(want4 < cap_blocks ? want4 : cap_blocks);
+  adam_kernel<<<ablocks, kThreads, 0, s>>>(ts, h, f, log_scale_hi, step_state);
+  return check_launch("fit adam step");
 }
 
 }  // extern "C"

@@ -880,6 +880,15 @@ int check_batch_render(const ss_batch* batch, int64_t n, float eps, Frames* f) {
 }
 
 }  // namespace
+
+size_t fit_grads_offset(int64_t n, int64_t cap, int deterministic) {
+  return align_up256(backward_ws_bytes(n, cap, deterministic));
+}
+
+size_t fit_ws_bytes(int64_t n, int64_t cap, int deterministic) {
+  return fit_grads_offset(n, cap, deterministic) + fit_grads_bytes(n);
+}
+
 }  // namespace ss
 
 using namespace ss;
@@ -1100,7 +1109,7 @@ int ss_fit_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int determi
                                     size_t* bytes) {
   if (!bytes) return fail(SS_ERR_INVALID_ARGUMENT, "null bytes pointer");
   if (n < 0 || gid_capacity < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
-  *bytes = backward_ws_bytes(n, gid_capacity, deterministic);
+  *bytes = fit_ws_bytes(n, gid_capacity, deterministic);
   return SS_OK;
 }
 
@@ -1113,7 +1122,7 @@ int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
   int rc = check_batch_render(batch, n, 1.0f, &f);
   if (rc) return rc;
   if (n == 0) return SS_OK;
-  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
+  const size_t need = fit_ws_bytes(n, gid_capacity, deterministic);
   if (batch->pixels == 0) {  // nothing rendered; the update sums no entries
     if (!deterministic) return SS_OK;
     if (workspace_bytes < need || !workspace)

@@ -127,9 +127,13 @@ def test_batch_validation_without_gpu(lib):
     assert rc == 1 and "loss_kind" in msg
     rc, msg = _status(lib, "ss_fit_backward_workspace_bytes", 10, 100, 1, ctypes.byref(size))
     # 12-float partials, two key and two order arrays per entry, begin/end per Gaussian (each
-    # 256-byte aligned), then the radix sort's scratch (queried from CUB; none without a GPU)
+    # 256-byte aligned), the radix sort's scratch (queried from CUB; none without a GPU), then
+    # the five gradient arrays of the Adam step (each 256-byte aligned)
     fixed = 4864 + 4 * 512 + 256
-    assert rc == 0 and size.value >= fixed and size.value % 256 == 0
+    grads = 5 * 256
+    assert rc == 0 and size.value >= fixed + grads and size.value % 256 == 0
+    rc, msg = _status(lib, "ss_fit_backward_workspace_bytes", 10, 100, 0, ctypes.byref(size))
+    assert rc == 0 and size.value == 512 + grads  # moments 360 B, then the gradients
     lrs = (ctypes.c_double * 5)(*([1e-2] * 5))
     ptrs = (ctypes.c_void_p * 5)()
     rc, msg = _status(lib, "ss_fit_adam_update", ctypes.byref(b), None, 10, None, 0, None, 0,
