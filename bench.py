@@ -625,10 +625,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--e2e-check", type=int, default=25)
     ap.add_argument("--psnr-thresholds", default="30,33,35,36,37,38,39")
+    ap.add_argument("--dependent-launch", type=int, default=1, choices=[0, 1],
+                    help="programmatic dependent launch of the library's kernels (1: on)")
     ap.add_argument("--profile", action="store_true",
                     help="only replay the captured step (for ncu launch lists)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.impl == "ours":
+        from structsplat_b200 import _native
+        _native.call("ss_set_dependent_launch", args.dependent_launch)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -710,6 +715,7 @@ def main():
                        "pairs": P, "tile_entries": res["entries"],
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}",
+                       "dependent_launch": args.dependent_launch,
                        "step": "one captured CUDA graph: RS projection, tile binning, forward, "
                                "backward, RS chain rule"},
             "roofline": {"bound": "fp32", "kernel": "backward_kernel",

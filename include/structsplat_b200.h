@@ -68,6 +68,12 @@ typedef struct ss_batch {
 
 /* ---------------------------------------------------------------- library */
 const char* ss_last_error(void);
+/* Programmatic dependent launch of the library's kernels (no counterpart in the reference):
+ * with 1 (the default) a kernel may become resident while its predecessor in the stream
+ * drains and waits on the device for that predecessor's results; 0 launches plainly.  Results
+ * do not depend on it.  Process-wide. */
+int ss_set_dependent_launch(int enable);
+int ss_get_dependent_launch(void);
 int ss_version(void);
 /* Bytes of one packed splat record (64). */
 size_t ss_splat_record_bytes(void);

@@ -62,6 +62,8 @@ SIGNATURES = {
     "ss_render_forward": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _f32, _f32, _vp, _vp,
                           _vp, _vp],
     "ss_set_backward_warps": [_int, _int],
+    "ss_set_dependent_launch": [_int],
+    "ss_get_dependent_launch": [],
     "ss_get_backward_warps": [_int],
     "ss_render_backward_workspace_bytes": [_i64, _i64, _int, _int, _int, _szp],
     "ss_render_backward": [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _int, _int, _int,

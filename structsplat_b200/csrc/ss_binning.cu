@@ -186,6 +186,8 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
 template <bool CULL>
 __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, Frames frames,
                                   float cutoff2, int* __restrict__ tile_count) {
+  pdl_wait();
+  pdl_trigger();
   enumerate_pairs<CULL>(rec, n, ts, frames, cutoff2,
                         [&](int, int, int t) { atomicAdd(tile_count + (int64_t)t * kCounterStride, 1); });
 }
@@ -199,6 +201,8 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
                                  int* __restrict__ tile_count, int32_t* __restrict__ offsets32,
                                  int32_t* __restrict__ gids, int64_t cap, int* big_count,
                                  uint32_t* status) {
+  pdl_wait();
+  pdl_trigger();
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int64_t stride = (int64_t)gridDim.x * blockDim.x;
   long long total = off64[T];
@@ -238,6 +242,8 @@ constexpr int64_t kSingleScanMax = (int64_t)kScanThreads * kScanPerThread;
 __global__ void __launch_bounds__(kScanThreads)
     single_scan_kernel(const int* __restrict__ tile_count, int64_t items,
                        long long* __restrict__ off64, int32_t* __restrict__ off32) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ long long warp_total[kScanThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t base = (int64_t)tid * kScanPerThread;
@@ -363,6 +369,8 @@ __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __re
                                                              int32_t* __restrict__ gids,
                                                              int64_t cap, int64_t T,
                                                              int* big_tiles, int* big_count) {
+  pdl_wait();
+  pdl_trigger();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t t = (int64_t)blockIdx.x * (kThreads / 32) + warp;
   if (t >= T) return;
@@ -393,6 +401,8 @@ __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __re
                                                              int32_t* __restrict__ gids,
                                                              const int* __restrict__ big_tiles,
                                                              const int* __restrict__ big_count) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ int sbuf[];
   int count = *big_count;
   for (int k = blockIdx.x; k < count; k += gridDim.x) {
@@ -459,16 +469,16 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
   if (n > 0 && T > 0) {
     int blocks = (int)((n + kThreads - 1) / kThreads);
     if (ellipse_cull)
-      tile_count_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2,
+      launch("tile_count_kernel", tile_count_kernel<true>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2,
                                                           w.tile_count);
     else
-      tile_count_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2,
+      launch("tile_count_kernel", tile_count_kernel<false>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2,
                                                            w.tile_count);
     if ((rc = check_launch("tile_count"))) return rc;
   }
   (void)status;
   if (T + 1 <= kSingleScanMax) {
-    single_scan_kernel<<<1, kScanThreads, 0, s>>>(w.tile_count, T + 1, w.offsets64,
+    launch("single_scan_kernel", single_scan_kernel, 1, kScanThreads, 0, s, w.tile_count, T + 1, w.offsets64,
                                                   tile_offsets);
     return check_launch("tile_offsets scan");
   }
@@ -479,7 +489,7 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
                                                  (int)(T + 1), s);
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, "tile offsets scan: %s", cudaGetErrorString(e));
   // int32 offsets for callers that only run stage 1 (the fill rewrites them identically).
-  tile_fill_kernel<false><<<(int)((T + 1 + kThreads - 1) / kThreads), kThreads, 0, s>>>(
+  launch("tile_fill_kernel", tile_fill_kernel<false>, (int)((T + 1 + kThreads - 1) / kThreads), kThreads, 0, s, 
       rec, 0, ts, frames, cutoff2, T, w.offsets64, w.tile_count, tile_offsets, nullptr,
       INT64_MAX, w.big_count, nullptr);
   return check_launch("tile_offsets");
@@ -505,22 +515,22 @@ int index_fill(const Frames& frames, int ts, int64_t T, const void* records, int
   int blocks = (int)((threads_needed + kThreads - 1) / kThreads);
   int32_t* offsets32 = const_cast<int32_t*>(tile_offsets);
   if (ellipse_cull)
-    tile_fill_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2, T,
+    launch("tile_fill_kernel", tile_fill_kernel<true>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2, T,
                                                        w.offsets64, w.tile_count, offsets32,
                                                        tile_gids, gid_capacity, w.big_count,
                                                        status);
   else
-    tile_fill_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ts, frames, cutoff2, T,
+    launch("tile_fill_kernel", tile_fill_kernel<false>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2, T,
                                                         w.offsets64, w.tile_count, offsets32,
                                                         tile_gids, gid_capacity, w.big_count,
                                                         status);
   if ((rc = check_launch("tile_fill"))) return rc;
   int sort_blocks = (int)((T + (kThreads / 32) - 1) / (kThreads / 32));
-  tile_sort_kernel<<<sort_blocks, kThreads, 0, s>>>(tile_offsets, tile_gids, gid_capacity, T,
+  launch("tile_sort_kernel", tile_sort_kernel, sort_blocks, kThreads, 0, s, tile_offsets, tile_gids, gid_capacity, T,
                                                      w.big_tiles, w.big_count);
   if ((rc = check_launch("tile_sort"))) return rc;
   if ((rc = allow_big_sort_smem())) return rc;
-  tile_sort_big_kernel<<<kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s>>>(
+  launch("tile_sort_big_kernel", tile_sort_big_kernel, kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s, 
       tile_offsets, tile_gids, w.big_tiles, w.big_count);
   return check_launch("tile_sort_big");
 }

@@ -33,6 +33,43 @@ int check_launch(const char* what);
 
 inline cudaStream_t as_stream(ss_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Programmatic dependent launch.  The kernels of a step (projection, binning, forward,
+// backward, epilogues, update) are launched with the programmatic-serialization attribute, so a
+// kernel's CTAs may become resident while its predecessor in the stream drains.  Every kernel
+// of the library therefore begins with pdl_wait(): it returns once the preceding grid has
+// completed and its writes are visible (immediately when the launch had no attribute), and
+// nothing before it reads another kernel's output.  pdl_trigger() then lets the next grid
+// launch.  dependent_launch_enabled() is the process-wide switch (ss_set_dependent_launch).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+bool dependent_launch_enabled();
+void note_launch_error(cudaError_t e);
+
+// Launches `kern` on `s` with the programmatic-serialization attribute when enabled; returns
+// SS_OK or the launch error, which the next check_launch of the thread also reports.
+template <typename... KArgs, typename... Args>
+int launch(const char* what, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+           cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = dependent_launch_enabled() ? 1 : 0;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+  if (e != cudaSuccess) {
+    note_launch_error(e);  // the caller's next check_launch reports it too
+    return fail(SS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  return SS_OK;
+}
+
 // 2^x on the SFU (PTX ex2.approx.ftz.f32: one MUFU operation, documented max relative error
 // 2^-22; results below 2^-126 flush to zero, which for a weight is an absolute error < 1.2e-38).
 __device__ __forceinline__ float fast_exp2(float x) {

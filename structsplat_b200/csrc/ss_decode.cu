@@ -28,6 +28,8 @@ __host__ __device__ inline int item_bytes(int bits) { return bits <= 8 ? 1 : (bi
 
 __global__ void unpack_kernel(const uint8_t* __restrict__ raw, int bits, int planar,
                               int64_t count, uint32_t* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int nb = item_bytes(bits);
@@ -58,6 +60,8 @@ __global__ void dequant_kernel(const uint32_t* __restrict__ qm, const uint32_t* 
                                float* __restrict__ means, float* __restrict__ log_scales,
                                float* __restrict__ rotations, float* __restrict__ colors,
                                float* __restrict__ logits) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
   const int64_t n = a.n;

@@ -61,6 +61,8 @@ __global__ void __launch_bounds__(kThreads)
                     const int32_t* __restrict__ seg, const float* __restrict__ log_scales,
                     const float* __restrict__ rotations, const float* __restrict__ logits,
                     float dilation, FieldPtrs grad) {
+  pdl_wait();
+  pdl_trigger();
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n;
@@ -123,6 +125,8 @@ __device__ __forceinline__ float clamp_log_scale(float x, float hi, float lo) {
 __global__ void __launch_bounds__(kThreads)
     adam_kernel(AdamTensors ts, AdamHyper h, Frames frames, const float* __restrict__ log_hi,
                 int* __restrict__ step_state) {
+  pdl_wait();
+  pdl_trigger();
   const int t = step_state[0] + 1;
   AdamStep st;
   st.w1 = (float)(1.0 - h.beta1);
@@ -236,11 +240,11 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
   const unsigned blocks = (unsigned)(want < cap_blocks ? want : cap_blocks);
   if (deterministic) {
     const EntryOrder eo = entry_order_layout(workspace, n, gid_capacity);
-    fit_grad_kernel<true><<<blocks, kThreads, 0, s>>>(rec, n, nullptr, eo.partials, eo.order,
+    launch("fit_grad_kernel", fit_grad_kernel<true>, blocks, kThreads, 0, s, rec, n, nullptr, eo.partials, eo.order,
                                                       eo.seg, p.log_scales, p.rotations,
                                                       p.logits, dilation, gp);
   } else {
-    fit_grad_kernel<false><<<blocks, kThreads, 0, s>>>(rec, n, ws, nullptr, nullptr, nullptr,
+    launch("fit_grad_kernel", fit_grad_kernel<false>, blocks, kThreads, 0, s, rec, n, ws, nullptr, nullptr, nullptr,
                                                        p.log_scales, p.rotations, p.logits,
                                                        dilation, gp);
   }
@@ -258,7 +262,7 @@ int ss_fit_adam_update(const ss_batch* batch, const void* records, int64_t n,
   }
   const int64_t want4 = (3 * n / 4 + kThreads - 1) / kThreads + 1;
   const unsigned ablocks = (unsigned)(want4 < cap_blocks ? want4 : cap_blocks);
-  adam_kernel<<<ablocks, kThreads, 0, s>>>(ts, h, f, log_scale_hi, step_state);
+  launch("adam_kernel", adam_kernel, ablocks, kThreads, 0, s, ts, h, f, log_scale_hi, step_state);
   return check_launch("fit adam step");
 }
 

@@ -27,6 +27,8 @@ template <int G, bool FADE>
 __global__ void __launch_bounds__(kThreads)
     activity_kernel(const Splat* __restrict__ rec, int64_t n, float tail,
                     float* __restrict__ activity) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t gid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
   const int sub = threadIdx.x % G;
   float acc = 0.f;

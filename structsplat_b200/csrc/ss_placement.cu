@@ -48,6 +48,8 @@ __device__ __forceinline__ double np_clip(double x, double lo, double hi) {
 __global__ void density_kernel(const float* __restrict__ energy, int64_t n,
                                const double* __restrict__ ref, double base, double power,
                                double* __restrict__ d) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double e = (double)energy[i];
@@ -58,6 +60,8 @@ __global__ void density_kernel(const float* __restrict__ energy, int64_t n,
 
 __global__ void normalize_kernel(double* __restrict__ d, int64_t n,
                                  const double* __restrict__ sum, int uniform_if_empty) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double s = *sum;
@@ -76,6 +80,8 @@ __device__ __forceinline__ double reflect(double v, double hi) {
 __global__ void sample_kernel(const double* __restrict__ cdf, int64_t npx, int W, int H,
                               const double* __restrict__ uniforms, int64_t n,
                               double* __restrict__ pts, int64_t* __restrict__ index_out) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double last = cdf[npx - 1];
@@ -127,6 +133,8 @@ __global__ void place_kernel(const double* __restrict__ pts, int64_t n,
                              const float* __restrict__ image, int H, int W, PlaceParams pp,
                              float* __restrict__ means, float* __restrict__ log_scales,
                              float* __restrict__ rotations, float* __restrict__ colors) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double px = pts[2 * i], py = pts[2 * i + 1];

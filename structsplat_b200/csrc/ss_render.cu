@@ -174,6 +174,8 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
                    float tail, float* __restrict__ out, float* __restrict__ den,
                    const float* __restrict__ target, float4* __restrict__ pixel_grad,
                    float* __restrict__ loss, float charb_eps2) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = Tiling<TS>::kFwdThreads;
   __shared__ __align__(16) float4 stage[kStageAll][4];
   const int tile = blockIdx.x;
@@ -304,6 +306,8 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
                     int64_t cap, const int32_t* __restrict__ offsets, Frames frames,
                     int normalize, float eps, float tail, float* __restrict__ moments,
                     float* __restrict__ partials, uint32_t* status) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
   constexpr int kHalf = kStageMax / 2;  // entries per chunk when a long list streams through
   __shared__ __align__(16) float4 stage[kStageMax][4];
@@ -553,6 +557,8 @@ __global__ void finalize_moments_kernel(const Splat* __restrict__ rec, int64_t n
                                         float* __restrict__ g_conics,
                                         float* __restrict__ g_colors,
                                         float* __restrict__ g_opac) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
   float m[kMoments];
@@ -571,6 +577,8 @@ __global__ void reduce_partials_kernel(const Splat* __restrict__ rec, int64_t n,
                                        float* __restrict__ g_conics,
                                        float* __restrict__ g_colors,
                                        float* __restrict__ g_opac) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   float acc[kMoments];
   sum_entry_partials(partials, order, seg, n, g, g < n, acc);
@@ -592,6 +600,8 @@ __global__ void finalize_rs_kernel(const Splat* __restrict__ rec, int64_t n,
                                    float* __restrict__ g_means, float* __restrict__ g_ls,
                                    float* __restrict__ g_rot, float* __restrict__ g_colors,
                                    float* __restrict__ g_logits) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   float m[kMoments];
   if (DETERMINISTIC) sum_entry_partials(ws, order, seg, n, g, g < n, m);
@@ -622,6 +632,8 @@ __global__ void entry_keys_kernel(const int32_t* __restrict__ gids,
                                   const int32_t* __restrict__ offsets, int64_t T, int64_t cap,
                                   int64_t n, uint32_t* __restrict__ keys,
                                   int32_t* __restrict__ order) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t last = offsets[T];
   const int64_t total = last < cap ? last : cap;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -634,6 +646,8 @@ __global__ void entry_keys_kernel(const int32_t* __restrict__ gids,
 
 __global__ void entry_segments_kernel(const uint32_t* __restrict__ keys, int64_t cap, int64_t n,
                                       int32_t* __restrict__ seg) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
     const uint32_t k = keys[i];
@@ -671,7 +685,7 @@ int order_entries(const int32_t* gids, const int32_t* offsets, int64_t T, int64_
   const EntryOrder eo = entry_order_layout(ws, n, cap);
   const int64_t want = (cap + kEpilogueThreads - 1) / kEpilogueThreads;
   const unsigned blocks = (unsigned)(want < 148 * 16 ? want : 148 * 16);
-  entry_keys_kernel<<<blocks, kEpilogueThreads, 0, s>>>(gids, offsets, T, cap, n, eo.keys_in,
+  launch("entry_keys_kernel", entry_keys_kernel, blocks, kEpilogueThreads, 0, s, gids, offsets, T, cap, n, eo.keys_in,
                                                          eo.order_in);
   if ((rc = check_launch("entry keys"))) return rc;
   size_t tb = sort_temp_bytes(n, cap);
@@ -679,7 +693,7 @@ int order_entries(const int32_t* gids, const int32_t* offsets, int64_t T, int64_
                                                   eo.order, (int)cap, 0, key_bits(n), s);
   if (e != cudaSuccess)
     return fail(SS_ERR_CUDA, "entry order sort: %s", cudaGetErrorString(e));
-  entry_segments_kernel<<<blocks, kEpilogueThreads, 0, s>>>(eo.keys, cap, n, eo.seg);
+  launch("entry_segments_kernel", entry_segments_kernel, blocks, kEpilogueThreads, 0, s, eo.keys, cap, n, eo.seg);
   return check_launch("entry segments");
 }
 
@@ -700,9 +714,8 @@ void launch_forward_loss(int loss_kind, unsigned T, cudaStream_t s, const Splat*
                          const float* target, float4* pixel_grad, float* loss, float ce2) {
   constexpr int NT = Tiling<TS>::kFwdThreads;
 #define SS_FWD(LOSS)                                                                          \
-  forward_kernel<TS, NORM, FADE, LOSS><<<T, NT, 0, s>>>(rec, n, gids, cap, offsets, f, eps,   \
-                                                        tail, out, den, target, pixel_grad,   \
-                                                        loss, ce2)
+  launch("forward_kernel", forward_kernel<TS, NORM, FADE, LOSS>, T, NT, 0, s, rec, n, gids,   \
+         cap, offsets, f, eps, tail, out, den, target, pixel_grad, loss, ce2)
   switch (loss_kind) {
     case kL1: SS_FWD(kL1); break;
     case kL2: SS_FWD(kL2); break;
@@ -740,9 +753,9 @@ void launch_backward_nt(unsigned T, cudaStream_t s, bool deterministic, const fl
                         float tail, float* ws, uint32_t* status) {
   const bool fade = tail > 0.0f;
 #define SS_BWD(FADE, DET)                                                                     \
-  backward_kernel<TS, NT, FADE, DET, PIXGRAD><<<T, NT, 0, s>>>(                              \
-      grad_out, rec, n, den, out, pixel_grad, gids, cap, offsets, f, normalize, eps, tail, ws, \
-      ws, status)
+  launch("backward_kernel", backward_kernel<TS, NT, FADE, DET, PIXGRAD>, T, NT, 0, s, grad_out, \
+         rec, n, den, out, pixel_grad, gids, cap, offsets, f, normalize, eps, tail, ws, ws,    \
+         status)
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
@@ -864,11 +877,11 @@ int render_backward(const Frames& f, int ts, int64_t T, int64_t npx, const float
   const unsigned gblocks = (unsigned)((n + kEpilogueThreads - 1) / kEpilogueThreads);
   if (deterministic) {
     const EntryOrder eo = entry_order_layout(ws, n, cap);
-    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("reduce_partials_kernel", reduce_partials_kernel, gblocks, kEpilogueThreads, 0, s, 
         rec, n, eo.partials, eo.order, eo.seg, has_opacity, grad_means, grad_conics,
         grad_colors, grad_opacities);
   } else
-    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("finalize_moments_kernel", finalize_moments_kernel, gblocks, kEpilogueThreads, 0, s, 
         rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
   return check_launch("backward epilogue");
 }
@@ -1023,11 +1036,11 @@ int ss_render_backward_finalize(const void* records, int64_t n, const int32_t* t
   cudaStream_t s = as_stream(stream);
   if (deterministic) {
     const EntryOrder eo = entry_order_layout(const_cast<float*>(ws), n, gid_capacity);
-    reduce_partials_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("reduce_partials_kernel", reduce_partials_kernel, gblocks, kEpilogueThreads, 0, s, 
         rec, n, eo.partials, eo.order, eo.seg, has_opacity, grad_means, grad_conics,
         grad_colors, grad_opacities);
   } else
-    finalize_moments_kernel<<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("finalize_moments_kernel", finalize_moments_kernel, gblocks, kEpilogueThreads, 0, s, 
         rec, n, ws, has_opacity, grad_means, grad_conics, grad_colors, grad_opacities);
   return check_launch("backward finalize");
 }
@@ -1053,11 +1066,11 @@ int ss_render_backward_finalize_rs(const void* records, int64_t n, const int32_t
   cudaStream_t s = as_stream(stream);
   if (deterministic) {
     const EntryOrder eo = entry_order_layout(const_cast<float*>(ws), n, gid_capacity);
-    finalize_rs_kernel<true><<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("finalize_rs_kernel", finalize_rs_kernel<true>, gblocks, kEpilogueThreads, 0, s, 
         rec, n, eo.partials, eo.order, eo.seg, log_scales, rotations, opacity_logits, dilation,
         grad_means, grad_log_scales, grad_rotations, grad_colors, grad_opacity_logits);
   } else {
-    finalize_rs_kernel<false><<<gblocks, kEpilogueThreads, 0, s>>>(
+    launch("finalize_rs_kernel", finalize_rs_kernel<false>, gblocks, kEpilogueThreads, 0, s, 
         rec, n, ws, nullptr, nullptr, log_scales, rotations, opacity_logits, dilation,
         grad_means, grad_log_scales, grad_rotations, grad_colors, grad_opacity_logits);
   }

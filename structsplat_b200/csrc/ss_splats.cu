@@ -1,5 +1,6 @@
 // Library plumbing (errors, version) and the per-Gaussian kernels: record packing and the
 // fused RS projection with its chain rule.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 
@@ -17,8 +18,21 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+namespace {
+thread_local cudaError_t t_launch_error = cudaSuccess;  // a failed cudaLaunchKernelEx
+std::atomic<int> g_dependent_launch{1};
+}  // namespace
+
+void note_launch_error(cudaError_t e) { t_launch_error = e; }
+
+bool dependent_launch_enabled() {
+  return g_dependent_launch.load(std::memory_order_relaxed) != 0;
+}
+
 int check_launch(const char* what) {
   cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = t_launch_error;
+  t_launch_error = cudaSuccess;
   if (e != cudaSuccess) return fail(SS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
   return SS_OK;
 }
@@ -56,6 +70,8 @@ __global__ void pack_splats_kernel(const float* __restrict__ means,
                                    const int64_t* __restrict__ radii,
                                    const float* __restrict__ opacities, int64_t n, int H, int W,
                                    Splat* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float mx = means[2 * i], my = means[2 * i + 1];
@@ -78,6 +94,8 @@ __global__ void project_rs_kernel(const float* __restrict__ means,
                                   float cutoff, Frames frames, Splat* __restrict__ out,
                                   float* __restrict__ conics_out,
                                   int64_t* __restrict__ radii_out) {
+  pdl_wait();
+  pdl_trigger();
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float sx = expf(log_scales[2 * i]), sy = expf(log_scales[2 * i + 1]);
@@ -130,6 +148,8 @@ __global__ void project_rs_backward_kernel(const float* __restrict__ log_scales,
                                            float* __restrict__ g_log_scales,
                                            float* __restrict__ g_rot,
                                            float* __restrict__ g_logits) {
+  pdl_wait();
+  pdl_trigger();
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   rs_conic_chain(log_scales[2 * i], log_scales[2 * i + 1], rotations[i], dilation,
@@ -147,6 +167,15 @@ extern "C" {
 
 const char* ss_last_error(void) { return ss::g_error; }
 
+int ss_set_dependent_launch(int enable) {
+  if (enable != 0 && enable != 1)
+    return fail(SS_ERR_INVALID_ARGUMENT, "dependent launch switch must be 0 or 1");
+  ss::g_dependent_launch.store(enable, std::memory_order_relaxed);
+  return SS_OK;
+}
+
+int ss_get_dependent_launch(void) { return ss::dependent_launch_enabled() ? 1 : 0; }
+
 int ss_version(void) { return 1; }
 
 size_t ss_splat_record_bytes(void) { return sizeof(Splat); }
@@ -161,7 +190,7 @@ int ss_pack_splats(const float* means, const float* conics, const float* colors,
     return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (reinterpret_cast<uintptr_t>(records) % 16)
     return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
-  pack_splats_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+  launch("pack_splats_kernel", pack_splats_kernel, blocks_for(n), kThreads, 0, as_stream(stream), 
       means, conics, colors, radii, opacities, n, height, width,
       reinterpret_cast<Splat*>(records));
   return check_launch("pack_splats");
@@ -178,7 +207,7 @@ static int project_rs(const Frames& frames, const float* means, const float* log
     return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (reinterpret_cast<uintptr_t>(records) % 16)
     return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
-  project_rs_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+  launch("project_rs_kernel", project_rs_kernel, blocks_for(n), kThreads, 0, as_stream(stream), 
       means, log_scales, rotations, colors, opacity_logits, n, dilation, sigma_cutoff, frames,
       reinterpret_cast<Splat*>(records), conics_out, radii_out);
   return check_launch("project_rs");
@@ -214,7 +243,7 @@ int ss_project_rs_backward(const float* log_scales, const float* rotations,
   if (n == 0) return SS_OK;
   if (!log_scales || !rotations || !grad_conics || !grad_log_scales || !grad_rotations)
     return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
-  project_rs_backward_kernel<<<blocks_for(n), kThreads, 0, as_stream(stream)>>>(
+  launch("project_rs_backward_kernel", project_rs_backward_kernel, blocks_for(n), kThreads, 0, as_stream(stream), 
       log_scales, rotations, opacity_logits, n, dilation, grad_conics, grad_opacities,
       grad_log_scales, grad_rotations, grad_opacity_logits);
   return check_launch("project_rs_backward");

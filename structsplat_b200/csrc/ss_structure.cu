@@ -38,6 +38,8 @@ __device__ __forceinline__ int reflect(int i, int n) {
 // Source maps: luma (one map) or the first `chans` colour channels.
 __global__ void source_maps_kernel(const float* __restrict__ img, int H, int W, int C,
                                    int rgb, float* __restrict__ maps) {
+  pdl_wait();
+  pdl_trigger();
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= W || y >= H) return;
   const int64_t p = (int64_t)y * W + x, HW = (int64_t)H * W;
@@ -56,6 +58,8 @@ __global__ void source_maps_kernel(const float* __restrict__ img, int H, int W, 
 template <bool ALONG_Y>
 __global__ void blur_kernel(const float* __restrict__ src, float* __restrict__ dst, int H, int W,
                             Taps taps) {
+  pdl_wait();
+  pdl_trigger();
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= W || y >= H) return;
   const int64_t HW = (int64_t)H * W;
@@ -71,6 +75,8 @@ __global__ void blur_kernel(const float* __restrict__ src, float* __restrict__ d
 // Gradients of each smoothed map and the channel-summed outer products (Jxx, Jxy, Jyy).
 __global__ void tensor_kernel(const float* __restrict__ maps, int chans, int H, int W,
                               int op, float* __restrict__ J) {
+  pdl_wait();
+  pdl_trigger();
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= W || y >= H) return;
   const int64_t HW = (int64_t)H * W, p = (int64_t)y * W + x;
@@ -113,6 +119,8 @@ __global__ void eigen_kernel(const float* __restrict__ J, int64_t HW, float* __r
                              float* __restrict__ lam2, float* __restrict__ angle,
                              float* __restrict__ coherence, float* __restrict__ energy,
                              float* __restrict__ energy_keys) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= HW) return;
   const float jxx = J[p], jxy = J[HW + p], jyy = J[2 * HW + p];
@@ -147,6 +155,8 @@ __device__ double quantile_sorted(const float* s, int64_t n, double q) {
 
 __global__ void stats_kernel(const float* __restrict__ sorted, int64_t n, double flat_frac,
                              double* stats) {
+  pdl_wait();
+  pdl_trigger();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double med = 0.0;
   if (n > 0) {
@@ -164,6 +174,8 @@ __global__ void stats_kernel(const float* __restrict__ sorted, int64_t n, double
 __global__ void label_kernel(const float* __restrict__ energy, const float* __restrict__ lam2,
                              int64_t HW, const double* __restrict__ stats, double corner_frac,
                              uint8_t* __restrict__ label) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= HW) return;
   // The thresholds are Python floats compared against float32 arrays: NumPy casts them to

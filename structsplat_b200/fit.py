@@ -114,12 +114,13 @@ class RenderPlan:
                          int(self.normalize), float(self.eps), float(self.tail), _p(self.image),
                          _p(self.den), _p(self.status), _stream())
 
-    def backward(self, grad_out, params):
+    def backward(self, grad_out, params, moments_zeroed: bool = False):
         """Gradients w.r.t. the RS parameters: the backward tile kernel into moments (fast) or
-        entry partials (deterministic), then one per-Gaussian pass through the RS chain rule."""
+        entry partials (deterministic), then one per-Gaussian pass through the RS chain rule.
+        ``moments_zeroed``: the caller already cleared the fast-mode moments."""
         if not self.n:
             return
-        if not self.deterministic:
+        if not self.deterministic and not moments_zeroed:
             self.bwd_ws.zero_()
         self.backward_tiles(grad_out)
         _native.call("ss_render_backward_finalize_rs", _p(self.records), self.n, _p(self.gids),
@@ -160,8 +161,12 @@ class RenderPlan:
         return self.image
 
     def forward_backward(self, params, grad_out):
+        # the moments are cleared first so the step's kernels follow one another directly
+        # (each may start while its predecessor drains)
+        if self.n and not self.deterministic:
+            self.bwd_ws.zero_()
         self.forward(params)
-        self.backward(grad_out, params)
+        self.backward(grad_out, params, moments_zeroed=True)
         return self.grads()
 
     def grads(self):
