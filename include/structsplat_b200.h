@@ -236,6 +236,23 @@ int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
                     float fade_tail, const float* pixel_grad, int deterministic,
                     void* workspace, size_t workspace_bytes, uint32_t* status,
                     ss_stream_t stream);
+/* ss_fit_forward_loss followed by ss_fit_backward in one kernel launch: each tile's CTA stages
+ * its records once, renders its pixels, evaluates the pixel loss and keeps the loss gradient in
+ * shared memory for the tile's backward, so pixel_grad never goes through global memory.  The
+ * image, the loss (B,2) and the workspace's moments or partials are those of the two calls
+ * (the loss sums are float atomics in either form).  image (P,3), den (P) and loss are
+ * optional (NULL skips them; zero loss first).  The workspace is ss_fit_backward's (size
+ * ss_fit_backward_workspace_bytes); fast mode: moments zero on entry.  Deterministic mode: a
+ * tile whose list the capacity truncated raises SS_STATUS_DETERMINISTIC_TRUNCATED and renders
+ * nothing (re-plan with more capacity and redo the step).  No counterpart in the reference,
+ * whose fit loop runs its renderer and torch autograd as separate passes. */
+int ss_fit_forward_backward(const ss_batch* batch, const void* records, int64_t n,
+                            const int32_t* tile_gids, int64_t gid_capacity,
+                            const int32_t* tile_offsets, int normalize, float eps,
+                            float fade_tail, const float* target, int loss_kind,
+                            float charbonnier_eps, float* image, float* den, float* loss,
+                            int deterministic, void* workspace, size_t workspace_bytes,
+                            uint32_t* status, ss_stream_t stream);
 /* Gradients of the five parameter groups from the backward's workspace, then one Adam step
  * (torch.optim.Adam's multi-tensor step: lerp first moment, step factors formed in double, no
  * weight decay), then the clamp of log_scales to [log_scale_lo, log_scale_hi[image]] that the

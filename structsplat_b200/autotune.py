@@ -79,12 +79,15 @@ def _bucket(x: float) -> str:
 
 
 def workload_key(pixels: int, gaussians: int, entries: int, images: int, normalize: bool,
-                 fade: bool, deterministic: bool, fit: bool) -> str:
+                 fade: bool, deterministic: bool, fit: bool, fused: bool = False) -> str:
     dev = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return "|".join([dev, f"px={_bucket(pixels)}", f"g/px={_bucket(gaussians / max(pixels, 1))}",
-                     f"e/g={_bucket(entries / max(gaussians, 1))}", f"img={_bucket(images)}",
-                     f"norm={int(normalize)}", f"fade={int(fade)}", f"det={int(deterministic)}",
-                     f"fit={int(fit)}"])
+    parts = [dev, f"px={_bucket(pixels)}", f"g/px={_bucket(gaussians / max(pixels, 1))}",
+             f"e/g={_bucket(entries / max(gaussians, 1))}", f"img={_bucket(images)}",
+             f"norm={int(normalize)}", f"fade={int(fade)}", f"det={int(deterministic)}",
+             f"fit={int(fit)}"]
+    if fused:
+        parts.append("fused=1")
+    return "|".join(parts)
 
 
 def _time(fn, repeats: int) -> float:
@@ -164,8 +167,11 @@ def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
         plan = plans[ts]
 
         def run():
-            plan.forward_loss()
-            plan.backward()
+            if plan.s.fused:
+                plan.forward_backward()
+            else:
+                plan.forward_loss()
+                plan.backward()
         return run
 
     try:
@@ -173,7 +179,8 @@ def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
         entries = int(plans[candidates[0][0]].offsets[-1].item())
         pixels = sum(h * w for h, w in sizes)
         key = workload_key(pixels, sum(counts), entries, len(sizes), settings.normalize,
-                           settings.fade_alpha > 0, settings.deterministic, fit=True)
+                           settings.fade_alpha > 0, settings.deterministic, fit=True,
+                           fused=settings.fused)
         return _pick(key, candidates, build, repeats, use_cache)
     finally:
         for plan in plans.values():  # the probe backward added into the moments: clear them

@@ -123,6 +123,8 @@ class FitSettings:
     dilation: float = 0.0
     fade_alpha: float = 0.0
     deterministic: bool = False
+    # one tile kernel for forward, loss and backward (the same numbers as the two-kernel step)
+    fused: bool = True
     betas: tuple = (0.9, 0.999)
     adam_eps: float = 1e-8
     scale_min: float = 0.35  # log-scale floor ln(0.35) (fit.py:3033)
@@ -232,6 +234,17 @@ class FitPlan:
                      int(self.s.deterministic), _p(self.bwd_ws), self.bwd_ws_bytes,
                      _p(self.status), _stream())
 
+    def forward_backward(self):
+        """Forward, pixel loss and backward of every tile in one kernel (the loss gradient stays
+        on chip); the same images, losses and moments as forward_loss() + backward()."""
+        s = self.s
+        _native.call("ss_fit_forward_backward", self.batch.ref, _p(self.records), self.n,
+                     _p(self.gids), self.capacity, _p(self.offsets), int(s.normalize),
+                     float(s.eps), float(self.tail), _p(self.target), LOSS_KINDS[s.pixel_loss],
+                     float(s.charbonnier_eps), None, None, _p(self.loss),
+                     int(s.deterministic), _p(self.bwd_ws), self.bwd_ws_bytes, _p(self.status),
+                     _stream())
+
     def update(self):
         s = self.s
         _native.call("ss_fit_adam_update", self.batch.ref, _p(self.records), self.n,
@@ -247,8 +260,11 @@ class FitPlan:
         self.project()
         self.count()
         self.fill()
-        self.forward_loss()
-        self.backward()
+        if self.s.fused:
+            self.forward_backward()
+        else:
+            self.forward_loss()
+            self.backward()
         self.update()
 
     def render(self):

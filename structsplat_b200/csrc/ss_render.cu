@@ -162,11 +162,66 @@ __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int 
 // Pixel losses of fit.py:800-809 (mean over channels, then over the image's pixels).
 enum LossKind { kNoLoss = 0, kL1 = 1, kL2 = 2, kCharbonnier = 3 };
 
+// 1/(H W) then /3: autograd's factors for the mean over the image's pixels of the channel mean.
+__device__ __forceinline__ float pixel_loss_scale(int H, int W) {
+  const float per_pixel = 1.0f / (float)((int64_t)H * W);
+  return per_pixel / 3.0f;
+}
+
+// Finishes pixel p of a forward from its accumulators a = (num_r, num_g, num_b, den): writes
+// den and the image (LOSS == kNoLoss always, otherwise where the pointers are given) and, for a
+// fit iteration, returns the backward's per-pixel input (dL/dnum_rgb, dL/dden) with the pixel's
+// loss in lp and squared error in sq.  The loss gradient repeats autograd's arithmetic for the
+// mean-of-means, so it is bitwise the eager gradient.
+template <bool NORMALIZE, int LOSS>
+__device__ __forceinline__ float4 finish_pixel(const float* a, int64_t p, float eps,
+                                               float per_value, float charb_eps2, float* out,
+                                               float* den, const float* target, float& lp,
+                                               float& sq) {
+  float o[3];
+  const float denom = a[3] + eps;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) o[ch] = NORMALIZE ? a[ch] / denom : a[ch];
+  if (LOSS == kNoLoss || den) den[p] = a[3];
+  if (LOSS == kNoLoss || out) {
+    out[3 * p] = o[0];
+    out[3 * p + 1] = o[1];
+    out[3 * p + 2] = o[2];
+  }
+  lp = sq = 0.f;
+  if constexpr (LOSS == kNoLoss) {
+    return make_float4(0.f, 0.f, 0.f, 0.f);
+  } else {
+  float g[3];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const float d = o[ch] - target[3 * p + ch];
+    const float d2 = d * d;
+    sq += d2;
+    if (LOSS == kL2) {
+      g[ch] = per_value * d + per_value * d;
+      lp += d2;
+    } else if (LOSS == kL1) {
+      g[ch] = per_value * (float)((d > 0.f) - (d < 0.f));
+      lp += fabsf(d);
+    } else {
+      const float r = sqrtf(d2 + charb_eps2);
+      const float q = per_value / (2.0f * r);
+      g[ch] = q * d + q * d;
+      lp += r;
+    }
+  }
+  if (NORMALIZE)
+    return make_float4(g[0] / denom, g[1] / denom, g[2] / denom,
+                       -(g[0] * o[0] + g[1] * o[1] + g[2] * o[2]) / denom);
+  return make_float4(g[0], g[1], g[2], 0.f);
+  }
+}
+
 // Forward of one tile.  LOSS == kNoLoss: writes out and den.  Otherwise (a fit iteration) it
 // also evaluates the pixel loss against target and writes the backward's per-pixel input
 // pixel_grad = (dL/dnum_rgb, dL/dden) (out and den only when given) and adds each image's loss
-// and mean squared error into loss[2 b], loss[2 b + 1].  The loss gradient repeats autograd's
-// arithmetic for the mean-of-means (1/(H W) then /3) so it is bitwise the eager gradient.
+// and mean squared error into loss[2 b], loss[2 b + 1] (finish_pixel).
 template <int TS, bool NORMALIZE, bool FADE, int LOSS>
 __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
     forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
@@ -214,51 +269,17 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
     }
   }
   float loss_sum = 0.f, sq_sum = 0.f;
-  const float per_pixel = 1.0f / (float)((int64_t)H * W);  // autograd: grad / numel
-  const float per_value = per_pixel / 3.0f;                 // then the channel mean
+  const float per_value = pixel_loss_scale(H, W);
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     const int py = k ? py1 : py0;
     const float* a = k ? acc1 : acc0;
     if (px < W && py < H) {
       const int64_t p = fr.pixel_base + (int64_t)py * W + px;
-      float o[3];
-      const float denom = a[3] + eps;
-#pragma unroll
-      for (int ch = 0; ch < 3; ++ch) o[ch] = NORMALIZE ? a[ch] / denom : a[ch];
-      if (LOSS == kNoLoss || den) den[p] = a[3];
-      if (LOSS == kNoLoss || out) {
-        out[3 * p] = o[0];
-        out[3 * p + 1] = o[1];
-        out[3 * p + 2] = o[2];
-      }
+      float lp, sq;
+      const float4 v = finish_pixel<NORMALIZE, LOSS>(a, p, eps, per_value, charb_eps2, out, den,
+                                                     target, lp, sq);
       if (LOSS != kNoLoss) {
-        float g[3], lp = 0.f, sq = 0.f;
-#pragma unroll
-        for (int ch = 0; ch < 3; ++ch) {
-          const float d = o[ch] - target[3 * p + ch];
-          const float d2 = d * d;
-          sq += d2;
-          if (LOSS == kL2) {
-            g[ch] = per_value * d + per_value * d;
-            lp += d2;
-          } else if (LOSS == kL1) {
-            g[ch] = per_value * (float)((d > 0.f) - (d < 0.f));
-            lp += fabsf(d);
-          } else {
-            const float r = sqrtf(d2 + charb_eps2);
-            const float q = per_value / (2.0f * r);
-            g[ch] = q * d + q * d;
-            lp += r;
-          }
-        }
-        float4 v;
-        if (NORMALIZE) {
-          v = make_float4(g[0] / denom, g[1] / denom, g[2] / denom,
-                          -(g[0] * o[0] + g[1] * o[1] + g[2] * o[2]) / denom);
-        } else {
-          v = make_float4(g[0], g[1], g[2], 0.f);
-        }
         pixel_grad[p] = v;
         loss_sum += lp;
         sq_sum += sq;
@@ -293,19 +314,50 @@ __device__ __forceinline__ void scatter_level(const float (&v)[N], float (&w)[K]
   }
 }
 
+// Inputs and outputs of the fused fit tile pass (FUSED backward): the forward of the tile runs
+// first in the same CTA over the staged records and its loss gradient goes straight into the
+// backward's shared-memory pixel inputs.  image / den / loss are optional (NULL skips them).
+struct FusedFit {
+  const float* target;
+  float* image;
+  float* den;
+  float* loss;
+  int loss_kind;  // LossKind: kL1, kL2 or kCharbonnier
+  float charb_eps2;
+};
+
+// finish_pixel with the loss kind and normalisation chosen at run time (uniform per launch).
+__device__ __forceinline__ float4 finish_pixel_rt(int normalize, int loss_kind, const float* a,
+                                                  int64_t p, float eps, float per_value,
+                                                  float ce2, float* out, float* den,
+                                                  const float* target, float& lp, float& sq) {
+#define SS_FIN(N, K) finish_pixel<N, K>(a, p, eps, per_value, ce2, out, den, target, lp, sq)
+  if (normalize) {
+    if (loss_kind == kL1) return SS_FIN(true, kL1);
+    if (loss_kind == kL2) return SS_FIN(true, kL2);
+    return SS_FIN(true, kCharbonnier);
+  }
+  if (loss_kind == kL1) return SS_FIN(false, kL1);
+  if (loss_kind == kL2) return SS_FIN(false, kL2);
+  return SS_FIN(false, kCharbonnier);
+#undef SS_FIN
+}
+
 template <int TS, int NT>
 struct BackwardOccupancy {  // CTAs per SM the register budget is planned for
   static constexpr int kBlocks = TS == 16 ? (NT == 128 ? 6 : 4) : (NT == 256 ? 4 : 2);
 };
 
-template <int TS, int NT, bool FADE, bool DETERMINISTIC, bool PIXGRAD>
+// FUSED: the pixel inputs come from the tile's own forward (FusedFit) instead of grad_out /
+// out / den or pixel_grad.
+template <int TS, int NT, bool FADE, bool DETERMINISTIC, bool PIXGRAD, bool FUSED = false>
 __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     backward_kernel(const float* __restrict__ grad_out, const Splat* __restrict__ rec,
                     int64_t n, const float* __restrict__ den, const float* __restrict__ out,
                     const float4* __restrict__ pixel_grad, const int32_t* __restrict__ gids,
                     int64_t cap, const int32_t* __restrict__ offsets, Frames frames,
                     int normalize, float eps, float tail, float* __restrict__ moments,
-                    float* __restrict__ partials, uint32_t* status) {
+                    float* __restrict__ partials, uint32_t* status, FusedFit ff) {
   pdl_wait();
   pdl_trigger();
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
@@ -335,7 +387,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   // Per-pixel inputs of the tile: every load is issued before the first is used.
   constexpr int kPx = TS * TS / NT;
   static_assert(TS * TS % NT == 0, "pixels per thread");
-  {
+  if constexpr (!FUSED) {
     float4 va[kPx];
     float dn[kPx], o0[kPx], o1[kPx], o2[kPx];
 #pragma unroll
@@ -508,6 +560,89 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       work_group(st, ord, gsm, m, g, k0);
     }
   };
+  if constexpr (FUSED) {
+    // The tile's forward over the staged records, in forward_kernel's per-pixel order (so the
+    // image, the loss gradient and the moments are bitwise those of the two-kernel step), then
+    // each pixel's loss gradient straight into pix.  Warp w takes the 8x8 blocks w, w + NT/32, …
+    constexpr int kBlocks = (TS / 8) * (TS / 8);
+    constexpr int kWarps = NT / 32;
+    constexpr int kPer = (kBlocks + kWarps - 1) / kWarps;
+    float acc[kPer][2][4];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[i][0][k] = acc[i][1][k] = 0.f;
+    auto accumulate = [&](const float4(*st)[4], int m) {
+#pragma unroll
+      for (int i = 0; i < kPer; ++i) {
+        const int b = warp + i * kWarps;
+        if (b < kBlocks) {
+          const int sx0 = tx0 + (b % (TS / 8)) * 8, sy0 = ty0 + (b / (TS / 8)) * 8;
+          const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3);
+          forward_block<FADE>(st, m, sx0, sy0, lane, px, py0, (float)px, (float)py0, tail,
+                              acc[i][0], acc[i][1]);
+        }
+      }
+    };
+    if (L.count <= kStageMax) {
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      __syncthreads();
+      accumulate(stage, (int)L.count);
+    } else {  // a long list streams through once for the forward, again for the backward
+      float4(*buf)[kHalf][4] = reinterpret_cast<float4(*)[kHalf][4]>(stage);
+      const int64_t count = L.count;
+      const int nchunks = (int)((count + kHalf - 1) / kHalf);
+      auto len = [&](int64_t k0) { return (int)(count - k0 < kHalf ? count - k0 : kHalf); };
+      for (int c = 0; c < nchunks; ++c) {
+        const int64_t k0 = (int64_t)c * kHalf;
+        if (c + 1 < nchunks)
+          stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kHalf, len(k0 + kHalf),
+                          stage_gid + ((c + 1) & 1) * kHalf);
+        cp_async_commit();
+        cp_async_wait_one();
+        __syncthreads();
+        accumulate(buf[c & 1], len(k0));
+        __syncthreads();
+      }
+      stage_range<NT>(buf[0], rec, L, 0, len(0), stage_gid);  // chunk 0 for the backward
+      cp_async_commit();
+    }
+    const float per_value = pixel_loss_scale(H, W);
+    float loss_sum = 0.f, sq_sum = 0.f;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int b = warp + i * kWarps;
+      if (b < kBlocks) {
+        const int lx = (b % (TS / 8)) * 8 + (lane & 7), px = tx0 + lx;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int ly = (b / (TS / 8)) * 8 + (lane >> 3) + 4 * k, py = ty0 + ly;
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (px < W && py < H) {
+            const int64_t p = fr.pixel_base + (int64_t)py * W + px;
+            float lp, sq;
+            v = finish_pixel_rt(normalize, ff.loss_kind, acc[i][k], p, eps, per_value,
+                                ff.charb_eps2, ff.image, ff.den, ff.target, lp, sq);
+            loss_sum += lp;
+            sq_sum += sq;
+          }
+          pix[ly * TS + lx] = v;
+        }
+      }
+    }
+    if (ff.loss) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        loss_sum += __shfl_xor_sync(0xffffffffu, loss_sum, o);
+        sq_sum += __shfl_xor_sync(0xffffffffu, sq_sum, o);
+      }
+      if (lane == 0) {
+        atomicAdd(ff.loss + 2 * fr.image, loss_sum * per_value);
+        atomicAdd(ff.loss + 2 * fr.image + 1, sq_sum * per_value);
+      }
+    }
+    // the barrier before the first group (below) orders these pix writes before their reads
+  }
   if (L.count <= kStageMax) {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
@@ -755,7 +890,7 @@ void launch_backward_nt(unsigned T, cudaStream_t s, bool deterministic, const fl
 #define SS_BWD(FADE, DET)                                                                     \
   launch("backward_kernel", backward_kernel<TS, NT, FADE, DET, PIXGRAD>, T, NT, 0, s, grad_out, \
          rec, n, den, out, pixel_grad, gids, cap, offsets, f, normalize, eps, tail, ws, ws,    \
-         status)
+         status, FusedFit{})
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
@@ -780,6 +915,40 @@ void launch_backward(unsigned T, cudaStream_t s, bool deterministic, const float
     launch_backward_nt<TS, kLarge, PIXGRAD>(T, s, deterministic, grad_out, rec, n, den, out,
                                             pixel_grad, gids, cap, offsets, f, normalize, eps,
                                             tail, ws, status);
+}
+
+// The fused fit tile pass (forward + loss + backward in one CTA per tile).
+template <int TS, int NT>
+void launch_fused_nt(unsigned T, cudaStream_t s, bool deterministic, const Splat* rec, int64_t n,
+                     const int32_t* gids, int64_t cap, const int32_t* offsets, const Frames& f,
+                     int normalize, float eps, float tail, float* ws, uint32_t* status,
+                     const FusedFit& ff) {
+  const bool fade = tail > 0.0f;
+#define SS_FUS(FADE, DET)                                                                       \
+  launch("fit_tile_kernel", backward_kernel<TS, NT, FADE, DET, false, true>, T, NT, 0, s,      \
+         nullptr, rec, n, nullptr, nullptr, nullptr, gids, cap, offsets, f, normalize, eps,    \
+         tail, ws, ws, status, ff)
+  if (deterministic) {
+    if (fade) SS_FUS(true, true); else SS_FUS(false, true);
+  } else {
+    if (fade) SS_FUS(true, false); else SS_FUS(false, false);
+  }
+#undef SS_FUS
+}
+
+template <int TS>
+void launch_fused(unsigned T, cudaStream_t s, bool deterministic, const Splat* rec, int64_t n,
+                  const int32_t* gids, int64_t cap, const int32_t* offsets, const Frames& f,
+                  int normalize, float eps, float tail, float* ws, uint32_t* status,
+                  const FusedFit& ff) {
+  const int warps = g_backward_warps[TS == 16 ? 0 : 1].load(std::memory_order_relaxed);
+  constexpr int kSmall = TS == 16 ? 128 : 256, kLarge = TS == 16 ? 256 : 512;
+  if (warps * 32 == kSmall || (TS == 32 && warps == 0))
+    launch_fused_nt<TS, kSmall>(T, s, deterministic, rec, n, gids, cap, offsets, f, normalize,
+                                eps, tail, ws, status, ff);
+  else
+    launch_fused_nt<TS, kLarge>(T, s, deterministic, rec, n, gids, cap, offsets, f, normalize,
+                                eps, tail, ws, status, ff);
 }
 
 // Forward over any tile set; loss_kind selects the plain render or a fit forward.
@@ -1151,6 +1320,52 @@ int ss_fit_backward(const ss_batch* batch, const void* records, int64_t n,
                                nullptr, pixel_grad, tile_gids, gid_capacity, tile_offsets, 1,
                                1.0f, fade_tail, deterministic, static_cast<float*>(workspace),
                                status, as_stream(stream));
+}
+
+int ss_fit_forward_backward(const ss_batch* batch, const void* records, int64_t n,
+                            const int32_t* tile_gids, int64_t gid_capacity,
+                            const int32_t* tile_offsets, int normalize, float eps,
+                            float fade_tail, const float* target, int loss_kind,
+                            float charbonnier_eps, float* image, float* den, float* loss,
+                            int deterministic, void* workspace, size_t workspace_bytes,
+                            uint32_t* status, ss_stream_t stream) {
+  Frames f;
+  int rc = check_batch_render(batch, n, eps, &f);
+  if (rc) return rc;
+  if (loss_kind < 0 || loss_kind > 2)
+    return fail(SS_ERR_INVALID_ARGUMENT, "loss_kind must be 0 (l1), 1 (l2) or 2 (charbonnier)");
+  const size_t need = fit_ws_bytes(n, gid_capacity, deterministic);
+  if (workspace_bytes < need || !workspace)
+    return fail(SS_ERR_INVALID_ARGUMENT, "fit workspace too small (%zu < %zu)", workspace_bytes,
+                need);
+  cudaStream_t s = as_stream(stream);
+  if (batch->pixels == 0)  // nothing rendered; the update sums no entries
+    return deterministic && n > 0 ? clear_entry_segments(workspace, n, gid_capacity, s) : SS_OK;
+  if (!tile_offsets || !target) return fail(SS_ERR_INVALID_ARGUMENT, "null tile offsets or target");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  if (deterministic && gid_capacity > (int64_t)INT32_MAX)
+    return fail(SS_ERR_INVALID_ARGUMENT, "deterministic backward needs capacity < 2^31");
+  const int64_t T = batch->tiles;
+  if (T > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "too many tiles");
+  const int kinds[3] = {kL1, kL2, kCharbonnier};
+  FusedFit ff;
+  ff.target = target;
+  ff.image = image;
+  ff.den = den;
+  ff.loss = loss;
+  ff.loss_kind = kinds[loss_kind];
+  ff.charb_eps2 = (float)((double)charbonnier_eps * (double)charbonnier_eps);
+  const Splat* rec = static_cast<const Splat*>(records);
+  float* ws = static_cast<float*>(workspace);
+  if (batch->tile_size == 16)
+    launch_fused<16>((unsigned)T, s, deterministic, rec, n, tile_gids, gid_capacity,
+                     tile_offsets, f, normalize, eps, fade_tail, ws, status, ff);
+  else
+    launch_fused<32>((unsigned)T, s, deterministic, rec, n, tile_gids, gid_capacity,
+                     tile_offsets, f, normalize, eps, fade_tail, ws, status, ff);
+  if ((rc = check_launch("fit forward + backward"))) return rc;
+  if (!deterministic || n == 0) return SS_OK;
+  return order_entries(tile_gids, tile_offsets, T, gid_capacity, n, workspace, s);
 }
 
 }  // extern "C"
