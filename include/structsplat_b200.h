@@ -253,6 +253,24 @@ int ss_fit_forward_backward(const ss_batch* batch, const void* records, int64_t 
                             float charbonnier_eps, float* image, float* den, float* loss,
                             int deterministic, void* workspace, size_t workspace_bytes,
                             uint32_t* status, ss_stream_t stream);
+/* SSIM term of the fit loss (metrics.py:130-150, builtin backend: 11-tap Gaussian window,
+ * sigma 1.5, zero padding, C1 = 0.01^2, C2 = 0.03^2, mean over channels and pixels of each
+ * image), mixed as fit.py:3244 mixes it: loss = (1 - w) pixel_loss + w (1 - SSIM).
+ * ss_ssim_workspace_bytes: scratch of both calls (72 B per pixel).
+ * ss_ssim_target_stats: the target's window statistics (6P floats: mu_t per channel, then
+ * sig_t), constant over a fit (metrics.py:85-118, SSIMTargetStats); target (P,3).
+ * ss_fit_ssim: after ss_fit_forward_loss has written image (P,3), den (P) and the pixel loss's
+ * pixel_grad (P,4), scales pixel_grad by (1 - w) and adds -w dSSIM/dimage mapped to the
+ * backward's per-pixel input (normalized: (g, -(g . image)) / (den + eps); additive: (g, 0)).
+ * ssim (B), optional, receives each image's SSIM added atomically (zero it first).  With w = 1,
+ * normalize = 0 and a zero pixel_grad, pixel_grad[:, :3] is -dSSIM/dimage. */
+int ss_ssim_workspace_bytes(int64_t pixels, size_t* bytes);
+int ss_ssim_target_stats(const ss_batch* batch, const float* target, float* stats,
+                         void* workspace, size_t workspace_bytes, ss_stream_t stream);
+int ss_fit_ssim(const ss_batch* batch, const float* image, const float* den, const float* target,
+                const float* stats, int normalize, float eps, float ssim_weight,
+                float* pixel_grad, float* ssim, void* workspace, size_t workspace_bytes,
+                ss_stream_t stream);
 /* Gradients of the five parameter groups from the backward's workspace, then one Adam step
  * (torch.optim.Adam's multi-tensor step: lerp first moment, step factors formed in double, no
  * weight decay), then the clamp of log_scales to [log_scale_lo, log_scale_hi[image]] that the

@@ -117,6 +117,10 @@ class FitSettings:
     lr_opacity: float = 1e-2
     pixel_loss: str = "l2"
     charbonnier_eps: float = 1e-3
+    # weight w of the SSIM term, loss = (1 - w) pixel_loss + w (1 - SSIM) (fit.py:3244); the
+    # reference's FitConfig default is 0.3 with pixel_loss "l1" (config.py:200, 241), its plain
+    # method MSE alone (w = 0)
+    ssim_weight: float = 0.0
     normalize: bool = True
     eps: float = DEFAULT_EPS
     sigma_cutoff: float = 3.0
@@ -177,6 +181,18 @@ class FitPlan:
         self.bwd_ws = torch.zeros(max(self.bwd_ws_bytes // 4, 4), **f32)
         self.pixel_grad = torch.empty(max(batch.pixels, 1), 4, **f32)
         self.loss = torch.zeros(batch.images, 2, **f32)
+        if not 0.0 <= s.ssim_weight <= 1.0:
+            raise ValueError(f"ssim_weight must lie in [0, 1], got {s.ssim_weight}")
+        if s.ssim_weight > 0.0:  # the SSIM term needs the whole image before the backward
+            P = max(batch.pixels, 1)
+            self.image = torch.empty(P, 3, **f32)
+            self.den = torch.empty(P, **f32)
+            self.ssim = torch.zeros(batch.images, **f32)
+            self.ssim_stats = torch.empty(6 * P, **f32)
+            self.ssim_ws_bytes = _native.size_query("ss_ssim_workspace_bytes", batch.pixels)
+            self.ssim_ws = torch.empty(max(self.ssim_ws_bytes // 4, 1), **f32)
+            _native.call("ss_ssim_target_stats", batch.ref, _p(target), _p(self.ssim_stats),
+                         _p(self.ssim_ws), self.ssim_ws_bytes, _stream())
         self.exp_avg = {k: torch.zeros_like(v) for k, v in params.items() if v is not None}
         self.exp_avg_sq = {k: torch.zeros_like(v) for k, v in params.items() if v is not None}
         self.step_state = torch.zeros(2, device=d, dtype=torch.int32)
@@ -245,6 +261,14 @@ class FitPlan:
                      int(s.deterministic), _p(self.bwd_ws), self.bwd_ws_bytes, _p(self.status),
                      _stream())
 
+    def ssim_term(self):
+        """Mixes the SSIM term into pixel_grad after forward_loss wrote the image and den."""
+        s = self.s
+        _native.call("ss_fit_ssim", self.batch.ref, _p(self.image), _p(self.den),
+                     _p(self.target), _p(self.ssim_stats), int(s.normalize), float(s.eps),
+                     float(s.ssim_weight), _p(self.pixel_grad), _p(self.ssim), _p(self.ssim_ws),
+                     self.ssim_ws_bytes, _stream())
+
     def update(self):
         s = self.s
         _native.call("ss_fit_adam_update", self.batch.ref, _p(self.records), self.n,
@@ -260,7 +284,12 @@ class FitPlan:
         self.project()
         self.count()
         self.fill()
-        if self.s.fused:
+        if self.s.ssim_weight > 0.0:
+            self.ssim.zero_()
+            self.forward_loss(image=self.image, den=self.den)
+            self.ssim_term()
+            self.backward()
+        elif self.s.fused:
             self.forward_backward()
         else:
             self.forward_loss()

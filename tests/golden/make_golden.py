@@ -258,10 +258,37 @@ def codec_cases(ref, make_field, make_target):
         np.savez_compressed(HERE / f"codec_{name}.npz", **out)
 
 
+def ssim_cases(ref, make_target):
+    """The SSIM term of the fit loss (metrics.py:130-150) and its mix with the L1 pixel loss
+    (fit.py:3244): value and gradient w.r.t. the rendered image, from the reference's own
+    metrics.ssim and fit._pixel_loss under torch autograd."""
+    import torch
+    M = ref.metrics
+    for name, (H, W, seed, w) in {"ssim_small": (23, 31, 3, 0.3), "ssim_tiny": (7, 5, 4, 0.3),
+                                  "ssim_square": (40, 40, 5, 0.8)}.items():
+        target = torch.tensor(make_target(H, W, seed=seed))
+        rng = np.random.default_rng(seed + 100)
+        pred0 = np.clip(target.numpy() + rng.normal(0, 0.15, target.shape), 0, 1)
+        pred = torch.tensor(pred0.astype(np.float32), requires_grad=True)
+        s = M.ssim(pred, target)
+        (g_ssim,) = torch.autograd.grad(s, pred)
+        pred2 = torch.tensor(pred0.astype(np.float32), requires_grad=True)
+        stats = M.SSIMTargetStats(target)
+        s_cached = M.ssim(pred2, target, target_stats=stats)
+        pix = ref.fit._pixel_loss(pred2, target, "l1")
+        loss = (1 - w) * pix + w * (1 - s_cached)
+        (g_loss,) = torch.autograd.grad(loss, pred2)
+        np.savez(HERE / f"{name}.npz", pred=pred0.astype(np.float32), target=target.numpy(),
+                 weight=np.float32(w), ssim=np.float32(s.item()),
+                 ssim_cached=np.float32(s_cached.item()), grad_ssim=g_ssim.numpy(),
+                 loss=np.float32(loss.item()), grad_loss=g_loss.numpy())
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-src", default="/root/reference/src")
-    ap.add_argument("--only", choices=["placement", "passes", "fit", "codec"], default=None,
+    ap.add_argument("--only", choices=["placement", "passes", "fit", "codec", "ssim"],
+                    default=None,
                     help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
     sys.path.insert(0, args.reference_src)
@@ -274,6 +301,7 @@ def main() -> None:
     import structsplat.fit
     import structsplat.gaussians
     import structsplat.init
+    import structsplat.metrics
     import structsplat.render
     import structsplat.structure_tensor
 
@@ -287,10 +315,17 @@ def main() -> None:
         fit = structsplat.fit
         gaussians = structsplat.gaussians
         init = structsplat.init
+        metrics = structsplat.metrics
         render = structsplat.render
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "ssim":
+        for old in HERE.glob("ssim_*.npz"):
+            old.unlink()
+        ssim_cases(Ref, make_target)
+        print("wrote", len(list(HERE.glob("ssim_*.npz"))), "ssim fixtures")
+        return
     if args.only == "codec":
         for old in HERE.glob("codec_*.npz"):
             old.unlink()
@@ -400,6 +435,7 @@ def main() -> None:
     passes_cases(Ref)
     fit_case(Ref, make_field, make_target)
     codec_cases(Ref, make_field, make_target)
+    ssim_cases(Ref, make_target)
     print("wrote", len(list(HERE.glob("*.npz"))), "fixtures")
 
 
