@@ -451,18 +451,41 @@ def run_batched(args, dev, workload):
         if "img_s" in res["reference_loop"]:
             res["speedup_vs_reference_loop"] = round(
                 res["batched_img_s"] / res["reference_loop"]["img_s"], 2)
+    # the reference FitConfig's default loss: 0.7 L1 + 0.3 (1 - SSIM) (config.py:200, 241)
+    ws = FitSettings(pixel_loss="l1", ssim_weight=0.3)
+    fs = fresh()
+    plan = FitPlan(batch, Batch.concat_fields(fs), batch.concat_images(targets), ws)
+    step = GraphStep(plan)
+    for _ in range(Wm):
+        step.replay()
+    t_ssim = timed(step.replay, K)
+    (t_ssim,) = max_over_ranks([t_ssim], device=dev)
+    del step, plan
+    res["ssim_loss"] = {"loss": "0.7 l1 + 0.3 (1 - SSIM), 11-tap window",
+                        "batched_img_s": round(B_all * K / (t_ssim * 1e-3), 1),
+                        "batched_ms_per_step": round(t_ssim / K, 3)}
+    if not args.no_ref_cuda and world == 1:
+        ref = ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev,
+                                steps=args.ref_batch_steps, ssim_weight=0.3)
+        res["ssim_loss"]["reference_loop"] = ref
+        if "img_s" in ref:
+            res["ssim_loss"]["speedup_vs_reference_loop"] = round(
+                res["ssim_loss"]["batched_img_s"] / ref["img_s"], 2)
     return res
 
 
-def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2):
+def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2, ssim_weight=0.0):
     """The reference's plain fit iteration per image (its CUDA extension, tiled arm, through
-    render_cuda_exact; pixel MSE; torch.optim.Adam over its parameter groups; log-scale clamp),
-    looped over the images; img/s over `steps` timed passes after one warm-up pass."""
+    render_cuda_exact; pixel MSE — or, with ssim_weight, (1 - w) L1 + w (1 - SSIM) through its
+    metrics.ssim with cached target statistics; torch.optim.Adam over its parameter groups;
+    log-scale clamp), looped over the images; img/s over `steps` timed passes after one
+    warm-up pass."""
     try:
         sys.path.insert(0, str(REPO / "baseline"))
         from build_ref_cuda import load_reference_extension
         cuda_render = load_reference_extension()
         from structsplat.gaussians import GaussianField
+        from structsplat import metrics as ref_metrics
     except Exception as exc:
         return {"unavailable": str(exc)[:200]}
     names = ["means", "log_scales", "rotations", "colors", "opacity_logits"]
@@ -473,14 +496,19 @@ def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2):
         g = GaussianField(*vals)
         g.trainable()
         groups = g.parameter_groups(5e-2, 3e-2, 1e-2, 3e-2, 1e-2)
-        runs.append((g, torch.optim.Adam(groups), targets[b], sizes[b]))
+        stats = ref_metrics.SSIMTargetStats(targets[b]) if ssim_weight else None
+        runs.append((g, torch.optim.Adam(groups), targets[b], sizes[b], stats))
 
     def one_pass():
-        for g, opt, tgt, (H, W) in runs:
+        for g, opt, tgt, (H, W), stats in runs:
             img = cuda_render.render_cuda_exact(g.means, g.conics(), g.colors, g.radii(3.0), H, W,
                                                 opacities=g.opacity_values(), tiled=True)
             d = img - tgt
-            loss = (d * d).mean(dim=2).mean()
+            if ssim_weight:
+                sv = ref_metrics.ssim(img, tgt, target_stats=stats)
+                loss = (1 - ssim_weight) * d.abs().mean(dim=2).mean() + ssim_weight * (1 - sv)
+            else:
+                loss = (d * d).mean(dim=2).mean()
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()

@@ -278,6 +278,173 @@ __global__ void __launch_bounds__(kThreads)
   pixel_grad[p] = v;
 }
 
+// The same two windows per pass, one CTA per tile of the batch's tile grid (TS x TS pixels):
+// the tile's inputs with a kRadius halo are staged in shared memory (zeros outside the image,
+// the zero padding), the horizontal pass runs over all halo rows, the vertical pass over the
+// tile, channel by channel.  The taps are summed in the order of the per-pixel kernels above
+// (the same results to float rounding), with one global read of each input instead of eleven.
+constexpr int kTileThreads = 256;
+
+template <int TS>
+__global__ void __launch_bounds__(kTileThreads)
+    ssim_maps_tile_kernel(const float* __restrict__ img, const float* __restrict__ tgt,
+                          const float* __restrict__ stats, Frames frames, int64_t P, Window win,
+                          float* __restrict__ abc, float* __restrict__ ssim) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr int R = TS + 2 * kRadius;
+  __shared__ float sp[R * R], st[R * R];
+  __shared__ float hs[3][R][TS];
+  __shared__ float red[kTileThreads / 32];
+  const Frame fr = frame_of_tile(frames, blockIdx.x, 0);
+  const int local = blockIdx.x - fr.first_tile;
+  const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
+  const int H = fr.H, W = fr.W;
+  float ssum = 0.f;
+  for (int c = 0; c < 3; ++c) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
+      const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
+      const bool in = x >= 0 && x < W && y >= 0 && y < H;
+      const int64_t q = fr.pixel_base + (int64_t)y * W + x;
+      sp[i] = in ? img[3 * q + c] : 0.f;
+      st[i] = in ? tgt[3 * q + c] : 0.f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < R * TS; i += kTileThreads) {
+      const int r = i / TS, x = i % TS;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * kRadius; ++k) {
+        const float g = win.g[k], v = sp[r * R + x + k], t = st[r * R + x + k];
+        a0 = fmaf(g, v, a0);
+        a1 = fmaf(g, v * v, a1);
+        a2 = fmaf(g, v * t, a2);
+      }
+      hs[0][r][x] = a0;
+      hs[1][r][x] = a1;
+      hs[2][r][x] = a2;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < TS * TS; i += kTileThreads) {
+      const int y = i / TS, x = i % TS;
+      if (tx0 + x >= W || ty0 + y >= H) continue;
+      float mu_p = 0.f, e_pp = 0.f, e_pt = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * kRadius; ++k) {
+        const float g = win.g[k];
+        mu_p = fmaf(g, hs[0][y + k][x], mu_p);
+        e_pp = fmaf(g, hs[1][y + k][x], e_pp);
+        e_pt = fmaf(g, hs[2][y + k][x], e_pt);
+      }
+      const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
+      const float mu_t = stats[(int64_t)c * P + p], sig_t = stats[(int64_t)(3 + c) * P + p];
+      const float mu_p2 = mu_p * mu_p, mu_pt = mu_p * mu_t, mu_t2 = mu_t * mu_t;
+      const float A1 = 2.0f * mu_pt + kC1, A2 = 2.0f * (e_pt - mu_pt) + kC2;
+      const float B1 = mu_p2 + mu_t2 + kC1, B2 = (e_pp - mu_p2) + sig_t + kC2;
+      const float D = B1 * B2;
+      const float S = (A1 * A2) / D;
+      ssum += S;
+      abc[(int64_t)(3 * c) * P + p] = (2.0f * mu_t * (A2 - A1) - S * 2.0f * mu_p * (B2 - B1)) / D;
+      abc[(int64_t)(3 * c + 1) * P + p] = -S / B2;
+      abc[(int64_t)(3 * c + 2) * P + p] = 2.0f * A1 / D;
+    }
+  }
+  if (!ssim) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ssum += __shfl_xor_sync(0xffffffffu, ssum, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ssum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < kTileThreads / 32; ++w) t += red[w];
+    atomicAdd(ssim + fr.image, t / (float)(3 * (int64_t)H * W));
+  }
+}
+
+template <int TS>
+__global__ void __launch_bounds__(kTileThreads)
+    ssim_grad_tile_kernel(const float* __restrict__ abc, const float* __restrict__ img,
+                          const float* __restrict__ tgt, const float* __restrict__ den,
+                          Frames frames, int64_t P, Window win, int normalize, float eps,
+                          float weight, float4* __restrict__ pixel_grad) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr int R = TS + 2 * kRadius;
+  constexpr int kPer = (TS * TS + kTileThreads - 1) / kTileThreads;
+  __shared__ float sm[3][R * R];
+  __shared__ float hs[3][R][TS];
+  const Frame fr = frame_of_tile(frames, blockIdx.x, 0);
+  const int local = blockIdx.x - fr.first_tile;
+  const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
+  const int H = fr.H, W = fr.W;
+  const float inv_n = 1.0f / (float)(3 * (int64_t)H * W);
+  float g[kPer][3];
+  for (int c = 0; c < 3; ++c) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
+      const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
+      const bool in = x >= 0 && x < W && y >= 0 && y < H;
+      const int64_t q = fr.pixel_base + (int64_t)y * W + x;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) sm[m][i] = in ? abc[(int64_t)(3 * c + m) * P + q] : 0.f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < R * TS; i += kTileThreads) {
+      const int r = i / TS, x = i % TS;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        float a = 0.f;
+#pragma unroll
+        for (int k = 0; k <= 2 * kRadius; ++k) a = fmaf(win.g[k], sm[m][r * R + x + k], a);
+        hs[m][r][x] = a;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int i = threadIdx.x + j * kTileThreads;
+      const int y = i / TS, x = i % TS;
+      g[j][c] = 0.f;
+      if (i >= TS * TS || tx0 + x >= W || ty0 + y >= H) continue;
+      float acc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k <= 2 * kRadius; ++k)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) acc[m] = fmaf(win.g[k], hs[m][y + k][x], acc[m]);
+      const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
+      const float o = img[3 * p + c], t = tgt[3 * p + c];
+      g[j][c] = -weight * ((acc[0] + 2.0f * o * acc[1] + t * acc[2]) * inv_n);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) {
+    const int i = threadIdx.x + j * kTileThreads;
+    const int y = i / TS, x = i % TS;
+    if (i >= TS * TS || tx0 + x >= W || ty0 + y >= H) continue;
+    const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
+    float4 v = pixel_grad[p];
+    const float keep = 1.0f - weight;
+    v.x *= keep;
+    v.y *= keep;
+    v.z *= keep;
+    v.w *= keep;
+    if (normalize) {
+      const float d = den[p] + eps;
+      const float o0 = img[3 * p], o1 = img[3 * p + 1], o2 = img[3 * p + 2];
+      v.x += g[j][0] / d;
+      v.y += g[j][1] / d;
+      v.z += g[j][2] / d;
+      v.w += -(g[j][0] * o0 + g[j][1] * o1 + g[j][2] * o2) / d;
+    } else {
+      v.x += g[j][0];
+      v.y += g[j][1];
+      v.z += g[j][2];
+    }
+    pixel_grad[p] = v;
+  }
+}
+
 Geo geo_of(const ss_batch* b) {
   Geo g;
   g.table = b->image_table;
@@ -359,6 +526,25 @@ int ss_fit_ssim(const ss_batch* batch, const float* image, const float* den, con
   cudaStream_t s = as_stream(stream);
   float* h = static_cast<float*>(workspace);
   float* abc = h + 9 * P;
+  Frames f;
+  const int ts = batch->tile_size;
+  if ((ts == 16 || ts == 32) && batch->tiles > 0 && batch->tiles <= (int64_t)INT32_MAX &&
+      frames_of_batch(batch, 0, &f) == SS_OK) {  // the tile grid of a render batch
+    const unsigned T = (unsigned)batch->tiles;
+    float4* pg = reinterpret_cast<float4*>(pixel_grad);
+    if (ts == 32) {
+      launch("ssim maps", ssim_maps_tile_kernel<32>, T, kTileThreads, 0, s, image, target, stats,
+             f, P, win, abc, ssim);
+      launch("ssim gradient", ssim_grad_tile_kernel<32>, T, kTileThreads, 0, s, abc, image,
+             target, den, f, P, win, normalize, eps, ssim_weight, pg);
+    } else {
+      launch("ssim maps", ssim_maps_tile_kernel<16>, T, kTileThreads, 0, s, image, target, stats,
+             f, P, win, abc, ssim);
+      launch("ssim gradient", ssim_grad_tile_kernel<16>, T, kTileThreads, 0, s, abc, image,
+             target, den, f, P, win, normalize, eps, ssim_weight, pg);
+    }
+    return check_launch("fit ssim");
+  }
   const unsigned blocks = blocks_for(P);
   launch("ssim window", window_products_h_kernel<0>, blocks, kThreads, 0, s, image, target, geo,
          win, h);

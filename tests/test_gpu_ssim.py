@@ -128,3 +128,28 @@ def test_ssim_fit_follows_the_eager_iteration():
     for k, leaf in zip(PARAM_NAMES, leaves):
         diff = float((plan.params[k] - leaf.detach()).abs().max())
         assert diff <= 2e-3 * lr, (k, diff)
+
+
+def test_tile_passes_equal_the_per_pixel_passes():
+    """Tile sizes 16 and 32 stage each tile with its halo in shared memory; other tile sizes
+    run the per-pixel passes.  Same taps in the same order: the same gradient to float rounding
+    (the compiler may fuse a product into an FMA in one form and not the other)."""
+    require_cuda()
+    sizes = [(70, 45), (33, 64), (5, 7)]
+    rng = np.random.default_rng(3)
+    target = torch.tensor(np.concatenate([make_target(H, W, seed=b).reshape(-1, 3)
+                                          for b, (H, W) in enumerate(sizes)]), device="cuda")
+    image = (target + torch.tensor(rng.normal(0, 0.1, target.shape), dtype=torch.float32,
+                                   device="cuda")).clamp(0, 1).contiguous()
+    den = torch.tensor(rng.uniform(0.5, 2.0, target.shape[0]), dtype=torch.float32, device="cuda")
+    out = {}
+    for ts in (8, 16, 32):
+        batch = Batch(sizes, [0] * len(sizes), tile_size=ts)
+        pg0 = torch.tensor(rng.normal(0, 1e-3, (target.shape[0], 4)), dtype=torch.float32,
+                           device="cuda") if ts == 8 else out[8][2].clone()
+        pg, ssim = _ssim_grad(batch, image, target, weight=0.3, normalize=1, den=den,
+                              pixel_grad=pg0.clone())
+        out[ts] = (pg, ssim, pg0)
+    for ts in (16, 32):
+        assert rel_err(out[ts][0], out[8][0]) <= 1e-6, ts
+        assert float((out[ts][1] - out[8][1]).abs().max()) <= 1e-6
