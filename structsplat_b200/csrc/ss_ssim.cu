@@ -12,10 +12,12 @@
 // The gradient of SSIM = mean S at pixel q is (1/N) (G a + 2 p G b + t G c)(q) with the maps
 //   a = dS/dmu_p = (2 mu_t (A2 - A1) - S 2 mu_p (B2 - B1)) / (B1 B2),
 //   b = dS/dE_pp = -S / B2,   c = dS/dE_pt = 2 A1 / (B1 B2),
-// because the zero-padded symmetric window is its own adjoint.  Four passes over the batch:
-// horizontal then vertical window of (p, p^2, p t); the maps; horizontal then vertical window of
-// (a, b, c) and the gradient.  The last pass folds -w dSSIM/dp, with (1 - w) times the pixel
-// loss's part already in pixel_grad, through the normalisation into pixel_grad.
+// because the zero-padded symmetric window is its own adjoint.  Four passes over the batch
+// (per pixel), or, on the tile grid of a render batch (tile sizes 16 and 32), two passes of one
+// CTA per (tile, channel) and a per-pixel fold: horizontal then vertical window of
+// (p, p^2, p t) and the maps; horizontal then vertical window of (a, b, c) and the gradient.
+// The last step folds -w dSSIM/dp, with (1 - w) times the pixel loss's part already in
+// pixel_grad, through the normalisation into pixel_grad.
 #include <cmath>
 
 #include "ss_common.cuh"
@@ -284,6 +286,27 @@ __global__ void __launch_bounds__(kThreads)
 // tile, channel by channel.  The taps are summed in the order of the per-pixel kernels above
 // (the same results to float rounding), with one global read of each input instead of eleven.
 constexpr int kTileThreads = 256;
+constexpr int kRun = 4;  // consecutive outputs per thread in a window pass
+
+// Window of `M` arrays along a line: out[m][o] = sum_k g[k] in[m][(o + k) * stride] for the
+// kRun outputs o of one thread, the 10 + kRun inputs loaded once into registers.
+template <int M>
+__device__ __forceinline__ void window_run(const float* const (&in)[M], int stride,
+                                           const Window& win, float (&out)[M][kRun]) {
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    float v[2 * kRadius + kRun];
+#pragma unroll
+    for (int i = 0; i < 2 * kRadius + kRun; ++i) v[i] = in[m][i * stride];
+#pragma unroll
+    for (int o = 0; o < kRun; ++o) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k <= 2 * kRadius; ++k) a = fmaf(win.g[k], v[o + k], a);
+      out[m][o] = a;
+    }
+  }
+}
 
 template <int TS>
 __global__ void __launch_bounds__(kTileThreads)
@@ -293,61 +316,60 @@ __global__ void __launch_bounds__(kTileThreads)
   pdl_wait();
   pdl_trigger();
   constexpr int R = TS + 2 * kRadius;
-  __shared__ float sp[R * R], st[R * R];
-  __shared__ float hs[3][R][TS];
+  constexpr int kGroups = TS / kRun;  // runs per line
+  __shared__ float src[3][R * R];     // p, p^2, p t over the tile and its halo
+  __shared__ float hs[3][R * TS];     // horizontal window, every halo row
   __shared__ float red[kTileThreads / 32];
   const Frame fr = frame_of_tile(frames, blockIdx.x, 0);
   const int local = blockIdx.x - fr.first_tile;
   const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
   const int H = fr.H, W = fr.W;
+  const int c = blockIdx.y;  // one channel per CTA: a single load phase each
   float ssum = 0.f;
-  for (int c = 0; c < 3; ++c) {
-    __syncthreads();
+  {
     for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
       const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
       const bool in = x >= 0 && x < W && y >= 0 && y < H;
       const int64_t q = fr.pixel_base + (int64_t)y * W + x;
-      sp[i] = in ? img[3 * q + c] : 0.f;
-      st[i] = in ? tgt[3 * q + c] : 0.f;
+      const float v = in ? img[3 * q + c] : 0.f, t = in ? tgt[3 * q + c] : 0.f;
+      src[0][i] = v;
+      src[1][i] = v * v;
+      src[2][i] = v * t;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < R * TS; i += kTileThreads) {
-      const int r = i / TS, x = i % TS;
-      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int w = threadIdx.x; w < R * kGroups; w += kTileThreads) {
+      const int r = w / kGroups, x0 = (w % kGroups) * kRun;
+      const float* const in[3] = {&src[0][r * R + x0], &src[1][r * R + x0], &src[2][r * R + x0]};
+      float out[3][kRun];
+      window_run<3>(in, 1, win, out);
 #pragma unroll
-      for (int k = 0; k <= 2 * kRadius; ++k) {
-        const float g = win.g[k], v = sp[r * R + x + k], t = st[r * R + x + k];
-        a0 = fmaf(g, v, a0);
-        a1 = fmaf(g, v * v, a1);
-        a2 = fmaf(g, v * t, a2);
-      }
-      hs[0][r][x] = a0;
-      hs[1][r][x] = a1;
-      hs[2][r][x] = a2;
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int o = 0; o < kRun; ++o) hs[m][r * TS + x0 + o] = out[m][o];
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < TS * TS; i += kTileThreads) {
-      const int y = i / TS, x = i % TS;
-      if (tx0 + x >= W || ty0 + y >= H) continue;
-      float mu_p = 0.f, e_pp = 0.f, e_pt = 0.f;
+    for (int w = threadIdx.x; w < TS * kGroups; w += kTileThreads) {
+      const int x = w % TS, y0 = (w / TS) * kRun;
+      const float* const in[3] = {&hs[0][y0 * TS + x], &hs[1][y0 * TS + x], &hs[2][y0 * TS + x]};
+      float out[3][kRun];
+      window_run<3>(in, TS, win, out);
 #pragma unroll
-      for (int k = 0; k <= 2 * kRadius; ++k) {
-        const float g = win.g[k];
-        mu_p = fmaf(g, hs[0][y + k][x], mu_p);
-        e_pp = fmaf(g, hs[1][y + k][x], e_pp);
-        e_pt = fmaf(g, hs[2][y + k][x], e_pt);
+      for (int o = 0; o < kRun; ++o) {
+        const int y = y0 + o;
+        if (tx0 + x >= W || ty0 + y >= H) continue;
+        const float mu_p = out[0][o], e_pp = out[1][o], e_pt = out[2][o];
+        const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
+        const float mu_t = stats[(int64_t)c * P + p], sig_t = stats[(int64_t)(3 + c) * P + p];
+        const float mu_p2 = mu_p * mu_p, mu_pt = mu_p * mu_t, mu_t2 = mu_t * mu_t;
+        const float A1 = 2.0f * mu_pt + kC1, A2 = 2.0f * (e_pt - mu_pt) + kC2;
+        const float B1 = mu_p2 + mu_t2 + kC1, B2 = (e_pp - mu_p2) + sig_t + kC2;
+        const float D = B1 * B2;
+        const float S = (A1 * A2) / D;
+        ssum += S;
+        abc[(int64_t)(3 * c) * P + p] = (2.0f * mu_t * (A2 - A1) - S * 2.0f * mu_p * (B2 - B1)) / D;
+        abc[(int64_t)(3 * c + 1) * P + p] = -S / B2;
+        abc[(int64_t)(3 * c + 2) * P + p] = 2.0f * A1 / D;
       }
-      const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
-      const float mu_t = stats[(int64_t)c * P + p], sig_t = stats[(int64_t)(3 + c) * P + p];
-      const float mu_p2 = mu_p * mu_p, mu_pt = mu_p * mu_t, mu_t2 = mu_t * mu_t;
-      const float A1 = 2.0f * mu_pt + kC1, A2 = 2.0f * (e_pt - mu_pt) + kC2;
-      const float B1 = mu_p2 + mu_t2 + kC1, B2 = (e_pp - mu_p2) + sig_t + kC2;
-      const float D = B1 * B2;
-      const float S = (A1 * A2) / D;
-      ssum += S;
-      abc[(int64_t)(3 * c) * P + p] = (2.0f * mu_t * (A2 - A1) - S * 2.0f * mu_p * (B2 - B1)) / D;
-      abc[(int64_t)(3 * c + 1) * P + p] = -S / B2;
-      abc[(int64_t)(3 * c + 2) * P + p] = 2.0f * A1 / D;
     }
   }
   if (!ssim) return;
@@ -362,87 +384,88 @@ __global__ void __launch_bounds__(kTileThreads)
   }
 }
 
+// The adjoint window and the gradient of one channel per CTA (blockIdx.y): thread (x, y0) of
+// the tile owns the kRun pixels (x, y0 .. y0 + kRun - 1); their -w dSSIM/dp goes to
+// gbuf[c P + p] for ssim_fold_kernel.
 template <int TS>
 __global__ void __launch_bounds__(kTileThreads)
     ssim_grad_tile_kernel(const float* __restrict__ abc, const float* __restrict__ img,
-                          const float* __restrict__ tgt, const float* __restrict__ den,
-                          Frames frames, int64_t P, Window win, int normalize, float eps,
-                          float weight, float4* __restrict__ pixel_grad) {
+                          const float* __restrict__ tgt, Frames frames, int64_t P, Window win,
+                          float weight, float* __restrict__ gbuf) {
   pdl_wait();
   pdl_trigger();
   constexpr int R = TS + 2 * kRadius;
-  constexpr int kPer = (TS * TS + kTileThreads - 1) / kTileThreads;
+  constexpr int kGroups = TS / kRun;
   __shared__ float sm[3][R * R];
-  __shared__ float hs[3][R][TS];
+  __shared__ float hs[3][R * TS];
   const Frame fr = frame_of_tile(frames, blockIdx.x, 0);
   const int local = blockIdx.x - fr.first_tile;
   const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
   const int H = fr.H, W = fr.W;
+  const int c = blockIdx.y;
   const float inv_n = 1.0f / (float)(3 * (int64_t)H * W);
-  float g[kPer][3];
-  for (int c = 0; c < 3; ++c) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
-      const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
-      const bool in = x >= 0 && x < W && y >= 0 && y < H;
-      const int64_t q = fr.pixel_base + (int64_t)y * W + x;
+  for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
+    const int xx = tx0 - kRadius + i % R, yy = ty0 - kRadius + i / R;
+    const bool in = xx >= 0 && xx < W && yy >= 0 && yy < H;
+    const int64_t q = fr.pixel_base + (int64_t)yy * W + xx;
 #pragma unroll
-      for (int m = 0; m < 3; ++m) sm[m][i] = in ? abc[(int64_t)(3 * c + m) * P + q] : 0.f;
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < R * TS; i += kTileThreads) {
-      const int r = i / TS, x = i % TS;
-#pragma unroll
-      for (int m = 0; m < 3; ++m) {
-        float a = 0.f;
-#pragma unroll
-        for (int k = 0; k <= 2 * kRadius; ++k) a = fmaf(win.g[k], sm[m][r * R + x + k], a);
-        hs[m][r][x] = a;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      const int i = threadIdx.x + j * kTileThreads;
-      const int y = i / TS, x = i % TS;
-      g[j][c] = 0.f;
-      if (i >= TS * TS || tx0 + x >= W || ty0 + y >= H) continue;
-      float acc[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-      for (int k = 0; k <= 2 * kRadius; ++k)
-#pragma unroll
-        for (int m = 0; m < 3; ++m) acc[m] = fmaf(win.g[k], hs[m][y + k][x], acc[m]);
-      const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
-      const float o = img[3 * p + c], t = tgt[3 * p + c];
-      g[j][c] = -weight * ((acc[0] + 2.0f * o * acc[1] + t * acc[2]) * inv_n);
-    }
+    for (int m = 0; m < 3; ++m) sm[m][i] = in ? abc[(int64_t)(3 * c + m) * P + q] : 0.f;
   }
+  __syncthreads();
+  for (int w = threadIdx.x; w < R * kGroups; w += kTileThreads) {
+    const int r = w / kGroups, x0 = (w % kGroups) * kRun;
+    const float* const in[3] = {&sm[0][r * R + x0], &sm[1][r * R + x0], &sm[2][r * R + x0]};
+    float out[3][kRun];
+    window_run<3>(in, 1, win, out);
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int i = threadIdx.x + j * kTileThreads;
-    const int y = i / TS, x = i % TS;
-    if (i >= TS * TS || tx0 + x >= W || ty0 + y >= H) continue;
-    const int64_t p = fr.pixel_base + (int64_t)(ty0 + y) * W + tx0 + x;
-    float4 v = pixel_grad[p];
-    const float keep = 1.0f - weight;
-    v.x *= keep;
-    v.y *= keep;
-    v.z *= keep;
-    v.w *= keep;
-    if (normalize) {
-      const float d = den[p] + eps;
-      const float o0 = img[3 * p], o1 = img[3 * p + 1], o2 = img[3 * p + 2];
-      v.x += g[j][0] / d;
-      v.y += g[j][1] / d;
-      v.z += g[j][2] / d;
-      v.w += -(g[j][0] * o0 + g[j][1] * o1 + g[j][2] * o2) / d;
-    } else {
-      v.x += g[j][0];
-      v.y += g[j][1];
-      v.z += g[j][2];
-    }
-    pixel_grad[p] = v;
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int k = 0; k < kRun; ++k) hs[m][r * TS + x0 + k] = out[m][k];
   }
+  __syncthreads();
+  if (threadIdx.x >= TS * kGroups) return;
+  const int x = threadIdx.x % TS, y0 = (threadIdx.x / TS) * kRun;
+  const float* const in[3] = {&hs[0][y0 * TS + x], &hs[1][y0 * TS + x], &hs[2][y0 * TS + x]};
+  float out[3][kRun];
+  window_run<3>(in, TS, win, out);
+#pragma unroll
+  for (int j = 0; j < kRun; ++j) {
+    if (tx0 + x >= W || ty0 + y0 + j >= H) continue;
+    const int64_t p = fr.pixel_base + (int64_t)(ty0 + y0 + j) * W + tx0 + x;
+    const float o = img[3 * p + c], t = tgt[3 * p + c];
+    gbuf[(int64_t)c * P + p] = -weight * ((out[0][j] + 2.0f * o * out[1][j] + t * out[2][j]) *
+                                          inv_n);
+  }
+}
+
+// pixel_grad <- (1 - w) pixel_grad + V(g) with g = gbuf's three channels (see ssim_grad_kernel).
+__global__ void __launch_bounds__(kThreads)
+    ssim_fold_kernel(const float* __restrict__ gbuf, const float* __restrict__ img,
+                     const float* __restrict__ den, int64_t P, int normalize, float eps,
+                     float weight, float4* __restrict__ pixel_grad) {
+  pdl_wait();
+  pdl_trigger();
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const float g0 = gbuf[p], g1 = gbuf[P + p], g2 = gbuf[2 * P + p];
+  float4 v = pixel_grad[p];
+  const float keep = 1.0f - weight;
+  v.x *= keep;
+  v.y *= keep;
+  v.z *= keep;
+  v.w *= keep;
+  if (normalize) {
+    const float d = den[p] + eps;
+    v.x += g0 / d;
+    v.y += g1 / d;
+    v.z += g2 / d;
+    v.w += -(g0 * img[3 * p] + g1 * img[3 * p + 1] + g2 * img[3 * p + 2]) / d;
+  } else {
+    v.x += g0;
+    v.y += g1;
+    v.z += g2;
+  }
+  pixel_grad[p] = v;
 }
 
 Geo geo_of(const ss_batch* b) {
@@ -530,19 +553,22 @@ int ss_fit_ssim(const ss_batch* batch, const float* image, const float* den, con
   const int ts = batch->tile_size;
   if ((ts == 16 || ts == 32) && batch->tiles > 0 && batch->tiles <= (int64_t)INT32_MAX &&
       frames_of_batch(batch, 0, &f) == SS_OK) {  // the tile grid of a render batch
-    const unsigned T = (unsigned)batch->tiles;
+    const dim3 grid((unsigned)batch->tiles, 3);  // (tile, channel)
     float4* pg = reinterpret_cast<float4*>(pixel_grad);
+    float* gbuf = h;  // 3P: each channel's -w dSSIM/dp
     if (ts == 32) {
-      launch("ssim maps", ssim_maps_tile_kernel<32>, T, kTileThreads, 0, s, image, target, stats,
-             f, P, win, abc, ssim);
-      launch("ssim gradient", ssim_grad_tile_kernel<32>, T, kTileThreads, 0, s, abc, image,
-             target, den, f, P, win, normalize, eps, ssim_weight, pg);
+      launch("ssim maps", ssim_maps_tile_kernel<32>, grid, kTileThreads, 0, s, image, target,
+             stats, f, P, win, abc, ssim);
+      launch("ssim gradient", ssim_grad_tile_kernel<32>, grid, kTileThreads, 0, s, abc, image,
+             target, f, P, win, ssim_weight, gbuf);
     } else {
-      launch("ssim maps", ssim_maps_tile_kernel<16>, T, kTileThreads, 0, s, image, target, stats,
-             f, P, win, abc, ssim);
-      launch("ssim gradient", ssim_grad_tile_kernel<16>, T, kTileThreads, 0, s, abc, image,
-             target, den, f, P, win, normalize, eps, ssim_weight, pg);
+      launch("ssim maps", ssim_maps_tile_kernel<16>, grid, kTileThreads, 0, s, image, target,
+             stats, f, P, win, abc, ssim);
+      launch("ssim gradient", ssim_grad_tile_kernel<16>, grid, kTileThreads, 0, s, abc, image,
+             target, f, P, win, ssim_weight, gbuf);
     }
+    launch("ssim fold", ssim_fold_kernel, blocks_for(P), kThreads, 0, s, gbuf, image, den, P,
+           normalize, eps, ssim_weight, pg);
     return check_launch("fit ssim");
   }
   const unsigned blocks = blocks_for(P);
