@@ -9,6 +9,7 @@
 // single-CTA kernel for up to 16,384 tiles and CUB's device scan beyond.
 #include <climits>
 
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -397,20 +398,43 @@ __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __re
 }
 
 // Long lists: one CTA per list, in shared memory up to kBigSortSmem ids, else in place.
+// Lists of up to kRadixSortMax ids sort with CUB's block radix sort over the bits the ids need
+// (key_bits: pad keys 2^bits - 1 sort last); longer ones with the shared-memory bitonic network
+// (the ids of a list are distinct, so both give the one ascending order).
+constexpr int kRadixItems = 4;
+constexpr int kRadixSortMax = 1024 * kRadixItems;
+using BigRadixSort = cub::BlockRadixSort<unsigned, 1024, kRadixItems>;
+
 __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __restrict__ offsets,
                                                              int32_t* __restrict__ gids,
                                                              const int* __restrict__ big_tiles,
-                                                             const int* __restrict__ big_count) {
+                                                             const int* __restrict__ big_count,
+                                                             int key_bits) {
   pdl_wait();
   pdl_trigger();
   extern __shared__ int sbuf[];
+  __shared__ typename BigRadixSort::TempStorage radix_temp;
   int count = *big_count;
+  const unsigned pad = key_bits >= 32 ? 0xffffffffu : (1u << key_bits) - 1u;
   for (int k = blockIdx.x; k < count; k += gridDim.x) {
     int t = big_tiles[k];
     int64_t lo = offsets[t];
     int len = (int)(offsets[t + 1] - lo);
     auto sync = [] { __syncthreads(); };
-    if (len <= kBigSortSmem) {
+    if (len <= kRadixSortMax) {
+      unsigned keys[kRadixItems];
+#pragma unroll
+      for (int i = 0; i < kRadixItems; ++i) {
+        const int e = threadIdx.x * kRadixItems + i;
+        keys[i] = e < len ? (unsigned)gids[lo + e] : pad;
+      }
+      BigRadixSort(radix_temp).Sort(keys, 0, key_bits);
+#pragma unroll
+      for (int i = 0; i < kRadixItems; ++i) {
+        const int e = threadIdx.x * kRadixItems + i;
+        if (e < len) gids[lo + e] = (int32_t)keys[i];
+      }
+    } else if (len <= kBigSortSmem) {
       for (int e = threadIdx.x; e < len; e += blockDim.x) sbuf[e] = gids[lo + e];
       __syncthreads();
       bitonic_sort(sbuf, len, threadIdx.x, blockDim.x, sync);
@@ -420,6 +444,13 @@ __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __re
     }
     __syncthreads();
   }
+}
+
+// Bits that hold every id below n and the pad 2^bits - 1 above them.
+int sort_key_bits(int64_t n) {
+  int b = 1;
+  while (b < 32 && ((int64_t)1 << b) <= n) ++b;
+  return b;
 }
 
 constexpr int kBigSortCtas = 296;  // 2 per SM: long lists are common under heavy-tailed fields
@@ -530,8 +561,9 @@ int index_fill(const Frames& frames, int ts, int64_t T, const void* records, int
                                                      w.big_tiles, w.big_count);
   if ((rc = check_launch("tile_sort"))) return rc;
   if ((rc = allow_big_sort_smem())) return rc;
-  launch("tile_sort_big_kernel", tile_sort_big_kernel, kBigSortCtas, 1024, kBigSortSmem * sizeof(int), s, 
-      tile_offsets, tile_gids, w.big_tiles, w.big_count);
+  launch("tile_sort_big_kernel", tile_sort_big_kernel, kBigSortCtas, 1024,
+         kBigSortSmem * sizeof(int), s, tile_offsets, tile_gids, w.big_tiles, w.big_count,
+         sort_key_bits(n));
   return check_launch("tile_sort_big");
 }
 
