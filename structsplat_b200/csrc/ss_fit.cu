@@ -49,11 +49,55 @@ __device__ __forceinline__ float adam(float p, float g, float& m, float& v, floa
   return fmaf(-step, m / denom, p);
 }
 
+// Inputs of one Gaussian's gradients: its nine summed moments, the record's opacity and conic,
+// and the current log-scales, rotation and opacity logit.
+struct GradIn {
+  float m[kMoments];
+  float op, a, b, c, ls0, ls1, th, lg;
+};
+
+__device__ __forceinline__ void load_grad_in(const Splat* __restrict__ rec,
+                                             const float* __restrict__ log_scales,
+                                             const float* __restrict__ rotations,
+                                             const float* __restrict__ logits, int64_t g,
+                                             GradIn& in) {
+  const float4 p1 = reinterpret_cast<const float4*>(rec + g)[1];
+  const float4 p2 = reinterpret_cast<const float4*>(rec + g)[2];
+  in.op = p1.y;
+  in.a = p2.y;
+  in.b = p2.z;
+  in.c = p2.w;
+  in.ls0 = log_scales[2 * g];
+  in.ls1 = log_scales[2 * g + 1];
+  in.th = rotations[g];
+  in.lg = logits ? logits[g] : 0.f;
+}
+
+// The same arithmetic as the plain backward epilogue, then the RS chain rule.
+__device__ __forceinline__ void store_grads(const GradIn& in, int64_t g, float dilation,
+                                            bool has_logits, const FieldPtrs& grad) {
+  const float* m = in.m;
+  float gls0, gls1, grot;
+  rs_conic_chain(in.ls0, in.ls1, in.th, dilation, -0.5f * in.op * m[6], -in.op * m[7],
+                 -0.5f * in.op * m[8], gls0, gls1, grot);
+  grad.means[2 * g] = in.op * (in.a * m[4] + in.b * m[5]);
+  grad.means[2 * g + 1] = in.op * (in.b * m[4] + in.c * m[5]);
+  grad.log_scales[2 * g] = gls0;
+  grad.log_scales[2 * g + 1] = gls1;
+  grad.rotations[g] = grot;
+  grad.colors[3 * g] = in.op * m[0];
+  grad.colors[3 * g + 1] = in.op * m[1];
+  grad.colors[3 * g + 2] = in.op * m[2];
+  if (has_logits) grad.logits[g] = logit_chain(in.lg, m[3]);
+}
+
 // Per-Gaussian gradients of the five parameter groups: the summed moments (fast: the atomic
 // accumulators, read and zeroed; deterministic: the entry partials in their fixed order) become
 // render-input gradients, and the chain rule carries them to the RS parameters at their current
 // values.  Grid-stride, a warp's 32 consecutive Gaussians per round (the deterministic sum is
-// warp-collective).  The gradients go to tensors shaped like the parameters.
+// warp-collective); fast mode takes two rounds at a time with every load issued before the first
+// store, so each thread keeps two Gaussians' loads in flight.  The gradients go to tensors shaped
+// like the parameters.
 template <bool DETERMINISTIC>
 __global__ void __launch_bounds__(kThreads)
     fit_grad_kernel(const Splat* __restrict__ rec, int64_t n, float* __restrict__ moments,
@@ -65,40 +109,36 @@ __global__ void __launch_bounds__(kThreads)
   pdl_trigger();
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < n;
-       base += stride) {
-    const int64_t g = base + lane;
-    const bool active = g < n;
-    float m[kMoments];
-    if (DETERMINISTIC) sum_entry_partials(partials, order, seg, n, g, active, m);
-    if (!active) continue;
-    if (!DETERMINISTIC) {
-#pragma unroll
-      for (int k = 0; k < kMoments; ++k) m[k] = moments[k * n + g];
+  const int64_t first = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane);
+  if (DETERMINISTIC) {
+    for (int64_t base = first; base < n; base += stride) {
+      const int64_t g = base + lane;
+      const bool active = g < n;
+      GradIn in;
+      sum_entry_partials(partials, order, seg, n, g, active, in.m);
+      if (!active) continue;
+      load_grad_in(rec, log_scales, rotations, logits, g, in);
+      store_grads(in, g, dilation, logits != nullptr, grad);
     }
-    const float4 p1 = reinterpret_cast<const float4*>(rec + g)[1];
-    const float4 p2 = reinterpret_cast<const float4*>(rec + g)[2];
-    const float ls0 = log_scales[2 * g], ls1 = log_scales[2 * g + 1];
-    const float th = rotations[g];
-    const float lg = logits ? logits[g] : 0.f;
-    if (!DETERMINISTIC) {
+    return;
+  }
+  for (int64_t base = first; base < n; base += 2 * stride) {
+    const int64_t g[2] = {base + lane, base + stride + lane};
+    GradIn in[2];
 #pragma unroll
-      for (int k = 0; k < kMoments; ++k) moments[k * n + g] = 0.0f;
+    for (int u = 0; u < 2; ++u) {
+      if (g[u] >= n) continue;
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) in[u].m[k] = moments[k * n + g[u]];
+      load_grad_in(rec, log_scales, rotations, logits, g[u], in[u]);
     }
-    const float op = p1.y, a = p2.y, b = p2.z, c = p2.w;
-    // the same arithmetic as the plain backward epilogue, then the RS chain rule
-    float gls0, gls1, grot;
-    rs_conic_chain(ls0, ls1, th, dilation, -0.5f * op * m[6], -op * m[7], -0.5f * op * m[8],
-                   gls0, gls1, grot);
-    grad.means[2 * g] = op * (a * m[4] + b * m[5]);
-    grad.means[2 * g + 1] = op * (b * m[4] + c * m[5]);
-    grad.log_scales[2 * g] = gls0;
-    grad.log_scales[2 * g + 1] = gls1;
-    grad.rotations[g] = grot;
-    grad.colors[3 * g] = op * m[0];
-    grad.colors[3 * g + 1] = op * m[1];
-    grad.colors[3 * g + 2] = op * m[2];
-    if (logits) grad.logits[g] = logit_chain(lg, m[3]);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (g[u] >= n) continue;
+#pragma unroll
+      for (int k = 0; k < kMoments; ++k) moments[k * n + g[u]] = 0.0f;
+      store_grads(in[u], g[u], dilation, logits != nullptr, grad);
+    }
   }
 }
 

@@ -151,3 +151,12 @@ def test_backward_warps_knob_validation(lib):
     assert lib.ss_set_backward_warps(32, 16) == 0 and lib.ss_get_backward_warps(32) == 16
     assert lib.ss_set_backward_warps(32, 0) == 0 and lib.ss_get_backward_warps(32) == 8
     assert lib.ss_get_backward_warps(7) == -1
+
+
+def test_dependent_launch_switch(lib):
+    """Programmatic dependent launch is on by default; the switch takes 0 or 1 only."""
+    assert lib.ss_get_dependent_launch() == 1
+    rc, msg = _status(lib, "ss_set_dependent_launch", 2)
+    assert rc == 1 and "0 or 1" in msg
+    assert lib.ss_set_dependent_launch(0) == 0 and lib.ss_get_dependent_launch() == 0
+    assert lib.ss_set_dependent_launch(1) == 0 and lib.ss_get_dependent_launch() == 1

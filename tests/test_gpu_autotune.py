@@ -67,3 +67,25 @@ def test_tuned_batched_fit_reaches_the_same_psnr(tmp_path, monkeypatch):
         assert abs(pa - pb) <= 0.01
     for ts in (16, 32):
         _native.call("ss_set_backward_warps", ts, 0)
+
+
+def test_dependent_launch_does_not_change_results():
+    """The step's kernels give bitwise the same image and deterministic gradients whether or not
+    they may start while their predecessor drains."""
+    require_cuda()
+    H, W = 160, 144
+    params = _field(H, W, 3000, seed=4)
+    go = torch.randn(H, W, 3, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    runs = []
+    for enable in (1, 0):
+        _native.call("ss_set_dependent_launch", enable)
+        try:
+            plan = RenderPlan.for_field(params, H, W, deterministic=True)
+            grads = {k: v.clone() for k, v in plan.forward_backward(params, go).items()}
+            torch.cuda.synchronize()
+            runs.append((plan.image.clone(), grads))
+        finally:
+            _native.call("ss_set_dependent_launch", 1)
+    assert torch.equal(runs[0][0], runs[1][0])
+    for k in runs[0][1]:
+        assert torch.equal(runs[0][1][k], runs[1][1][k]), k
