@@ -23,8 +23,8 @@ from structsplat_b200.synthetic import make_field, make_target
 
 pytestmark = pytest.mark.gpu
 
-SIZES = [(64, 96), (37, 50), (128, 128), (40, 33)]
-COUNTS = [500, 120, 1500, 60]
+SIZES = [(64, 96), (37, 50), (1, 1), (128, 128), (40, 33), (20, 17)]
+COUNTS = [500, 120, 3, 1500, 60, 0]  # a one-pixel image and an image without Gaussians
 
 
 def _fields(sizes, counts, seed, log_sigma_std=0.5):

@@ -98,7 +98,8 @@ def test_mixed_loss_pixel_grad_matches_autograd(normalize):
     assert abs(float(plan.ssim[0]) - s_val) <= 2e-5
 
 
-def test_ssim_fit_follows_the_eager_iteration():
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_ssim_fit_follows_the_eager_iteration(deterministic):
     """Three steps of the plan against render -> oracle mixed loss -> autograd -> Adam -> clamp
     in torch, from the same field."""
     require_cuda()
@@ -107,7 +108,7 @@ def test_ssim_fit_follows_the_eager_iteration():
     target = torch.tensor(make_target(H, W, seed=21), device="cuda")
     f = make_field(H, W, 250, seed=22)
     w, lr = 0.3, 1e-2
-    s = FitSettings.uniform_lr(lr, pixel_loss="l1", ssim_weight=w)
+    s = FitSettings.uniform_lr(lr, pixel_loss="l1", ssim_weight=w, deterministic=deterministic)
     field = {k: torch.tensor(getattr(f, k), device="cuda") for k in PARAM_NAMES}
     batch = Batch([(H, W)], [250])
     plan = FitPlan(batch, Batch.concat_fields([field]), batch.concat_images([target]), s)
