@@ -557,6 +557,39 @@ def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2, ssim_weig
             "ms_per_pass": round(ms / steps, 2), "arm": "cuda_tiled"}
 
 
+def run_ssim_profile(dev, H=2048, W=2048, calls=13):
+    """The SSIM term alone (ss_fit_ssim, w = 0.3, normalized) on one image: ms per call."""
+    from structsplat_b200 import _native
+    from structsplat_b200.batch import Batch
+    from structsplat_b200.render import _p, _stream
+    from structsplat_b200.synthetic import make_target
+    t = torch.tensor(make_target(H, W, seed=1), device=dev).reshape(-1, 3).contiguous()
+    gen = torch.Generator(device=dev).manual_seed(2)
+    img = (t + 0.05 * torch.randn(t.shape, device=dev, generator=gen)).clamp(0, 1).contiguous()
+    den = torch.rand(H * W, device=dev, generator=gen) + 0.5
+    batch = Batch([(H, W)], [0], device=dev)
+    wsb = _native.size_query("ss_ssim_workspace_bytes", H * W)
+    ws = torch.empty(wsb // 4, device=dev)
+    stats = torch.empty(6 * H * W, device=dev)
+    _native.call("ss_ssim_target_stats", batch.ref, _p(t), _p(stats), _p(ws), wsb, _stream())
+    pg = torch.zeros(H * W, 4, device=dev)
+    ssim = torch.zeros(1, device=dev)
+
+    def call():
+        _native.call("ss_fit_ssim", batch.ref, _p(img), _p(den), _p(t), _p(stats), 1, 1e-8, 0.3,
+                     _p(pg), _p(ssim), _p(ws), wsb, _stream())
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(calls - 3):
+        call()
+    e.record()
+    torch.cuda.synchronize()
+    return {"image": f"{W}x{H}", "ms_per_call": round(s.elapsed_time(e) / (calls - 3), 4)}
+
+
 def run_stress(args, dev):
     """C3: 2048² target, 1M heavy-tailed Gaussians (30% elongated along the structure tensor),
     the whole deterministic Adam fit iteration captured in one CUDA graph."""
@@ -682,6 +715,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2000)
     ap.add_argument("--e2e-check", type=int, default=25)
     ap.add_argument("--psnr-thresholds", default="30,33,35,36,37,38,39")
+    ap.add_argument("--ssim-profile", action="store_true",
+                    help="only time the SSIM term on one 2048x2048 image (for ncu)")
     ap.add_argument("--dependent-launch", type=int, default=1, choices=[0, 1],
                     help="programmatic dependent launch of the library's kernels (1: on)")
     ap.add_argument("--profile", action="store_true",
@@ -724,6 +759,11 @@ def main():
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(
             seconds=120))
+    if args.ssim_profile:
+        dev = torch.device(f"cuda:{local}")
+        torch.cuda.set_device(dev)
+        print(json.dumps({"ssim_profile": run_ssim_profile(dev)}))
+        return
     if args.stress or args.e2e_fit:
         dev = torch.device(f"cuda:{local}")
         torch.cuda.set_device(dev)
