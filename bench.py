@@ -396,7 +396,7 @@ def run_batched(args, dev, workload):
     def fresh():
         return [{k: torch.tensor(getattr(f, k), device=dev) for k in names} for f in fields_np]
 
-    settings = FitSettings()
+    settings = FitSettings(fused=_fused_flag(args))
     K, Wm = args.batch_steps, args.warmup
 
     def timed(fn, iters):
@@ -461,6 +461,7 @@ def run_batched(args, dev, workload):
                     f"2048x1536}} (WxH), 0.1 Gaussians/px, seeded generator targets; "
                     f"normalized, pixel MSE, Adam (reference per-group lrs)",
         "images": B_all, "pixels": int(px_all), "gaussians": int(g_all),
+        "fused_tile_pass": settings.use_fused(),
         "tile_entries": int(e_all), "steps": K, "warmup": Wm,
         "scaling": "strong (the images are split across ranks)",
         "batched_img_s": round(B_all * K / (t_batch * 1e-3), 1),
@@ -557,6 +558,10 @@ def ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev, steps=2, ssim_weig
             "ms_per_pass": round(ms / steps, 2), "arm": "cuda_tiled"}
 
 
+def _fused_flag(args):
+    return None if args.fused < 0 else bool(args.fused)
+
+
 def run_ssim_profile(dev, H=2048, W=2048, calls=13):
     """The SSIM term alone (ss_fit_ssim, w = 0.3, normalized) on one image: ms per call."""
     from structsplat_b200 import _native
@@ -605,7 +610,7 @@ def run_stress(args, dev):
     along = (tensor.across_edge_angle + math.pi / 2.0).cpu().numpy()
     f = make_stress_field(H, W, N, seed=32, along_edge_angle=along)
     params = {k: torch.tensor(getattr(f, k), device=dev) for k in names}
-    settings = FitSettings(deterministic=True)
+    settings = FitSettings(deterministic=True, fused=_fused_flag(args))
     batch = Batch([(H, W)], [N], device=dev)
     plan = FitPlan(batch, params, target.reshape(-1, 3).contiguous(), settings)
     counts = (plan.offsets[1:] - plan.offsets[:-1]).to(torch.int64)
@@ -632,6 +637,7 @@ def run_stress(args, dev):
                         "(aspect U[5,50]) along structure-tensor orientation (sigma 1, rho 3); "
                         "deterministic two-pass backward; Adam fit iteration in one CUDA graph",
             "ms_per_step": round(ms, 3), "steps": K, "warmup": args.warmup,
+            "fused_tile_pass": settings.use_fused(),
             "pairs": pairs, "gpairs_per_s": round(pairs / (ms * 1e-3) / 1e9, 2),
             "step_roofline_frac": round(pairs * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (
                 SM_COUNT * FP32_LANES * (measured_peaks().get("sm_max_mhz") or 1965.0) * 1e6)
@@ -667,7 +673,8 @@ def run_e2e_fit(args, dev):
         t_place.record()
         field["opacity_logits"] = None
         batch = Batch([(H, W)], [N], device=dev)
-        plan = FitPlan(batch, field, target.reshape(-1, 3).contiguous(), FitSettings())
+        plan = FitPlan(batch, field, target.reshape(-1, 3).contiguous(),
+                       FitSettings(fused=_fused_flag(args)))
         runner = GraphStep(plan).replay if form == "graph" else plan.step
         torch.cuda.synchronize()
         placement_ms = t0.elapsed_time(t_place)
@@ -717,6 +724,9 @@ def main():
     ap.add_argument("--psnr-thresholds", default="30,33,35,36,37,38,39")
     ap.add_argument("--ssim-profile", action="store_true",
                     help="only time the SSIM term on one 2048x2048 image (for ncu)")
+    ap.add_argument("--fused", type=int, default=-1, choices=[-1, 0, 1],
+                    help="fit legs: forward, loss and backward in one tile pass (1), two (0), "
+                         "or the plan's choice (-1: fused in fast mode)")
     ap.add_argument("--dependent-launch", type=int, default=1, choices=[0, 1],
                     help="programmatic dependent launch of the library's kernels (1: on)")
     ap.add_argument("--profile", action="store_true",

@@ -167,7 +167,7 @@ def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
         plan = plans[ts]
 
         def run():
-            if plan.s.fused:
+            if plan.s.use_fused():
                 plan.forward_backward()
             else:
                 plan.forward_loss()
@@ -180,7 +180,7 @@ def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
         pixels = sum(h * w for h, w in sizes)
         key = workload_key(pixels, sum(counts), entries, len(sizes), settings.normalize,
                            settings.fade_alpha > 0, settings.deterministic, fit=True,
-                           fused=settings.fused)
+                           fused=settings.use_fused())
         return _pick(key, candidates, build, repeats, use_cache)
     finally:
         for plan in plans.values():  # the probe backward added into the moments: clear them

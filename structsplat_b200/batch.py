@@ -127,8 +127,14 @@ class FitSettings:
     dilation: float = 0.0
     fade_alpha: float = 0.0
     deterministic: bool = False
-    # one tile kernel for forward, loss and backward (the same numbers as the two-kernel step)
-    fused: bool = True
+    # one tile kernel for forward, loss and backward (the same numbers as the two-kernel step);
+    # None: fused in fast mode, two kernels in deterministic mode (where the fused kernel's extra
+    # registers spill: 9.75 vs 9.65 ms on the 2048^2 / 1 M stress step, 8.79 vs 9.20 ms fused
+    # on the 64-image batched step)
+    fused: bool | None = None
+
+    def use_fused(self) -> bool:
+        return (not self.deterministic) if self.fused is None else bool(self.fused)
     betas: tuple = (0.9, 0.999)
     adam_eps: float = 1e-8
     scale_min: float = 0.35  # log-scale floor ln(0.35) (fit.py:3033)
@@ -289,7 +295,7 @@ class FitPlan:
             self.forward_loss(image=self.image, den=self.den)
             self.ssim_term()
             self.backward()
-        elif self.s.fused:
+        elif self.s.use_fused():
             self.forward_backward()
         else:
             self.forward_loss()
