@@ -36,6 +36,8 @@ METRIC = "fwd+bwd ms/iter (1024², 100k Gaussians); batched fit img/s vs plain k
 WORKLOAD = {"H": 1024, "W": 1024, "N": 100_000, "seed": 0, "mode": "normalized"}
 PAIR_SLOTS_FWD, PAIR_SLOTS_BWD = 14, 40   # FP32 issue slots per in-rectangle pair (reference)
 BACKWARD_DRAM_BYTES = 40_248_576 + 768  # one backward_kernel launch at this workload (ncu)
+# one fused forward + backward tile pass launch at this workload (ncu; bench.py --fused 1)
+FUSED_DRAM_BYTES = 23_515_392 + 512
 SM_COUNT, FP32_LANES = 148, 128
 
 
@@ -146,7 +148,7 @@ def run_ours(args, rank, world, dev):
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
 
     # ---- the measured step: forward + backward as one captured CUDA graph ----
-    plan = RenderPlan.for_field(params, H, W, normalize=normalize)
+    plan = RenderPlan.for_field(params, H, W, normalize=normalize, fused=args.fused == 1)
     _native.CALLS.clear()
     plan.forward_backward(params, grad_out)
     torch.cuda.synchronize()
@@ -184,6 +186,7 @@ def run_ours(args, rank, world, dev):
     kt = {}
     for name, fn in (("forward", plan.render), ("backward_kernel", lambda: plan.backward_tiles(grad_out)),
                      ("backward", lambda: plan.backward(grad_out, params)),
+                     ("fused_tile_pass", lambda: plan.tile_pass(grad_out)),
                      ("binning", lambda: (plan.count(), plan.fill())),
                      ("project", lambda: plan.project(params))):
         for _ in range(3):
@@ -245,6 +248,7 @@ def run_ours(args, rank, world, dev):
     if world > 1:
         torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
     return {"total_ms": float(stats[0]), "e2e_total_ms": float(stats[1]), "step_ms": step_ms,
+            "fused": plan.use_fused(),
             "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
             "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
             "clocks": clocks.summary(), "host": host}
@@ -256,6 +260,7 @@ KERNELS_PER_CALL = {
     "ss_project_rs": 1, "ss_pack_splats": 1, "ss_tile_index_count": 2, "ss_tile_index_fill": 3,
     "ss_render_forward": 1, "ss_render_backward": 2, "ss_project_rs_backward": 1,
     "ss_render_backward_moments": 1, "ss_render_backward_finalize_rs": 1,
+    "ss_render_forward_backward": 1,
 }
 
 
@@ -726,7 +731,8 @@ def main():
                     help="only time the SSIM term on one 2048x2048 image (for ncu)")
     ap.add_argument("--fused", type=int, default=-1, choices=[-1, 0, 1],
                     help="fit legs: forward, loss and backward in one tile pass (1), two (0), "
-                         "or the plan's choice (-1: fused in fast mode)")
+                         "or the plan's choice (-1: fused in fast mode); the fwd+bwd step: "
+                         "one tile pass only with 1")
     ap.add_argument("--dependent-launch", type=int, default=1, choices=[0, 1],
                     help="programmatic dependent launch of the library's kernels (1: on)")
     ap.add_argument("--profile", action="store_true",
@@ -810,6 +816,23 @@ def main():
         kt = res["kernels_ms"]
         bwd_ach = P * PAIR_SLOTS_BWD / (kt["backward_kernel"] * 1e-3) / 1e9
         fwd_ach = P * PAIR_SLOTS_FWD / (kt["forward"] * 1e-3) / 1e9
+        fused_ach = P * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (kt["fused_tile_pass"] * 1e-3) / 1e9
+        if res["fused"]:
+            roof = {"kernel": "backward_kernel (fused forward + backward tile pass)",
+                    "achieved": fused_ach, "traffic": FUSED_DRAM_BYTES,
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one fused "
+                                      "tile pass launch, ncu --set full "
+                                      "(profiles/fused_tile_pass_1024x1024_100k.md)",
+                    "work": f"{PAIR_SLOTS_FWD}+{PAIR_SLOTS_BWD} FP32 issue slots per "
+                            f"in-rectangle pair x {P} pairs per launch"}
+        else:
+            roof = {"kernel": "backward_kernel", "achieved": bwd_ach,
+                    "traffic": BACKWARD_DRAM_BYTES,
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                      "backward_kernel launch, ncu --set full "
+                                      "(profiles/backward_kernel_1024x1024_100k.md)",
+                    "work": f"{PAIR_SLOTS_BWD} FP32 issue slots per in-rectangle pair x "
+                            f"{P} pairs per launch"}
         t_bound_ms = P * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (peak_slots * 1e9) * 1e3
         line = {
             "metric": METRIC, "value": round(ms, 4), "unit": "ms/iter", "n_gpus": world,
@@ -824,18 +847,16 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "dependent_launch": args.dependent_launch,
                        "step": "one captured CUDA graph: RS projection, tile binning, forward, "
-                               "backward, RS chain rule"},
-            "roofline": {"bound": "fp32", "kernel": "backward_kernel",
-                         "achieved": round(bwd_ach, 1), "peak": round(peak_slots, 1),
-                         "unit": "Gslot/s", "frac": round(bwd_ach / peak_slots, 4),
-                         "traffic": BACKWARD_DRAM_BYTES,
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                           "backward_kernel launch, ncu --set full "
-                                           "(profiles/backward_kernel_1024x1024_100k.md)",
-                         "work": f"{PAIR_SLOTS_BWD} FP32 issue slots per in-rectangle pair x "
-                                 f"{P} pairs per launch",
+                               "backward, RS chain rule",
+                       "fused_tile_pass": res["fused"]},
+            "roofline": {"bound": "fp32", "kernel": roof["kernel"],
+                         "achieved": round(roof["achieved"], 1), "peak": round(peak_slots, 1),
+                         "unit": "Gslot/s", "frac": round(roof["achieved"] / peak_slots, 4),
+                         "traffic": roof["traffic"], "traffic_source": roof["traffic_source"],
+                         "work": roof["work"],
                          "peak_source": "148 SMs x 128 FP32 lanes x sm_max_mhz of "
                                         "MEASURED_PEAKS.json"},
+            "backward_kernel_roofline_frac": round(bwd_ach / peak_slots, 4),
             "kernels_ms": {k: round(v, 4) for k, v in kt.items()},
             "eager_autograd_ms_per_step": round(res["eager_ms"], 4),
             "forward_roofline_frac": round(fwd_ach / peak_slots, 4),

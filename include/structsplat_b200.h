@@ -271,6 +271,22 @@ int ss_fit_ssim(const ss_batch* batch, const float* image, const float* den, con
                 const float* stats, int normalize, float eps, float ssim_weight,
                 float* pixel_grad, float* ssim, void* workspace, size_t workspace_bytes,
                 ss_stream_t stream);
+/* ss_render_forward followed by ss_render_backward_moments in one kernel launch, for a caller
+ * that holds grad_out (H,W,3) before the forward (a fixed image-space gradient, as the
+ * reference's fwd+bwd benchmark uses): each tile's CTA stages its records once, renders out and
+ * den (written as ss_render_forward writes them) and forms the backward's pixel inputs from
+ * grad_out and its own accumulators in shared memory.  The workspace is
+ * ss_render_backward_moments's (fast mode: moments zero on entry); finish with
+ * ss_render_backward_finalize or ss_render_backward_finalize_rs.  Deterministic mode: a tile
+ * whose list the capacity truncated raises SS_STATUS_DETERMINISTIC_TRUNCATED and renders
+ * nothing.  No counterpart in the reference, whose renderer and autograd run as separate
+ * passes. */
+int ss_render_forward_backward(const void* records, int64_t n, const int32_t* tile_gids,
+                               int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                               int width, int tile_size, int normalize, float eps,
+                               float fade_tail, const float* grad_out, float* out, float* den,
+                               int deterministic, void* workspace, size_t workspace_bytes,
+                               uint32_t* status, ss_stream_t stream);
 /* Gradients of the five parameter groups from the backward's workspace, then one Adam step
  * (torch.optim.Adam's multi-tensor step: lerp first moment, step factors formed in double, no
  * weight decay), then the clamp of log_scales to [log_scale_lo, log_scale_hi[image]] that the

@@ -104,6 +104,8 @@ SIGNATURES = {
     "ss_ssim_target_stats": [_bp, _vp, _vp, _vp, ctypes.c_size_t, _vp],
     "ss_fit_ssim": [_bp, _vp, _vp, _vp, _vp, _int, _f32, _f32, _vp, _vp, _vp, ctypes.c_size_t,
                     _vp],
+    "ss_render_forward_backward": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _f32, _f32,
+                                   _vp, _vp, _vp, _int, _vp, ctypes.c_size_t, _vp, _vp],
     "ss_fit_forward_backward": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _f32, _f32, _vp, _int,
                                 _f32, _vp, _vp, _vp, _int, _vp, ctypes.c_size_t, _vp, _vp],
     "ss_fit_adam_update": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _vp, _f32, _pp, _pp, _pp, _dp,

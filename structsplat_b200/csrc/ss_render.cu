@@ -324,7 +324,29 @@ struct FusedFit {
   float* loss;
   int loss_kind;  // LossKind: kL1, kL2 or kCharbonnier
   float charb_eps2;
+  // render mode (target unused): the pixel inputs come from this (P,3) image gradient as in the
+  // backward's own prologue, and image / den are always written
+  const float* grad_out;
 };
+
+// A render forward's outputs at pixel p and the backward's per-pixel input from grad_out: the
+// arithmetic of forward_kernel's epilogue and of the backward prologue (out = num / (den + eps)
+// in normalized mode).
+__device__ __forceinline__ float4 render_pixel_grad(int normalize, const float* a, int64_t p,
+                                                    float eps, const float* __restrict__ go,
+                                                    float* out, float* den) {
+  const float denom = a[3] + eps;
+  float o[3];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) o[ch] = normalize ? a[ch] / denom : a[ch];
+  den[p] = a[3];
+  out[3 * p] = o[0];
+  out[3 * p + 1] = o[1];
+  out[3 * p + 2] = o[2];
+  const float gr = go[3 * p], gg = go[3 * p + 1], gb = go[3 * p + 2];
+  if (!normalize) return make_float4(gr, gg, gb, 0.f);
+  return make_float4(gr / denom, gg / denom, gb / denom, -(gr * o[0] + gg * o[1] + gb * o[2]) / denom);
+}
 
 // finish_pixel with the loss kind and normalisation chosen at run time (uniform per launch).
 __device__ __forceinline__ float4 finish_pixel_rt(int normalize, int loss_kind, const float* a,
@@ -620,11 +642,15 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
           float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
           if (px < W && py < H) {
             const int64_t p = fr.pixel_base + (int64_t)py * W + px;
-            float lp, sq;
-            v = finish_pixel_rt(normalize, ff.loss_kind, acc[i][k], p, eps, per_value,
-                                ff.charb_eps2, ff.image, ff.den, ff.target, lp, sq);
-            loss_sum += lp;
-            sq_sum += sq;
+            if (ff.grad_out) {
+              v = render_pixel_grad(normalize, acc[i][k], p, eps, ff.grad_out, ff.image, ff.den);
+            } else {
+              float lp, sq;
+              v = finish_pixel_rt(normalize, ff.loss_kind, acc[i][k], p, eps, per_value,
+                                  ff.charb_eps2, ff.image, ff.den, ff.target, lp, sq);
+              loss_sum += lp;
+              sq_sum += sq;
+            }
           }
           pix[ly * TS + lx] = v;
         }
@@ -1355,6 +1381,7 @@ int ss_fit_forward_backward(const ss_batch* batch, const void* records, int64_t 
   ff.loss = loss;
   ff.loss_kind = kinds[loss_kind];
   ff.charb_eps2 = (float)((double)charbonnier_eps * (double)charbonnier_eps);
+  ff.grad_out = nullptr;
   const Splat* rec = static_cast<const Splat*>(records);
   float* ws = static_cast<float*>(workspace);
   if (batch->tile_size == 16)
@@ -1364,6 +1391,47 @@ int ss_fit_forward_backward(const ss_batch* batch, const void* records, int64_t 
     launch_fused<32>((unsigned)T, s, deterministic, rec, n, tile_gids, gid_capacity,
                      tile_offsets, f, normalize, eps, fade_tail, ws, status, ff);
   if ((rc = check_launch("fit forward + backward"))) return rc;
+  if (!deterministic || n == 0) return SS_OK;
+  return order_entries(tile_gids, tile_offsets, T, gid_capacity, n, workspace, s);
+}
+
+int ss_render_forward_backward(const void* records, int64_t n, const int32_t* tile_gids,
+                               int64_t gid_capacity, const int32_t* tile_offsets, int height,
+                               int width, int tile_size, int normalize, float eps,
+                               float fade_tail, const float* grad_out, float* out, float* den,
+                               int deterministic, void* workspace, size_t workspace_bytes,
+                               uint32_t* status, ss_stream_t stream) {
+  int rc = check_render_args(n, height, width, tile_size, eps);
+  if (rc) return rc;
+  const size_t need = backward_ws_bytes(n, gid_capacity, deterministic);
+  if (workspace_bytes < need || !workspace)
+    return fail(SS_ERR_INVALID_ARGUMENT, "backward workspace too small (%zu < %zu)",
+                workspace_bytes, need);
+  cudaStream_t s = as_stream(stream);
+  if ((int64_t)height * width == 0)
+    return deterministic && n > 0 ? clear_entry_segments(workspace, n, gid_capacity, s) : SS_OK;
+  if (!tile_offsets || !grad_out || !out || !den)
+    return fail(SS_ERR_INVALID_ARGUMENT, "null tile offsets, grad_out, out or den");
+  if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
+  if (deterministic && gid_capacity > (int64_t)INT32_MAX)
+    return fail(SS_ERR_INVALID_ARGUMENT, "deterministic backward needs capacity < 2^31");
+  const int64_t T = (int64_t)((width + tile_size - 1) / tile_size) *
+                    ((height + tile_size - 1) / tile_size);
+  if (T > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "too many tiles");
+  FusedFit ff{};
+  ff.image = out;
+  ff.den = den;
+  ff.grad_out = grad_out;
+  const Frames f = single_frame(height, width, tile_size);
+  const Splat* rec = static_cast<const Splat*>(records);
+  float* ws = static_cast<float*>(workspace);
+  if (tile_size == 16)
+    launch_fused<16>((unsigned)T, s, deterministic, rec, n, tile_gids, gid_capacity,
+                     tile_offsets, f, normalize, eps, fade_tail, ws, status, ff);
+  else
+    launch_fused<32>((unsigned)T, s, deterministic, rec, n, tile_gids, gid_capacity,
+                     tile_offsets, f, normalize, eps, fade_tail, ws, status, ff);
+  if ((rc = check_launch("render forward + backward"))) return rc;
   if (!deterministic || n == 0) return SS_OK;
   return order_entries(tile_gids, tile_offsets, T, gid_capacity, n, workspace, s);
 }
