@@ -90,17 +90,22 @@ __device__ __forceinline__ int chunk_len(int64_t count, int64_t k0) {
   return r < kChunk ? (int)r : kChunk;
 }
 
-// Mask of the staged entries [32 r, 32 r + 32) whose support rectangle touches the 8x8 block
-// at (sx0, sy0): lane l tests entry 32 r + l, a ballot collects the answers.
-__device__ __forceinline__ unsigned hit_mask(const float4 (*st)[4], int m, int sx0, int sy0,
-                                             int lane, int r) {
-  const int j = lane + 32 * r;
-  bool hit = false;
-  if (j < m) {
-    const int4 b = *reinterpret_cast<const int4*>(&st[j][3]);
-    hit = b.x < sx0 + 8 && b.z > sx0 && b.y < sy0 + 8 && b.w > sy0;
+// Ballot of the staged entries [0, min(m, 32)) whose support rectangle touches the 8x8 block at
+// (sx0, sy0); lane l also gets entry l's cover of the block: bit c (c < 8) for block column c
+// inside [x0, x1), bit 8 + k for block row k inside [y0, y1).  A rectangle touches the block
+// exactly when both halves of its cover are non-zero.
+__device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int sx0, int sy0,
+                                              int lane, unsigned& cover) {
+  cover = 0u;
+  if (lane < m) {
+    const int4 b = *reinterpret_cast<const int4*>(&st[lane][3]);
+    const int x0 = min(max(b.x - sx0, 0), 8), x1 = min(max(b.z - sx0, 0), 8);
+    const int y0 = min(max(b.y - sy0, 0), 8), y1 = min(max(b.w - sy0, 0), 8);
+    const unsigned xm = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
+    const unsigned ym = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
+    if (xm && ym) cover = xm | (ym << 8);
   }
-  return __ballot_sync(0xffffffffu, hit);
+  return __ballot_sync(0xffffffffu, cover != 0u);
 }
 
 // Lists up to kStageAll Gaussians are staged whole (one barrier per tile; the warps then run
@@ -121,24 +126,27 @@ __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
   }
 }
 
-// Accumulates the staged entries [0, m) into one warp's two pixels per lane.
+// Accumulates the staged entries [0, m) into one warp's two pixels per lane: lane l holds
+// block column l & 7 of block rows l >> 3 and (l >> 3) + 4; a pixel outside an entry's
+// rectangle (a clear bit of the entry's cover) adds a zero weight.
 template <bool FADE>
 __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int sx0, int sy0,
                                               int lane, int px, int py0, float fx, float fy0,
                                               float tail, float (&acc0)[4], float (&acc1)[4]) {
+  const unsigned col = 1u << (lane & 7);
+  const unsigned need0 = col | (1u << (8 + (lane >> 3)));
+  const unsigned need1 = col | (1u << (12 + (lane >> 3)));
   for (int base = 0; base < m; base += 32) {
-    unsigned hits = hit_mask(st + base, m - base, sx0, sy0, lane, 0);
+    unsigned cover;
+    unsigned hits = hit_cover(st + base, m - base, sx0, sy0, lane, cover);
     while (hits) {
-      const int j = base + __ffs(hits) - 1;
+      const int src = __ffs(hits) - 1;
       hits &= hits - 1;
-      const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
+      const int j = base + src;
+      const unsigned cv = __shfl_sync(0xffffffffu, cover, src);
       const float4 p0 = st[j][0], p1 = st[j][1];
       const float cb = st[j][2].x;
-      // half-open range tests as one unsigned compare each: x in [x0, x1) <=> x - x0 < x1 - x0
-      const unsigned ry = (unsigned)(py0 - r.y), rh = (unsigned)(r.w - r.y);
-      const bool inx = (unsigned)(px - r.x) < (unsigned)(r.z - r.x);
-      const bool in0 = inx && ry < rh;
-      const bool in1 = inx && ry + 4u < rh;
+      const bool in0 = (cv & need0) == need0, in1 = (cv & need1) == need1;
       const float dx = fx - p0.x, dy0 = fy0 - p0.y, dy1 = dy0 + 4.0f;
       const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
       const float raw0 = fast_exp2(fmaf(dy0, fmaf(p1.x, dy0, bdx), adx2));
