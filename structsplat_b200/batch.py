@@ -236,6 +236,16 @@ class FitPlan:
                      int(self.cull), float(self.s.sigma_cutoff), _p(self.offsets), _p(self.idx_ws),
                      self.idx_ws_bytes, _p(self.status), _stream())
 
+    def project_count(self):
+        """project() and count() in one kernel (ss_batch_project_rs_index_count)."""
+        p = self.params
+        _native.call("ss_batch_project_rs_index_count", self.batch.ref, _p(p["means"]),
+                     _p(p["log_scales"]), _p(p["rotations"]), _p(p["colors"]),
+                     _p(p.get("opacity_logits")), self.n, float(self.s.dilation),
+                     float(self.s.sigma_cutoff), int(self.cull), _p(self.records),
+                     _p(self.offsets), _p(self.idx_ws), self.idx_ws_bytes, _p(self.status),
+                     _stream())
+
     def fill(self):
         _native.call("ss_batch_tile_index_fill", self.batch.ref, _p(self.records), self.n,
                      int(self.cull), float(self.s.sigma_cutoff), _p(self.offsets), _p(self.gids),
@@ -287,8 +297,7 @@ class FitPlan:
     def step(self):
         """One fit iteration for every image of the batch."""
         self.loss.zero_()
-        self.project()
-        self.count()
+        self.project_count()
         self.fill()
         if self.s.ssim_weight > 0.0:
             self.ssim.zero_()
@@ -306,8 +315,7 @@ class FitPlan:
         """Current images (P,3) and the per-image [loss, mse] of the current field."""
         image = torch.empty(max(self.batch.pixels, 1), 3, device=self.target.device)
         self.loss.zero_()
-        self.project()
-        self.count()
+        self.project_count()
         self.fill()
         self.forward_loss(image=image)
         return image[: self.batch.pixels], self.loss.clone()

@@ -10,6 +10,7 @@
 #include <climits>
 
 #include <cub/block/block_radix_sort.cuh>
+#include <cub/block/block_scan.cuh>
 #include <cub/device/device_scan.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <thrust/iterator/transform_iterator.h>
@@ -184,13 +185,95 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
   }
 }
 
-template <bool CULL>
+// Exclusive scan of the T+1 counters into int64 and int32 offsets by one CTA of kThreads
+// threads, in rounds of 4 kThreads items; the counters are read from L2 (other CTAs' atomics).
+__device__ void block_scan_counts(const int* tile_count, int64_t items, long long* off64,
+                                  int32_t* off32) {
+  using Scan = cub::BlockScan<long long, kThreads>;
+  __shared__ typename Scan::TempStorage tmp;
+  long long carry = 0;
+  for (int64_t b0 = 0; b0 < items; b0 += 4 * kThreads) {
+    long long v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t idx = b0 + 4 * threadIdx.x + k;
+      v[k] = idx < items ? __ldcg(tile_count + idx * kCounterStride) : 0;
+    }
+    long long total;
+    Scan(tmp).ExclusiveSum(v, v, total);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t idx = b0 + 4 * threadIdx.x + k;
+      if (idx < items) {
+        const long long o = carry + v[k];
+        off64[idx] = o;
+        off32[idx] = (int32_t)(o < 2147483647LL ? o : 2147483647LL);
+      }
+    }
+    carry += total;
+    __syncthreads();  // tmp is reused by the next round
+  }
+}
+
+// Per-tile counts by atomics.  SCAN: the last CTA to finish (a ticket in the padding word after
+// counter 0, zeroed with the counters) also scans the counts into the offsets, which saves the
+// separate scan launch for small tile sets.
+template <bool CULL, bool SCAN>
 __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int ts, Frames frames,
-                                  float cutoff2, int* __restrict__ tile_count) {
+                                  float cutoff2, int* __restrict__ tile_count, int64_t items,
+                                  long long* __restrict__ off64, int32_t* __restrict__ off32) {
   pdl_wait();
   pdl_trigger();
   enumerate_pairs<CULL>(rec, n, ts, frames, cutoff2,
                         [&](int, int, int t) { atomicAdd(tile_count + (int64_t)t * kCounterStride, 1); });
+  if constexpr (SCAN) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();  // this CTA's counts before its ticket
+      const unsigned ticket = atomicAdd(reinterpret_cast<unsigned*>(tile_count + 1), 1u);
+      last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();  // every other CTA's counts are visible after its ticket
+    block_scan_counts(tile_count, items, off64, off32);
+  }
+}
+
+// The RS projection (rs_project_one, as project_rs_kernel) and the per-tile counts in one pass:
+// each thread stores its Gaussian's record and counts its tiles from it, so the counts need no
+// second read of the records from DRAM.  The record is read back by its own thread (and, for a
+// rectangle the warp enumerates together, by the warp after __syncwarp), so `out` carries no
+// read-only qualifier.  SCAN as in tile_count_kernel.
+template <bool CULL, bool SCAN>
+__global__ void project_count_kernel(RSField field, int64_t n, int ts, Frames frames,
+                                     float cutoff2, Splat* out, int* __restrict__ tile_count,
+                                     int64_t items, long long* __restrict__ off64,
+                                     int32_t* __restrict__ off32) {
+  pdl_wait();
+  pdl_trigger();
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    long long rx, ry;
+    store_splat(out + i, rs_project_one(field, i, frame_of_gaussian(frames, i, n), rx, ry));
+  }
+  __syncwarp();
+  enumerate_pairs<CULL>(out, n, ts, frames, cutoff2,
+                        [&](int, int, int t) { atomicAdd(tile_count + (int64_t)t * kCounterStride, 1); });
+  if constexpr (SCAN) {
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned ticket = atomicAdd(reinterpret_cast<unsigned*>(tile_count + 1), 1u);
+      last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    block_scan_counts(tile_count, items, off64, off32);
+  }
 }
 
 // Writes int32 offsets, checks capacity, then claims one slot per pair.  Slots are claimed by
@@ -239,6 +322,7 @@ __global__ void tile_fill_kernel(const Splat* __restrict__ rec, int64_t n, int t
 constexpr int kScanThreads = 1024;
 constexpr int kScanPerThread = 16;
 constexpr int64_t kSingleScanMax = (int64_t)kScanThreads * kScanPerThread;
+constexpr int64_t kFusedScanMax = 16 * kThreads;
 
 __global__ void __launch_bounds__(kScanThreads)
     single_scan_kernel(const int* __restrict__ tile_count, int64_t items,
@@ -481,9 +565,12 @@ int check_index_args(int64_t n, int H, int W, int ts) {
 
 
 // Stage 1 over any tile set (one image or a batch): counts, scan, int32 offsets.
+// With `rs`, the records are first projected from that RS field in the same kernel
+// (project_count_kernel) and written to `records`.
 int index_count(const Frames& frames, int ts, int64_t T, const void* records, int64_t n,
                 int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets, void* workspace,
-                size_t workspace_bytes, uint32_t* status, ss_stream_t stream) {
+                size_t workspace_bytes, uint32_t* status, ss_stream_t stream,
+                const RSField* rs = nullptr) {
   int rc;
   if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
@@ -497,18 +584,42 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
     return check_launch("tile_index_count memset");
   const Splat* rec = static_cast<const Splat*>(records);
   float cutoff2 = sigma_cutoff * sigma_cutoff;
-  if (n > 0 && T > 0) {
+  // the count kernel's last CTA scans up to kFusedScanMax counters (four rounds); larger sets
+  // up to kSingleScanMax take the 1024-thread scan kernel, beyond that CUB's device scan
+  const bool fused_scan = T + 1 <= kFusedScanMax;
+  const bool single_scan = T + 1 <= kSingleScanMax;
+  if (rs && n > 0) {  // project even when the tile set is empty: the records are an output
+    if (reinterpret_cast<uintptr_t>(records) % 16)
+      return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
     int blocks = (int)((n + kThreads - 1) / kThreads);
-    if (ellipse_cull)
-      launch("tile_count_kernel", tile_count_kernel<true>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2,
-                                                          w.tile_count);
-    else
-      launch("tile_count_kernel", tile_count_kernel<false>, blocks, kThreads, 0, s, rec, n, ts, frames, cutoff2,
-                                                           w.tile_count);
+    Splat* out = static_cast<Splat*>(const_cast<void*>(records));
+#define SS_PCOUNT(C, S)                                                                       \
+  launch("project_count_kernel", project_count_kernel<C, S>, blocks, kThreads, 0, s, *rs, n,   \
+         ts, frames, cutoff2, out, w.tile_count, T + 1, w.offsets64, tile_offsets)
+    if (ellipse_cull) {
+      if (fused_scan) SS_PCOUNT(true, true); else SS_PCOUNT(true, false);
+    } else {
+      if (fused_scan) SS_PCOUNT(false, true); else SS_PCOUNT(false, false);
+    }
+#undef SS_PCOUNT
+    if ((rc = check_launch("project_count"))) return rc;
+    if (fused_scan) return SS_OK;
+  } else if (n > 0 && T > 0) {
+    int blocks = (int)((n + kThreads - 1) / kThreads);
+#define SS_COUNT(C, S)                                                                        \
+  launch("tile_count_kernel", tile_count_kernel<C, S>, blocks, kThreads, 0, s, rec, n, ts,     \
+         frames, cutoff2, w.tile_count, T + 1, w.offsets64, tile_offsets)
+    if (ellipse_cull) {
+      if (fused_scan) SS_COUNT(true, true); else SS_COUNT(true, false);
+    } else {
+      if (fused_scan) SS_COUNT(false, true); else SS_COUNT(false, false);
+    }
+#undef SS_COUNT
     if ((rc = check_launch("tile_count"))) return rc;
+    if (fused_scan) return SS_OK;
   }
   (void)status;
-  if (T + 1 <= kSingleScanMax) {
+  if (single_scan) {
     launch("single_scan_kernel", single_scan_kernel, 1, kScanThreads, 0, s, w.tile_count, T + 1, w.offsets64,
                                                   tile_offsets);
     return check_launch("tile_offsets scan");
@@ -612,6 +723,42 @@ int ss_batch_tile_index_count(const ss_batch* batch, const void* records, int64_
   if (rc) return rc;
   return index_count(f, batch->tile_size, batch->tiles, records, n, ellipse_cull, sigma_cutoff,
                      tile_offsets, workspace, workspace_bytes, status, stream);
+}
+
+int ss_project_rs_index_count(const float* means, const float* log_scales,
+                              const float* rotations, const float* colors,
+                              const float* opacity_logits, int64_t n, float dilation,
+                              float sigma_cutoff, int height, int width, int tile_size,
+                              int ellipse_cull, void* records, int32_t* tile_offsets,
+                              void* workspace, size_t workspace_bytes, uint32_t* status,
+                              ss_stream_t stream) {
+  int rc = check_index_args(n, height, width, tile_size);
+  if (rc) return rc;
+  if (n > 0 && (!means || !log_scales || !rotations || !colors))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null RS field pointer");
+  if (!(dilation >= 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "dilation must be >= 0");
+  const RSField f{means, log_scales, rotations, colors, opacity_logits, dilation, sigma_cutoff};
+  return index_count(single_frame(height, width, tile_size), tile_size,
+                     make_grid(height, width, tile_size).T, records, n, ellipse_cull,
+                     sigma_cutoff, tile_offsets, workspace, workspace_bytes, status, stream, &f);
+}
+
+int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
+                                    const float* log_scales, const float* rotations,
+                                    const float* colors, const float* opacity_logits, int64_t n,
+                                    float dilation, float sigma_cutoff, int ellipse_cull,
+                                    void* records, int32_t* tile_offsets, void* workspace,
+                                    size_t workspace_bytes, uint32_t* status,
+                                    ss_stream_t stream) {
+  Frames fr;
+  int rc = frames_of_batch(batch, n, &fr);
+  if (rc) return rc;
+  if (n > 0 && (!means || !log_scales || !rotations || !colors))
+    return fail(SS_ERR_INVALID_ARGUMENT, "null RS field pointer");
+  if (!(dilation >= 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "dilation must be >= 0");
+  const RSField f{means, log_scales, rotations, colors, opacity_logits, dilation, sigma_cutoff};
+  return index_count(fr, batch->tile_size, batch->tiles, records, n, ellipse_cull, sigma_cutoff,
+                     tile_offsets, workspace, workspace_bytes, status, stream, &f);
 }
 
 int ss_tile_index_fill(const void* records, int64_t n, int height, int width, int tile_size,

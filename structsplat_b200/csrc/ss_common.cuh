@@ -264,6 +264,51 @@ __device__ __forceinline__ Frame frame_of_gaussian(const Frames& f, int64_t g, i
   return frame_of_image(f, f.image ? f.gauss_image[g] : 0, n);
 }
 
+// An RS field in device memory (means 2n, log-scales 2n, rotations n, colours 3n, opacity
+// logits n or NULL) with the projection's dilation and sigma cutoff.
+struct RSField {
+  const float* means;
+  const float* log_scales;
+  const float* rotations;
+  const float* colors;
+  const float* logits;
+  float dilation, cutoff;
+};
+
+// RS -> splat record of Gaussian i of frame fr, with its radii.  The conic follows
+// gaussians.py:275-300 and the radii gaussians.py:302-321; every product and sum is rounded
+// separately (no FMA contraction) so the radii's ceil() sees the same float the reference's
+// elementwise torch ops produce.
+__device__ __forceinline__ Splat rs_project_one(const RSField& f, int64_t i, const Frame& fr,
+                                                long long& rx, long long& ry) {
+  const float dilation = f.dilation, cutoff = f.cutoff;
+  float sx = expf(f.log_scales[2 * i]), sy = expf(f.log_scales[2 * i + 1]);
+  float sx2 = __fmul_rn(sx, sx), sy2 = __fmul_rn(sy, sy);
+  float th = f.rotations[i];
+  float cs = cosf(th), sn = sinf(th);
+  float cc = __fmul_rn(cs, cs), ss2 = __fmul_rn(sn, sn);
+  // conic
+  float ix = __fdiv_rn(1.0f, __fadd_rn(sx2, dilation));
+  float iy = __fdiv_rn(1.0f, __fadd_rn(sy2, dilation));
+  float a = __fadd_rn(__fmul_rn(cc, ix), __fmul_rn(ss2, iy));
+  float b = __fmul_rn(__fmul_rn(cs, sn), __fsub_rn(ix, iy));
+  float c = __fadd_rn(__fmul_rn(ss2, ix), __fmul_rn(cc, iy));
+  // radii: ceil(cutoff * sqrt(var)) clamped >= 1
+  float vx2 = __fadd_rn(sx2, dilation), vy2 = __fadd_rn(sy2, dilation);
+  float varx = __fadd_rn(__fmul_rn(cc, vx2), __fmul_rn(ss2, vy2));
+  float vary = __fadd_rn(__fmul_rn(ss2, vx2), __fmul_rn(cc, vy2));
+  float fr_x = ceilf(__fmul_rn(cutoff, __fsqrt_rn(varx)));
+  float fr_y = ceilf(__fmul_rn(cutoff, __fsqrt_rn(vary)));
+  rx = isfinite(fr_x) ? (long long)fmaxf(fminf(fr_x, 1e15f), 1.0f) : (1LL << 40);
+  ry = isfinite(fr_y) ? (long long)fmaxf(fminf(fr_y, 1e15f), 1.0f) : (1LL << 40);
+  float op = f.logits ? 1.0f / (1.0f + expf(-f.logits[i])) : 1.0f;
+  float mx = f.means[2 * i], my = f.means[2 * i + 1];
+  int x0, y0, x1, y1;
+  support_rect(mx, my, rx, ry, fr.H, fr.W, x0, y0, x1, y1);
+  return make_splat(mx, my, a, b, c, op, f.colors[3 * i], f.colors[3 * i + 1],
+                    f.colors[3 * i + 2], x0, y0, x1, y1);
+}
+
 // The backward's per-(tile, Gaussian) record in deterministic mode: nine moments, padded.
 constexpr int kMoments = 9;
 constexpr int kPartialFloats = 12;

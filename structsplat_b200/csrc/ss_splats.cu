@@ -83,9 +83,7 @@ __global__ void pack_splats_kernel(const float* __restrict__ means,
                                   y0, x1, y1));
 }
 
-// RS -> conic, radii and opacity.  The conic follows gaussians.py:275-300 and the radii
-// gaussians.py:302-321; every product and sum is rounded separately (no FMA contraction) so
-// the radii's ceil() sees the same float the reference's elementwise torch ops produce.
+// RS -> splat record (rs_project_one), plus the conic and radii where asked for.
 __global__ void project_rs_kernel(const float* __restrict__ means,
                                   const float* __restrict__ log_scales,
                                   const float* __restrict__ rotations,
@@ -98,36 +96,14 @@ __global__ void project_rs_kernel(const float* __restrict__ means,
   pdl_trigger();
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float sx = expf(log_scales[2 * i]), sy = expf(log_scales[2 * i + 1]);
-  float sx2 = __fmul_rn(sx, sx), sy2 = __fmul_rn(sy, sy);
-  float th = rotations[i];
-  float cs = cosf(th), sn = sinf(th);
-  float cc = __fmul_rn(cs, cs), ss2 = __fmul_rn(sn, sn);
-  // conic
-  float ix = __fdiv_rn(1.0f, __fadd_rn(sx2, dilation));
-  float iy = __fdiv_rn(1.0f, __fadd_rn(sy2, dilation));
-  float a = __fadd_rn(__fmul_rn(cc, ix), __fmul_rn(ss2, iy));
-  float b = __fmul_rn(__fmul_rn(cs, sn), __fsub_rn(ix, iy));
-  float c = __fadd_rn(__fmul_rn(ss2, ix), __fmul_rn(cc, iy));
-  // radii: ceil(cutoff * sqrt(var)) clamped >= 1
-  float vx2 = __fadd_rn(sx2, dilation), vy2 = __fadd_rn(sy2, dilation);
-  float varx = __fadd_rn(__fmul_rn(cc, vx2), __fmul_rn(ss2, vy2));
-  float vary = __fadd_rn(__fmul_rn(ss2, vx2), __fmul_rn(cc, vy2));
-  float fr_x = ceilf(__fmul_rn(cutoff, __fsqrt_rn(varx)));
-  float fr_y = ceilf(__fmul_rn(cutoff, __fsqrt_rn(vary)));
-  long long rx = isfinite(fr_x) ? (long long)fmaxf(fminf(fr_x, 1e15f), 1.0f) : (1LL << 40);
-  long long ry = isfinite(fr_y) ? (long long)fmaxf(fminf(fr_y, 1e15f), 1.0f) : (1LL << 40);
-  float op = logits ? 1.0f / (1.0f + expf(-logits[i])) : 1.0f;
-  float mx = means[2 * i], my = means[2 * i + 1];
-  int x0, y0, x1, y1;
-  const Frame fr = frame_of_gaussian(frames, i, n);
-  support_rect(mx, my, rx, ry, fr.H, fr.W, x0, y0, x1, y1);
-  store_splat(out + i, make_splat(mx, my, a, b, c, op, colors[3 * i], colors[3 * i + 1],
-                                  colors[3 * i + 2], x0, y0, x1, y1));
+  const RSField f{means, log_scales, rotations, colors, logits, dilation, cutoff};
+  long long rx, ry;
+  const Splat sp = rs_project_one(f, i, frame_of_gaussian(frames, i, n), rx, ry);
+  store_splat(out + i, sp);
   if (conics_out) {
-    conics_out[3 * i] = a;
-    conics_out[3 * i + 1] = b;
-    conics_out[3 * i + 2] = c;
+    conics_out[3 * i] = sp.a;
+    conics_out[3 * i + 1] = sp.b;
+    conics_out[3 * i + 2] = sp.c;
   }
   if (radii_out) {
     radii_out[2 * i] = rx;

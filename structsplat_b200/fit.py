@@ -107,6 +107,15 @@ class RenderPlan:
                      self.tile_size, int(self.cull), float(self.sigma_cutoff), _p(self.offsets),
                      _p(self.idx_ws), self.idx_ws_bytes, _p(self.status), _stream())
 
+    def project_count(self, params):
+        """project() and count() in one kernel (ss_project_rs_index_count)."""
+        _native.call("ss_project_rs_index_count", _p(params["means"]), _p(params["log_scales"]),
+                     _p(params["rotations"]), _p(params["colors"]),
+                     _p(params.get("opacity_logits") if self.has_opacity else None), self.n,
+                     float(self.dilation), float(self.sigma_cutoff), self.H, self.W,
+                     self.tile_size, int(self.cull), _p(self.records), _p(self.offsets),
+                     _p(self.idx_ws), self.idx_ws_bytes, _p(self.status), _stream())
+
     def fill(self):
         _native.call("ss_tile_index_fill", _p(self.records), self.n, self.H, self.W,
                      self.tile_size, int(self.cull), float(self.sigma_cutoff), _p(self.offsets),
@@ -153,8 +162,7 @@ class RenderPlan:
 
     def forward(self, params):
         self.status.zero_()
-        self.project(params)
-        self.count()
+        self.project_count(params)
         self.fill()
         self.render()
         return self.image
@@ -175,8 +183,7 @@ class RenderPlan:
             self.backward(grad_out, params, moments_zeroed=True)
             return self.grads()
         self.status.zero_()
-        self.project(params)
-        self.count()
+        self.project_count(params)
         self.fill()
         self.tile_pass(grad_out)
         if self.n:

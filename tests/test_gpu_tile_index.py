@@ -70,6 +70,21 @@ def test_random_fields_match_oracle(ts, seed):
     assert not np.isin([40, 41, 42], gids).any()
 
 
+@pytest.mark.parametrize("H, W", [(1, 1), (31, 33), (63, 65), (64, 64), (127, 129), (128, 128)])
+def test_scan_regimes_match_oracle(H, W):
+    """Tile sets on both sides of each scan regime's limit (one-pixel tiles, so T = H W): the
+    count kernel's last CTA scans up to 4,095 tiles, the single-CTA scan kernel up to 16,383,
+    CUB's device scan beyond."""
+    require_cuda()
+    f = make_field(H, W, 500, seed=H + W, log_sigma_std=0.6)
+    radii = field_ref.radii(torch.tensor(f.log_scales), torch.tensor(f.rotations), 3.0).numpy()
+    for _ in range(2):  # built twice: the same index both times
+        gids, offsets = _index(f.means, radii, H, W, 1)
+    ref_g, ref_o = c_oracle.tile_index(f.means, radii, H, W, 1)
+    assert np.array_equal(offsets, ref_o)
+    assert np.array_equal(gids, ref_g)
+
+
 @pytest.mark.parametrize("n", [3000, 20000])
 def test_long_tile_lists_are_sorted(n):
     """Lists longer than the per-warp sort (1024) and the per-CTA shared-memory sort (16384)."""
