@@ -170,6 +170,15 @@ def run_ours(args, rank, world, dev):
     if plan.overflowed():
         raise RuntimeError("tile index capacity exceeded during the timed steps")
 
+    # ---- the additive mode's step (the same field, no normalisation) ----
+    plan_add = RenderPlan.for_field(params, H, W, normalize=False, fused=args.fused == 1)
+    step_add = CapturedStep(lambda: plan_add.forward_backward(params, grad_out),
+                            warmup=args.warmup)
+    additive_ms = timed_loop(step_add.replay, args.steps, flush)
+    if plan_add.overflowed():
+        raise RuntimeError("tile index capacity exceeded during the additive steps")
+    del step_add, plan_add
+
     # ---- the same step through the eager autograd API (render_gaussians + autograd.grad) ----
     leaves = [params[k].clone().requires_grad_(True) for k in names]
 
@@ -248,7 +257,7 @@ def run_ours(args, rank, world, dev):
     if world > 1:
         torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
     return {"total_ms": float(stats[0]), "e2e_total_ms": float(stats[1]), "step_ms": step_ms,
-            "fused": plan.use_fused(),
+            "fused": plan.use_fused(), "additive_ms": statistics.median(additive_ms),
             "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
             "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
             "clocks": clocks.summary(), "host": host}
@@ -319,7 +328,7 @@ def cpu_baseline(host, budget_s=20.0):
                       "for the median), torch CPU, all host threads"}
 
 
-def ref_cuda_baseline(host, dev, steps=10):
+def ref_cuda_baseline(host, dev, steps=10, normalize=True):
     """The reference's own CUDA extension (built unmodified for sm_100a into baseline/_ref)
     through its public render_cuda_exact, untiled and tiled arms; None when not built."""
     try:
@@ -340,7 +349,8 @@ def ref_cuda_baseline(host, dev, steps=10):
     for arm, kw in (("cuda", dict(tiled=False)), ("cuda_tiled", dict(tiled=True))):
         def step():
             img = cuda_render.render_cuda_exact(f.means, f.conics(), f.colors, f.radii(3.0), H, W,
-                                                opacities=f.opacity_values(), **kw)
+                                                opacities=f.opacity_values(),
+                                                normalize=normalize, **kw)
             torch.autograd.grad(img, params, go)
         for _ in range(3):
             step()
@@ -870,8 +880,12 @@ def main():
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(host)
+        line["additive"] = {"ms_per_step": round(res["additive_ms"], 4),
+                            "step": "the same captured step with normalize=False"}
         if world == 1 and not args.no_ref_cuda:
             line["reference_cuda_ms"] = ref_cuda_baseline(host, dev)
+            line["additive"]["reference_cuda_ms"] = ref_cuda_baseline(host, dev,
+                                                                      normalize=False)
         if batched is not None:
             line["batched"] = batched
         print(json.dumps(line), flush=True)
