@@ -60,7 +60,6 @@ class RenderPlan:
         f32 = dict(device=d, dtype=torch.float32)
         self.records = torch.empty(max(n, 1) * RECORD_FLOATS, **f32)
         self.offsets = torch.zeros(self.T + 1, device=d, dtype=torch.int32)
-        self.status = torch.zeros(1, device=d, dtype=torch.int32)
         self.idx_ws_bytes = _native.size_query("ss_tile_index_workspace_bytes", n, self.H, self.W,
                                                self.tile_size)
         self.idx_ws = torch.empty(max(self.idx_ws_bytes, 1), device=d, dtype=torch.uint8)
@@ -70,7 +69,12 @@ class RenderPlan:
         self.bwd_ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n,
                                                self.capacity, self.H, self.W,
                                                int(self.deterministic))
-        self.bwd_ws = torch.empty(max(self.bwd_ws_bytes, 16), device=d, dtype=torch.uint8)
+        # the backward workspace and the status word share one allocation, so a fast-mode step
+        # clears its moments and its status with one fill (clear_step)
+        ws_len = (max(self.bwd_ws_bytes, 16) + 255) // 256 * 256
+        self._step_block = torch.zeros(ws_len + 256, device=d, dtype=torch.uint8)
+        self.bwd_ws = self._step_block[:ws_len]
+        self.status = self._step_block[ws_len:ws_len + 4].view(torch.int32)
         self.image = torch.zeros(self.H, self.W, 3, **f32)
         self.den = torch.zeros(self.H, self.W, **f32)
         self.g_means = torch.zeros(n, 2, **f32)
@@ -160,8 +164,10 @@ class RenderPlan:
                      float(self.eps), float(self.tail), int(self.deterministic), _p(self.bwd_ws),
                      self.bwd_ws_bytes, _p(self.status), _stream())
 
-    def forward(self, params):
-        self.status.zero_()
+    def forward(self, params, cleared: bool = False):
+        """Project, bin and render; ``cleared``: clear_step() already zeroed the status."""
+        if not cleared:
+            self.status.zero_()
         self.project_count(params)
         self.fill()
         self.render()
@@ -170,19 +176,24 @@ class RenderPlan:
     def use_fused(self) -> bool:
         return bool(self.fused)
 
+    def clear_step(self):
+        """Zero the status word and, in fast mode, the backward's moments (one fill)."""
+        if self.n and not self.deterministic:
+            self._step_block.zero_()
+        else:
+            self.status.zero_()
+
     def forward_backward(self, params, grad_out):
         """Image, den and the RS gradients for a grad_out known before the forward: project,
         bin, then one tile pass rendering and back-propagating each tile (or the forward and
         backward tile kernels one after the other), then the per-Gaussian RS pass."""
         # the moments are cleared first so the step's kernels follow one another directly
         # (each may start while its predecessor drains)
-        if self.n and not self.deterministic:
-            self.bwd_ws.zero_()
+        self.clear_step()
         if not self.use_fused():
-            self.forward(params)
+            self.forward(params, cleared=True)
             self.backward(grad_out, params, moments_zeroed=True)
             return self.grads()
-        self.status.zero_()
         self.project_count(params)
         self.fill()
         self.tile_pass(grad_out)
