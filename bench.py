@@ -220,8 +220,7 @@ def run_ours(args, rank, world, dev):
     slots = [(params, grad_out)] + [({k: params[k].clone() for k in names}, grad_out.clone())]
 
     def fwd_part(p):
-        plan.clear_step()
-        plan.forward(p, cleared=True)
+        plan.forward(p, clear_moments=True)
 
     graphs = [(CapturedStep(lambda p=p: fwd_part(p), warmup=args.warmup),
                CapturedStep(lambda p=p, g=g: plan.backward(g, p, moments_zeroed=True), warmup=1))

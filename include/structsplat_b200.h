@@ -109,16 +109,19 @@ int ss_project_rs_backward(const float* log_scales, const float* rotations,
 /* ss_project_rs followed by ss_tile_index_count in one kernel: each thread projects its
  * Gaussian into `records` (bitwise the records ss_project_rs writes) and counts the tiles of
  * its rectangle from them, so the count reads no record back from DRAM; the offsets, status
- * and workspace are ss_tile_index_count's.  Continue with ss_tile_index_fill.  No counterpart
- * in the reference, which projects in torch and bins in its own kernel
+ * and workspace are ss_tile_index_count's.  Continue with ss_tile_index_fill.  `clear` (NULL
+ * when clear_bytes is 0) is a device region the same kernel zeroes, 16-byte aligned, a multiple
+ * of 16 bytes and disjoint from every other buffer of the call: a step's scratch that must start
+ * at zero (the fast-mode backward moments, a status word), cleared without a memset of its
+ * own.  No counterpart in the reference, which projects in torch and bins in its own kernel
  * (gaussians.py:275-321, render_ext.cu:858-952). */
 int ss_project_rs_index_count(const float* means, const float* log_scales,
                               const float* rotations, const float* colors,
                               const float* opacity_logits, int64_t n, float dilation,
                               float sigma_cutoff, int height, int width, int tile_size,
                               int ellipse_cull, void* records, int32_t* tile_offsets,
-                              void* workspace, size_t workspace_bytes, uint32_t* status,
-                              ss_stream_t stream);
+                              void* workspace, size_t workspace_bytes, void* clear,
+                              size_t clear_bytes, uint32_t* status, ss_stream_t stream);
 
 /* The same over a batch (ss_batch_project_rs, then ss_batch_tile_index_count). */
 int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
@@ -126,8 +129,8 @@ int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
                                     const float* colors, const float* opacity_logits, int64_t n,
                                     float dilation, float sigma_cutoff, int ellipse_cull,
                                     void* records, int32_t* tile_offsets, void* workspace,
-                                    size_t workspace_bytes, uint32_t* status,
-                                    ss_stream_t stream);
+                                    size_t workspace_bytes, void* clear, size_t clear_bytes,
+                                    uint32_t* status, ss_stream_t stream);
 
 /* ---------------------------------------------------------------- tile index
  * Tiles are tile_size x tile_size pixels, tiles_x = ceil(W/ts), T = tiles_x * ceil(H/ts);

@@ -58,7 +58,8 @@ SIGNATURES = {
     "ss_tile_index_fill": [_vp, _i64, _int, _int, _int, _int, _f32, _vp, _vp, _i64, _vp,
                            ctypes.c_size_t, _vp, _vp],
     "ss_project_rs_index_count": [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _int, _int, _int,
-                                  _int, _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp],
+                                  _int, _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t,
+                                  _vp, _vp],
     "ss_build_tile_index_static": [_vp, _vp, _vp, _i64, _int, _int, _int, _int, _f32, _vp, _i64,
                                    _vp, _vp, _vp],
     "ss_render_forward": [_vp, _i64, _vp, _i64, _vp, _int, _int, _int, _int, _f32, _f32, _vp, _vp,
@@ -93,7 +94,8 @@ SIGNATURES = {
     "ss_batch_tile_index_fill": [_bp, _vp, _i64, _int, _f32, _vp, _vp, _i64, _vp,
                                  ctypes.c_size_t, _vp, _vp],
     "ss_batch_project_rs_index_count": [_bp, _vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _int,
-                                        _vp, _vp, _vp, ctypes.c_size_t, _vp, _vp],
+                                        _vp, _vp, _vp, ctypes.c_size_t, _vp, ctypes.c_size_t,
+                                        _vp, _vp],
     "ss_batch_render_forward": [_bp, _vp, _i64, _vp, _i64, _vp, _int, _f32, _f32, _vp, _vp, _vp,
                                 _vp],
     "ss_batch_render_backward": [_bp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _f32,

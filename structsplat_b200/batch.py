@@ -243,8 +243,8 @@ class FitPlan:
                      _p(p["log_scales"]), _p(p["rotations"]), _p(p["colors"]),
                      _p(p.get("opacity_logits")), self.n, float(self.s.dilation),
                      float(self.s.sigma_cutoff), int(self.cull), _p(self.records),
-                     _p(self.offsets), _p(self.idx_ws), self.idx_ws_bytes, _p(self.status),
-                     _stream())
+                     _p(self.offsets), _p(self.idx_ws), self.idx_ws_bytes, None, 0,
+                     _p(self.status), _stream())
 
     def fill(self):
         _native.call("ss_batch_tile_index_fill", self.batch.ref, _p(self.records), self.n,

@@ -245,15 +245,19 @@ __global__ void tile_count_kernel(const Splat* __restrict__ rec, int64_t n, int 
 // each thread stores its Gaussian's record and counts its tiles from it, so the counts need no
 // second read of the records from DRAM.  The record is read back by its own thread (and, for a
 // rectangle the warp enumerates together, by the warp after __syncwarp), so `out` carries no
-// read-only qualifier.  SCAN as in tile_count_kernel.
+// read-only qualifier.  SCAN as in tile_count_kernel.  The grid also zeroes `clear_vec` 16-byte
+// words at `clear` (a caller's per-step scratch, such as the next backward's moments).
 template <bool CULL, bool SCAN>
 __global__ void project_count_kernel(RSField field, int64_t n, int ts, Frames frames,
                                      float cutoff2, Splat* out, int* __restrict__ tile_count,
                                      int64_t items, long long* __restrict__ off64,
-                                     int32_t* __restrict__ off32) {
+                                     int32_t* __restrict__ off32, uint4* __restrict__ clear,
+                                     int64_t clear_vec) {
   pdl_wait();
   pdl_trigger();
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t v = i; v < clear_vec; v += (int64_t)gridDim.x * blockDim.x)
+    clear[v] = make_uint4(0u, 0u, 0u, 0u);
   if (i < n) {
     long long rx, ry;
     store_splat(out + i, rs_project_one(field, i, frame_of_gaussian(frames, i, n), rx, ry));
@@ -570,7 +574,7 @@ int check_index_args(int64_t n, int H, int W, int ts) {
 int index_count(const Frames& frames, int ts, int64_t T, const void* records, int64_t n,
                 int ellipse_cull, float sigma_cutoff, int32_t* tile_offsets, void* workspace,
                 size_t workspace_bytes, uint32_t* status, ss_stream_t stream,
-                const RSField* rs = nullptr) {
+                const RSField* rs = nullptr, void* clear = nullptr, size_t clear_bytes = 0) {
   int rc;
   if (!tile_offsets || !workspace) return fail(SS_ERR_INVALID_ARGUMENT, "null pointer");
   if (n > 0 && !records) return fail(SS_ERR_INVALID_ARGUMENT, "null records");
@@ -588,6 +592,11 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
   // up to kSingleScanMax take the 1024-thread scan kernel, beyond that CUB's device scan
   const bool fused_scan = T + 1 <= kFusedScanMax;
   const bool single_scan = T + 1 <= kSingleScanMax;
+  if (clear_bytes && (!clear || reinterpret_cast<uintptr_t>(clear) % 16 || clear_bytes % 16))
+    return fail(SS_ERR_INVALID_ARGUMENT,
+                "clear region must be 16-byte aligned and a multiple of 16 bytes");
+  if (clear_bytes && !(rs && n > 0) && cudaMemsetAsync(clear, 0, clear_bytes, s) != cudaSuccess)
+    return check_launch("clear region memset");
   if (rs && n > 0) {  // project even when the tile set is empty: the records are an output
     if (reinterpret_cast<uintptr_t>(records) % 16)
       return fail(SS_ERR_INVALID_ARGUMENT, "records must be 16-byte aligned");
@@ -595,7 +604,8 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
     Splat* out = static_cast<Splat*>(const_cast<void*>(records));
 #define SS_PCOUNT(C, S)                                                                       \
   launch("project_count_kernel", project_count_kernel<C, S>, blocks, kThreads, 0, s, *rs, n,   \
-         ts, frames, cutoff2, out, w.tile_count, T + 1, w.offsets64, tile_offsets)
+         ts, frames, cutoff2, out, w.tile_count, T + 1, w.offsets64, tile_offsets,           \
+         static_cast<uint4*>(clear), (int64_t)(clear_bytes / 16))
     if (ellipse_cull) {
       if (fused_scan) SS_PCOUNT(true, true); else SS_PCOUNT(true, false);
     } else {
@@ -730,8 +740,8 @@ int ss_project_rs_index_count(const float* means, const float* log_scales,
                               const float* opacity_logits, int64_t n, float dilation,
                               float sigma_cutoff, int height, int width, int tile_size,
                               int ellipse_cull, void* records, int32_t* tile_offsets,
-                              void* workspace, size_t workspace_bytes, uint32_t* status,
-                              ss_stream_t stream) {
+                              void* workspace, size_t workspace_bytes, void* clear,
+                              size_t clear_bytes, uint32_t* status, ss_stream_t stream) {
   int rc = check_index_args(n, height, width, tile_size);
   if (rc) return rc;
   if (n > 0 && (!means || !log_scales || !rotations || !colors))
@@ -740,7 +750,8 @@ int ss_project_rs_index_count(const float* means, const float* log_scales,
   const RSField f{means, log_scales, rotations, colors, opacity_logits, dilation, sigma_cutoff};
   return index_count(single_frame(height, width, tile_size), tile_size,
                      make_grid(height, width, tile_size).T, records, n, ellipse_cull,
-                     sigma_cutoff, tile_offsets, workspace, workspace_bytes, status, stream, &f);
+                     sigma_cutoff, tile_offsets, workspace, workspace_bytes, status, stream, &f,
+                     clear, clear_bytes);
 }
 
 int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
@@ -748,8 +759,8 @@ int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
                                     const float* colors, const float* opacity_logits, int64_t n,
                                     float dilation, float sigma_cutoff, int ellipse_cull,
                                     void* records, int32_t* tile_offsets, void* workspace,
-                                    size_t workspace_bytes, uint32_t* status,
-                                    ss_stream_t stream) {
+                                    size_t workspace_bytes, void* clear, size_t clear_bytes,
+                                    uint32_t* status, ss_stream_t stream) {
   Frames fr;
   int rc = frames_of_batch(batch, n, &fr);
   if (rc) return rc;
@@ -758,7 +769,8 @@ int ss_batch_project_rs_index_count(const ss_batch* batch, const float* means,
   if (!(dilation >= 0.0f)) return fail(SS_ERR_INVALID_ARGUMENT, "dilation must be >= 0");
   const RSField f{means, log_scales, rotations, colors, opacity_logits, dilation, sigma_cutoff};
   return index_count(fr, batch->tile_size, batch->tiles, records, n, ellipse_cull, sigma_cutoff,
-                     tile_offsets, workspace, workspace_bytes, status, stream, &f);
+                     tile_offsets, workspace, workspace_bytes, status, stream, &f, clear,
+                     clear_bytes);
 }
 
 int ss_tile_index_fill(const void* records, int64_t n, int height, int width, int tile_size,

@@ -69,12 +69,13 @@ class RenderPlan:
         self.bwd_ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", n,
                                                self.capacity, self.H, self.W,
                                                int(self.deterministic))
-        # the backward workspace and the status word share one allocation, so a fast-mode step
-        # clears its moments and its status with one fill (clear_step)
+        # the backward workspace and the status word share one allocation, which the step's
+        # projection kernel clears (the moments in fast mode, the status word always)
         ws_len = (max(self.bwd_ws_bytes, 16) + 255) // 256 * 256
         self._step_block = torch.zeros(ws_len + 256, device=d, dtype=torch.uint8)
         self.bwd_ws = self._step_block[:ws_len]
-        self.status = self._step_block[ws_len:ws_len + 4].view(torch.int32)
+        self._status_slot = self._step_block[ws_len:]
+        self.status = self._status_slot[:4].view(torch.int32)
         self.image = torch.zeros(self.H, self.W, 3, **f32)
         self.den = torch.zeros(self.H, self.W, **f32)
         self.g_means = torch.zeros(n, 2, **f32)
@@ -111,14 +112,17 @@ class RenderPlan:
                      self.tile_size, int(self.cull), float(self.sigma_cutoff), _p(self.offsets),
                      _p(self.idx_ws), self.idx_ws_bytes, _p(self.status), _stream())
 
-    def project_count(self, params):
-        """project() and count() in one kernel (ss_project_rs_index_count)."""
+    def project_count(self, params, clear_moments: bool = False):
+        """project() and count() in one kernel (ss_project_rs_index_count), which also zeroes
+        the status word and, with ``clear_moments`` in fast mode, the backward's moments."""
+        region = self._step_block if clear_moments and not self.deterministic else self._status_slot
         _native.call("ss_project_rs_index_count", _p(params["means"]), _p(params["log_scales"]),
                      _p(params["rotations"]), _p(params["colors"]),
                      _p(params.get("opacity_logits") if self.has_opacity else None), self.n,
                      float(self.dilation), float(self.sigma_cutoff), self.H, self.W,
                      self.tile_size, int(self.cull), _p(self.records), _p(self.offsets),
-                     _p(self.idx_ws), self.idx_ws_bytes, _p(self.status), _stream())
+                     _p(self.idx_ws), self.idx_ws_bytes, _p(region), region.numel(),
+                     _p(self.status), _stream())
 
     def fill(self):
         _native.call("ss_tile_index_fill", _p(self.records), self.n, self.H, self.W,
@@ -164,11 +168,10 @@ class RenderPlan:
                      float(self.eps), float(self.tail), int(self.deterministic), _p(self.bwd_ws),
                      self.bwd_ws_bytes, _p(self.status), _stream())
 
-    def forward(self, params, cleared: bool = False):
-        """Project, bin and render; ``cleared``: clear_step() already zeroed the status."""
-        if not cleared:
-            self.status.zero_()
-        self.project_count(params)
+    def forward(self, params, clear_moments: bool = False):
+        """Project, bin and render (the status word starts the step at zero; with
+        ``clear_moments`` the fast-mode moments too, for a backward that follows)."""
+        self.project_count(params, clear_moments)
         self.fill()
         self.render()
         return self.image
@@ -176,25 +179,17 @@ class RenderPlan:
     def use_fused(self) -> bool:
         return bool(self.fused)
 
-    def clear_step(self):
-        """Zero the status word and, in fast mode, the backward's moments (one fill)."""
-        if self.n and not self.deterministic:
-            self._step_block.zero_()
-        else:
-            self.status.zero_()
-
     def forward_backward(self, params, grad_out):
         """Image, den and the RS gradients for a grad_out known before the forward: project,
         bin, then one tile pass rendering and back-propagating each tile (or the forward and
         backward tile kernels one after the other), then the per-Gaussian RS pass."""
-        # the moments are cleared first so the step's kernels follow one another directly
-        # (each may start while its predecessor drains)
-        self.clear_step()
+        # the projection kernel clears the moments, so the step's kernels follow one another
+        # directly (each may start while its predecessor drains)
         if not self.use_fused():
-            self.forward(params, cleared=True)
+            self.forward(params, clear_moments=True)
             self.backward(grad_out, params, moments_zeroed=True)
             return self.grads()
-        self.project_count(params)
+        self.project_count(params, clear_moments=True)
         self.fill()
         self.tile_pass(grad_out)
         if self.n:

@@ -1,7 +1,8 @@
 """The fused projection + tile count (``ss_project_rs_index_count`` and its batch form) against
 ``ss_project_rs`` followed by ``ss_tile_index_count``: the records and the offsets are bitwise
 equal, with and without the ellipse cull, for tile sets on both sides of the count kernel's
-own scan (up to 4,095 tiles) and beyond it, for an empty field and for an empty image."""
+own scan (up to 4,095 tiles) and beyond it, for an empty field and for an empty image; the
+region the call is asked to clear is zeroed, and nothing past it."""
 from __future__ import annotations
 
 import pytest
@@ -54,8 +55,10 @@ def test_fused_project_count_matches_the_two_calls(H, W, ts, n, cull):
     _native.call("ss_tile_index_count", _p(r1), n, H, W, ts, cull, 3.0, _p(o1), _p(w1), wsb,
                  _p(s1), _stream())
     for _ in range(2):  # twice over the same workspace: the same offsets
+        clear = torch.full((4096,), 7, dtype=torch.uint8, device="cuda")
         _native.call("ss_project_rs_index_count", *_rs(p), n, 0.25, 3.0, H, W, ts, cull, _p(r2),
-                     _p(o2), _p(w2), wsb, _p(s2), _stream())
+                     _p(o2), _p(w2), wsb, _p(clear), 4096 - 16, _p(s2), _stream())
+        assert not clear[:4096 - 16].any() and bool((clear[4096 - 16:] == 7).all())
     torch.cuda.synchronize()
     assert torch.equal(r1[: n * RECORD_FLOATS].view(torch.int32),
                        r2[: n * RECORD_FLOATS].view(torch.int32))
@@ -77,7 +80,7 @@ def test_batch_fused_project_count_matches_the_two_calls():
     _native.call("ss_batch_tile_index_count", batch.ref, _p(r1), n, 1, 3.0, _p(o1), _p(w1), wsb,
                  _p(s1), _stream())
     _native.call("ss_batch_project_rs_index_count", batch.ref, *_rs(p), n, 0.0, 3.0, 1, _p(r2),
-                 _p(o2), _p(w2), wsb, _p(s2), _stream())
+                 _p(o2), _p(w2), wsb, None, 0, _p(s2), _stream())
     torch.cuda.synchronize()
     assert torch.equal(r1.view(torch.int32), r2.view(torch.int32))
     assert torch.equal(o1, o2)
