@@ -49,6 +49,9 @@ struct Tiling {
   static constexpr int kFwdThreads = 32 * kWarps;
   // backward whole-list stage: what fits in 48 KB of static shared memory beside the pixels
   static constexpr int kBwdStageAll = TS == 16 ? 512 : 448;
+  // resident forward CTAs the register budget must allow: three 512-thread render CTAs per SM
+  // (at most 42 registers a thread); the loss variants keep two
+  static constexpr int fwd_min_blocks(int loss) { return TS == 32 && loss == 0 ? 3 : 1; }
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -94,6 +97,10 @@ __device__ __forceinline__ int chunk_len(int64_t count, int64_t k0) {
 // (sx0, sy0); lane l also gets entry l's cover of the block: bit c (c < 8) for block column c
 // inside [x0, x1), bit 8 + k for block row k inside [y0, y1).  A rectangle touches the block
 // exactly when both halves of its cover are non-zero.
+constexpr int kFarRect = 48;          // rectangle side (px) above which blocks are tested
+constexpr float kUnderflowQ = 230.0f;  // q beyond which every weight is +0 (174.7 + 30%)
+
+template <bool FAR>
 __device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int sx0, int sy0,
                                               int lane, unsigned& cover) {
   cover = 0u;
@@ -104,6 +111,18 @@ __device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int 
     const unsigned xm = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
     const unsigned ym = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
     if (xm && ym) cover = xm | (ym << 8);
+    // FAR: a large rectangle (an elongated or wide Gaussian) may touch the block only where every
+    // weight underflows: exp(-q/2) < 2^-126, which ex2.approx.ftz returns as +0, when
+    // q > 174.7.  Such a block is skipped when the exact minimum of q over the covered pixels
+    // exceeds kUnderflowQ, a margin of 30% for the rounding of q in either evaluation; adding
+    // the zero weights would leave every sum bitwise unchanged.
+    if (FAR && cover && (b.z - b.x > kFarRect || b.w - b.y > kFarRect)) {
+      const float4 p0 = st[lane][0], p2 = st[lane][2];  // (mx, my, ·, ·), (·, a, b, c)
+      const float qmin = rect_min_q(p0.x, p0.y, p2.y, p2.z, p2.w, (float)(sx0 + x0),
+                                    (float)(sx0 + x1 - 1), (float)(sy0 + y0),
+                                    (float)(sy0 + y1 - 1));
+      if (qmin > kUnderflowQ) cover = 0u;
+    }
   }
   return __ballot_sync(0xffffffffu, cover != 0u);
 }
@@ -129,7 +148,7 @@ __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
 // Accumulates the staged entries [0, m) into one warp's two pixels per lane: lane l holds
 // block column l & 7 of block rows l >> 3 and (l >> 3) + 4; a pixel outside an entry's
 // rectangle (a clear bit of the entry's cover) adds a zero weight.
-template <bool FADE>
+template <bool FADE, bool FAR>
 __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int sx0, int sy0,
                                               int lane, int px, int py0, float fx, float fy0,
                                               float tail, float (&acc0)[4], float (&acc1)[4]) {
@@ -138,7 +157,7 @@ __device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int 
   const unsigned need1 = col | (1u << (12 + (lane >> 3)));
   for (int base = 0; base < m; base += 32) {
     unsigned cover;
-    unsigned hits = hit_cover(st + base, m - base, sx0, sy0, lane, cover);
+    unsigned hits = hit_cover<FAR>(st + base, m - base, sx0, sy0, lane, cover);
     while (hits) {
       const int src = __ffs(hits) - 1;
       hits &= hits - 1;
@@ -231,7 +250,7 @@ __device__ __forceinline__ float4 finish_pixel(const float* a, int64_t p, float 
 // pixel_grad = (dL/dnum_rgb, dL/dden) (out and den only when given) and adds each image's loss
 // and mean squared error into loss[2 b], loss[2 b + 1] (finish_pixel).
 template <int TS, bool NORMALIZE, bool FADE, int LOSS>
-__global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
+__global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, Tiling<TS>::fwd_min_blocks(LOSS))
     forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
                    int64_t cap, const int32_t* __restrict__ offsets, Frames frames, float eps,
                    float tail, float* __restrict__ out, float* __restrict__ den,
@@ -258,7 +277,8 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
     cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    forward_block<FADE>(stage, (int)L.count, sx0, sy0, lane, px, py0, fx, fy0, tail, acc0, acc1);
+    forward_block<FADE, false>(stage, (int)L.count, sx0, sy0, lane, px, py0, fx, fy0, tail, acc0,
+                               acc1);
   } else {
     float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
     const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
@@ -271,8 +291,8 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads)
       cp_async_commit();
       cp_async_wait_one();
       __syncthreads();
-      forward_block<FADE>(buf[c & 1], chunk_len(L.count, k0), sx0, sy0, lane, px, py0, fx, fy0,
-                          tail, acc0, acc1);
+      forward_block<FADE, true>(buf[c & 1], chunk_len(L.count, k0), sx0, sy0, lane, px, py0, fx,
+                                fy0, tail, acc0, acc1);
       __syncthreads();
     }
   }
@@ -609,7 +629,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
         if (b < kBlocks) {
           const int sx0 = tx0 + (b % (TS / 8)) * 8, sy0 = ty0 + (b / (TS / 8)) * 8;
           const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3);
-          forward_block<FADE>(st, m, sx0, sy0, lane, px, py0, (float)px, (float)py0, tail,
+          forward_block<FADE, false>(st, m, sx0, sy0, lane, px, py0, (float)px, (float)py0, tail,
                               acc[i][0], acc[i][1]);
         }
       }
