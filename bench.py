@@ -862,17 +862,15 @@ def main():
         if res["fused"]:
             roof = {"kernel": "backward_kernel (fused forward + backward tile pass)",
                     "achieved": fused_ach, "traffic": FUSED_DRAM_BYTES,
-                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one fused "
-                                      "tile pass launch, ncu --set full "
-                                      "(profiles/fused_tile_pass_1024x1024_100k.md)",
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                      "fused tile pass launch at this workload",
                     "work": f"{PAIR_SLOTS_FWD}+{PAIR_SLOTS_BWD} FP32 issue slots per "
                             f"in-rectangle pair x {P} pairs per launch"}
         else:
             roof = {"kernel": "backward_kernel", "achieved": bwd_ach,
                     "traffic": BACKWARD_DRAM_BYTES,
-                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                      "backward_kernel launch, ncu --set full "
-                                      "(profiles/backward_kernel_1024x1024_100k.md)",
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                      "backward_kernel launch at this workload",
                     "work": f"{PAIR_SLOTS_BWD} FP32 issue slots per in-rectangle pair x "
                             f"{P} pairs per launch"}
         t_bound_ms = P * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (peak_slots * 1e9) * 1e3

@@ -162,7 +162,9 @@ int ss_tile_index_fill(const void* records, int64_t n, int height, int width, in
  * n <= 65536 Gaussians and at most 16384 tiles (SS_ERR_CAPACITY beyond).  All calls share the
  * array: calls that overlap on the GPU race and must be serialised.  The first call on each
  * device resolves the array's address (cudaGetSymbolAddress) with that device current and
- * should come before any stream capture on it.  No counterpart in the reference. */
+ * should come before any stream capture on it.  That address is cached per device for the
+ * life of the process and does not survive cudaDeviceReset: do not call this entry point after
+ * resetting a device it has already run on.  No counterpart in the reference. */
 int ss_build_tile_index_static(const float* means, const float* conics, const int64_t* radii,
                                int64_t n, int height, int width, int tile_size,
                                int ellipse_cull, float sigma_cutoff, int32_t* tile_gids,

@@ -106,3 +106,40 @@ def backward_f64(grad_out, means, conics, colors, radii, H: int, W: int, opaciti
                          g["means"], g["conics"], g["colors"],
                          None if op is None else g["opacities"].ctypes.data)
     return g
+
+
+def rs_render_backward_f64(grad_out, means, log_scales, rotations, colors, opacity_logits, H: int,
+                           W: int, normalize=True, eps: float = 1e-8, tail: float = 0.0,
+                           sigma_cutoff: float = 3.0, dilation: float = 0.0):
+    """Float64 image, den and gradients of sum(image * grad_out) w.r.t. the RS field
+    (means, log_scales, rotations, colors, opacity_logits) — the reference's GaussianField path
+    (gaussians.py:270-321) into its renderer (render.py:180-235).
+
+    The renderer inputs are the float32 conics, radii and opacities the field produces
+    (``field_ref``, as the GPU path rounds them); the render and its gradients are evaluated in
+    float64 by the C restatement, and the chain rule back to the log-scales, rotations and
+    logits in float64 by torch autograd through ``field_ref.conics`` / the sigmoid.
+    """
+    import torch
+
+    from . import field_ref
+    ls32 = torch.as_tensor(_np(log_scales, np.float32))
+    rot32 = torch.as_tensor(_np(rotations, np.float32))
+    conics32 = field_ref.conics(ls32, rot32, dilation)
+    radii = field_ref.radii(ls32, rot32, sigma_cutoff, dilation)
+    op32 = None
+    if opacity_logits is not None:
+        op32 = torch.sigmoid(torch.as_tensor(_np(opacity_logits, np.float32)))
+    out, den = render_f64(means, conics32, colors, radii, H, W, op32, normalize, eps, tail)
+    g = backward_f64(grad_out, means, conics32, colors, radii, H, W, op32, normalize, eps, tail,
+                     den=den, out=out)
+    ls64 = torch.as_tensor(_np(log_scales, np.float64)).requires_grad_(True)
+    rot64 = torch.as_tensor(_np(rotations, np.float64)).requires_grad_(True)
+    c64 = field_ref.conics(ls64, rot64, dilation)
+    g_ls, g_rot = torch.autograd.grad(c64, (ls64, rot64), torch.as_tensor(g["conics"]))
+    grads = {"means": g["means"], "log_scales": g_ls.numpy(), "rotations": g_rot.numpy(),
+             "colors": g["colors"], "opacity_logits": None}
+    if opacity_logits is not None:
+        s = 1.0 / (1.0 + np.exp(-_np(opacity_logits, np.float64)))
+        grads["opacity_logits"] = g["opacities"] * s * (1.0 - s)
+    return out, den, grads

@@ -323,6 +323,28 @@ class FitPlan:
     def overflowed(self) -> bool:
         return bool(int(self.status.item()) & 1)
 
+    def gradients(self) -> dict:
+        """The parameter gradients the last ``update()`` fed to Adam, as views into the fit
+        workspace: means (N,2), log_scales (N,2), rotations (N,), colors (N,3) and
+        opacity_logits (N,) (None without opacities).  They sit at the end of the workspace in
+        five 256-byte-aligned arrays (``fit_grads_layout`` of the CUDA library)."""
+        n = self.n
+
+        def a256(x):
+            return (x + 255) // 256 * 256
+        sizes = [a256(8 * n), a256(8 * n), a256(4 * n), a256(12 * n), a256(4 * n)]
+        off = (self.bwd_ws_bytes - sum(sizes)) // 4
+        out = {}
+        for k, shape, sz in zip(PARAM_NAMES, [(n, 2), (n, 2), (n,), (n, 3), (n,)], sizes):
+            count = 1
+            for d in shape:
+                count *= d
+            out[k] = self.bwd_ws[off:off + count].view(shape)
+            off += sz // 4
+        if not self.has_opacity:
+            out["opacity_logits"] = None
+        return out
+
     def state(self):
         """Snapshot of the optimisation state (field, Adam moments, step)."""
         keep = {k: v.clone() for k, v in self.params.items() if v is not None}

@@ -559,7 +559,7 @@ int allow_big_sort_smem() {
 int check_index_args(int64_t n, int H, int W, int ts) {
   if (n < 0 || H < 0 || W < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
   if (n > (int64_t)INT32_MAX) return fail(SS_ERR_INVALID_ARGUMENT, "n exceeds int32 ids");
-  if (ts <= 0 || ts * ts > 1024)
+  if (ts <= 0 || ts > 32)  // ts^2 <= 1024, without overflow
     return fail(SS_ERR_INVALID_ARGUMENT, "tile_size must be positive with tile_size^2 <= 1024");
   TileGrid g = make_grid(H, W, ts);
   if (g.T + 1 > (int64_t)INT32_MAX)

@@ -73,13 +73,14 @@ int ss_build_tile_index_static(const float* means, const float* conics, const in
                                int64_t gid_capacity, int32_t* tile_offsets, uint32_t* status,
                                ss_stream_t stream) {
   if (n < 0 || height < 0 || width < 0) return fail(SS_ERR_INVALID_ARGUMENT, "negative size");
-  if (tile_size <= 0 || tile_size * tile_size > 1024)
+  if (tile_size <= 0 || tile_size > 32)  // tile_size^2 <= 1024, without overflow
     return fail(SS_ERR_INVALID_ARGUMENT, "tile_size must be positive with tile_size^2 <= 1024");
   if (n > kStaticMaxGaussians)
     return fail(SS_ERR_CAPACITY, "static tile index takes at most %lld Gaussians, got %lld",
                 (long long)kStaticMaxGaussians, (long long)n);
-  const int64_t tiles = (int64_t)((width + tile_size - 1) / tile_size) *
-                        ((height + tile_size - 1) / tile_size);
+  // in int64: width or height near INT_MAX must not overflow before the limit check
+  const int64_t tiles = (((int64_t)width + tile_size - 1) / tile_size) *
+                        (((int64_t)height + tile_size - 1) / tile_size);
   if (tiles > kStaticMaxTiles)
     return fail(SS_ERR_CAPACITY, "static tile index takes at most %lld tiles, got %lld",
                 (long long)kStaticMaxTiles, (long long)tiles);

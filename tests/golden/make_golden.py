@@ -103,6 +103,23 @@ def render_case(ref, name, g, H, W, *, normalize, use_opacity, dilation, fade_al
     return out
 
 
+def streamed_cases(ref):
+    """A 96×96 cut of the heavy-tailed stress field (σ = exp(N(ln 2, 1.2)), 30 % elongated with
+    aspect U[5, 50]) with 3,500 Gaussians: every 16- and 32-px tile list holds 531–1,411
+    Gaussians, more than the CUDA kernels stage at once, and 911 rectangles are wider than
+    48 px — the fixture that takes the streamed kernel paths to the reference's own result."""
+    from structsplat_b200.synthetic import make_stress_field
+    H = W = 96
+    angle = np.random.default_rng(8).uniform(0, np.pi, (H, W)).astype(np.float32)
+    f = make_stress_field(H, W, 3500, seed=9, along_edge_angle=angle)
+    g = ref.gaussians.GaussianField.from_numpy(f.means, np.exp(f.log_scales), f.rotations,
+                                               f.colors, opacities=f.opacity_logits)
+    render_case(ref, "streamed_96_3500", g, H, W, normalize=True, use_opacity=True,
+                dilation=0.0, fade_alpha=0.0, seed=60)
+    render_case(ref, "streamed_96_3500_additive", g, H, W, normalize=False, use_opacity=True,
+                dilation=0.0, fade_alpha=0.0, seed=61)
+
+
 def tile_case(ref, name, means, radii, H, W, ts):
     import torch
     m = torch.as_tensor(np.asarray(means, np.float32))
@@ -286,8 +303,10 @@ def ssim_cases(ref, make_target):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-src", default="/root/reference/src")
-    ap.add_argument("--only", choices=["placement", "passes", "fit", "codec", "ssim"],
+    ap.add_argument("--reference-src", required=True,
+                    help="the reference project's src directory (holding structsplat/)")
+    ap.add_argument("--only", choices=["placement", "passes", "fit", "codec", "ssim",
+                                       "streamed"],
                     default=None,
                     help="regenerate one group of fixtures, leaving the others untouched")
     args = ap.parse_args()
@@ -320,6 +339,12 @@ def main() -> None:
         structure_tensor = structsplat.structure_tensor
 
     torch.manual_seed(0)
+    if args.only == "streamed":
+        for old in HERE.glob("render_streamed_*.npz"):
+            old.unlink()
+        streamed_cases(Ref)
+        print("wrote", len(list(HERE.glob("render_streamed_*.npz"))), "streamed render fixtures")
+        return
     if args.only == "ssim":
         for old in HERE.glob("ssim_*.npz"):
             old.unlink()
@@ -412,6 +437,7 @@ def main() -> None:
                                                np.full((3, 2), 1.5), np.zeros(3), np.ones((3, 3)))
     render_case(Ref, "far_away", g, 12, 12, normalize=True, use_opacity=False, dilation=0.0,
                 fade_alpha=0.0, seed=57)
+    streamed_cases(Ref)
 
     # --- structure tensor ------------------------------------------------------------
     edge = np.zeros((64, 64, 3), np.float32)

@@ -1,0 +1,194 @@
+"""Parity at the benchmark configurations and on every streamed path of the tile kernels.
+
+The golden fixtures are small (≤ 64×64, ≤ 97 Gaussians per tile), so they never reach the
+kernels' streamed paths.  This file checks, against the float64 C oracle (and the reference's
+own CUDA extension where it is built):
+
+* the 1024² / 100k-Gaussian field the benchmark times (seed 0, normalized and additive):
+  binning bit-exact against the oracle's index (16- and 32-px tiles), the captured render step's
+  image and RS-field gradients (fast and deterministic, two-kernel and fused), and one fused fit
+  iteration's loss and parameter gradients;
+* a 256² heavy-tailed stress field (σ = exp(N(ln 2, 1.2)), 30 % elongated with aspect U[5, 50]):
+  every tile list is longer than the forward's 512-record stage and the backward's 448-entry
+  stage (766–1,481 entries at 32-px tiles, 433–1,080 at 16), and thousands of rectangles are
+  wider than 48 px, so the double-buffered chunk streams of the forward, the backward and the
+  fused passes and the forward's underflow block skip all run; render step and fit pass, fast
+  and deterministic.
+
+Bars: images within 1e-5 and gradients within 1e-4 (norm-wise relative, max |Δ| / max |ref|)
+of float64; each error is printed.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_helpers import rel_err, require_cuda
+from oracle import c_oracle, field_ref
+from structsplat_b200.batch import Batch, FitPlan, FitSettings
+from structsplat_b200.fit import PARAM_NAMES, CapturedStep, RenderPlan
+from structsplat_b200.synthetic import make_field, make_stress_field, make_target
+
+pytestmark = pytest.mark.gpu
+
+FWD_TOL, GRAD_TOL = 1e-5, 1e-4
+_CACHE = {}
+
+
+def _benchmark_case():
+    """The benchmark's field and grad_out (1024² / 100k Gaussians, seed 0; grad_out = target −
+    0.5 of the seed-1 target), as the benchmark builds them."""
+    if "c2" not in _CACHE:
+        H = W = 1024
+        f = make_field(H, W, 100_000, seed=0)
+        target = make_target(H, W, seed=1)
+        _CACHE["c2"] = (H, W, f, target, target - np.float32(0.5))
+    return _CACHE["c2"]
+
+
+def _stress_case():
+    """256² cut of the stress workload (the per-pixel angle map stands in for the structure
+    tensor's orientation; the kernels only see the resulting elongated rectangles)."""
+    if "c3" not in _CACHE:
+        H = W = 256
+        angle = np.random.default_rng(3).uniform(0, np.pi, (H, W)).astype(np.float32)
+        f = make_stress_field(H, W, 15_000, seed=4, along_edge_angle=angle)
+        target = make_target(H, W, seed=5)
+        g = np.random.default_rng(6).normal(0, 1, (H, W, 3)).astype(np.float32)
+        _CACHE["c3"] = (H, W, f, target, g)
+    return _CACHE["c3"]
+
+
+def _params(f):
+    return {k: torch.tensor(getattr(f, k), device="cuda") for k in PARAM_NAMES}
+
+
+def _oracle(case, normalize, grad_out=None):
+    H, W, f, _, g = case
+    key = (id(case), normalize, None if grad_out is None else hash(grad_out.tobytes()))
+    if key not in _CACHE:
+        _CACHE[key] = c_oracle.rs_render_backward_f64(
+            g if grad_out is None else grad_out, f.means, f.log_scales, f.rotations, f.colors,
+            f.opacity_logits, H, W, normalize)
+    return _CACHE[key]
+
+
+def _check(name, image, grads, oracle):
+    out64, _, g64 = oracle
+    e_img = rel_err(image, out64)
+    print(f"{name}: image err vs f64 {e_img:.2e}")
+    assert e_img <= FWD_TOL, name
+    for k in PARAM_NAMES:
+        e = rel_err(grads[k], g64[k])
+        print(f"  {k}: grad err vs f64 {e:.2e}")
+        assert e <= GRAD_TOL, (name, k, e)
+
+
+@pytest.mark.parametrize("tile_size", [16, 32])
+def test_benchmark_field_binning_bit_exact(tile_size):
+    require_cuda()
+    H, W, f, _, _ = _benchmark_case()
+    params = _params(f)
+    plan = RenderPlan.for_field(params, H, W, tile_size=tile_size)
+    plan.project_count(params)
+    plan.fill()
+    torch.cuda.synchronize()
+    radii = field_ref.radii(torch.tensor(f.log_scales), torch.tensor(f.rotations), 3.0)
+    ref_g, ref_o = c_oracle.tile_index(f.means, radii, H, W, tile_size)
+    offsets = plan.offsets.cpu().numpy().astype(np.int64)
+    assert not plan.overflowed()
+    assert np.array_equal(offsets, ref_o)
+    assert np.array_equal(plan.gids[: offsets[-1]].cpu().numpy().astype(np.int64), ref_g)
+    print(f"tile {tile_size}: {offsets[-1]} entries, longest list {np.diff(offsets).max()}")
+
+
+def _render_step(case, normalize, deterministic, fused, tile_size, captured=False):
+    H, W, f, _, g = case
+    params = _params(f)
+    grad_out = torch.tensor(g, device="cuda")
+    plan = RenderPlan.for_field(params, H, W, normalize=normalize, deterministic=deterministic,
+                                fused=fused, tile_size=tile_size)
+    if captured:
+        step = CapturedStep(lambda: plan.forward_backward(params, grad_out))
+        step.replay()
+    else:
+        plan.forward_backward(params, grad_out)
+    torch.cuda.synchronize()
+    assert int(plan.status.item()) == 0
+    return plan.image.clone(), {k: v.clone() for k, v in plan.grads().items()}
+
+
+@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("deterministic", [False, True])
+@pytest.mark.parametrize("normalize", [True, False])
+def test_benchmark_field_render_step_matches_float64(normalize, deterministic, fused):
+    """The benchmark's captured step (RS projection, binning, forward, backward, RS chain rule)
+    on the benchmark field, against float64."""
+    require_cuda()
+    case = _benchmark_case()
+    image, grads = _render_step(case, normalize, deterministic, fused, 32, captured=True)
+    _check(f"1024x1024/100k normalize={normalize} det={deterministic} fused={fused}", image,
+           grads, _oracle(case, normalize))
+    if deterministic:  # the captured graph and the eager calls give the same bits
+        image2, grads2 = _render_step(case, normalize, True, fused, 32)
+        assert torch.equal(image, image2)
+        for k in grads:
+            assert torch.equal(grads[k], grads2[k]), k
+
+
+@pytest.mark.parametrize("tile_size", [16, 32])
+@pytest.mark.parametrize("fused", [False, True])
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_stress_field_render_step_matches_float64(deterministic, fused, tile_size):
+    require_cuda()
+    case = _stress_case()
+    H, W, f, _, _ = case
+    radii = field_ref.radii(torch.tensor(f.log_scales), torch.tensor(f.rotations), 3.0)
+    _, offs = c_oracle.tile_index(f.means, radii, H, W, tile_size)
+    assert np.diff(offs).min() > 448 and np.diff(offs).max() > 512  # every list is streamed
+    assert int(((2 * radii + 1).max(1).values > 48).sum()) > 1000
+    image, grads = _render_step(case, True, deterministic, fused, tile_size)
+    _check(f"stress 256x256/15k det={deterministic} fused={fused} ts={tile_size}", image, grads,
+           _oracle(case, True))
+
+
+def _fit_once(case, deterministic, fused, tile_size=32):
+    """One fit iteration (l2 loss) on a one-image batch; returns (mse, the gradients the Adam
+    step consumed).  The field tensors are fresh copies (the step updates them in place)."""
+    H, W, f, target, _ = case
+    params = _params(f)
+    batch = Batch([(H, W)], [f.n], tile_size=tile_size)
+    s = FitSettings(pixel_loss="l2", deterministic=deterministic, fused=fused)
+    plan = FitPlan(batch, params, torch.tensor(target, device="cuda").reshape(-1, 3), s)
+    plan.step()
+    torch.cuda.synchronize()
+    assert not plan.overflowed()
+    return float(plan.loss[0, 1]), {k: v.clone() for k, v in plan.gradients().items()}
+
+
+@pytest.mark.parametrize("case_name", ["benchmark", "stress"])
+@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("deterministic", [False, True])
+def test_fit_iteration_gradients_match_float64(case_name, deterministic, fused):
+    """The fit pass (fused: ss_fit_forward_backward; or ss_fit_forward_loss + ss_fit_backward)
+    and the update's gradient pass, against float64: the MSE of the pre-update render and the
+    gradients of mean((image − target)²) w.r.t. the RS field."""
+    require_cuda()
+    if case_name == "benchmark" and deterministic:
+        pytest.skip("the benchmark field's deterministic fit is covered by the render step")
+    case = _benchmark_case() if case_name == "benchmark" else _stress_case()
+    H, W, f, target, _ = case
+    mse, grads = _fit_once(case, deterministic, fused)
+    out64, _, _ = _oracle(case, True)
+    resid = out64 - target.astype(np.float64)
+    mse64 = float((resid ** 2).mean())
+    gout = (2.0 * resid / (3.0 * H * W)).astype(np.float64)
+    oracle = _oracle(case, True, grad_out=gout)
+    e_mse = abs(mse - mse64) / mse64
+    print(f"fit {case_name} det={deterministic} fused={fused}: mse err vs f64 {e_mse:.2e}")
+    assert e_mse <= FWD_TOL
+    for k in PARAM_NAMES:
+        e = rel_err(grads[k], oracle[2][k])
+        print(f"  {k}: grad err vs f64 {e:.2e}")
+        assert e <= GRAD_TOL, (k, e)

@@ -17,15 +17,13 @@ import pytest
 import torch
 
 from conftest import golden, golden_names
-from gpu_helpers import cuda, rel_err, require_cuda
+from gpu_helpers import GRAD_TOL, cuda, fwd_ok, grad_ok, rel_err, require_cuda
 from structsplat_b200 import render_b200, render_gaussians
 from structsplat_b200 import render as R
 
 pytestmark = pytest.mark.gpu
 
 RENDER_CASES = golden_names("render_")
-FWD_TOL = 1e-5
-GRAD_TOL = 1e-4
 
 
 def _case(z):
@@ -51,20 +49,11 @@ def _render(z, deterministic=False, want_grads=True):
 
 
 def _grad_ok(got, z, key, prefix="g"):
-    e32 = rel_err(got, z[f"{prefix}_{key}_f32"])
-    e64 = rel_err(got, z[f"{prefix}_{key}_f64"])
-    ref_err = rel_err(z[f"{prefix}_{key}_f32"], z[f"{prefix}_{key}_f64"])
-    if ref_err <= GRAD_TOL / 10:
-        return e32 <= GRAD_TOL, (e32, e64, ref_err)
-    return e64 <= max(GRAD_TOL, 2 * ref_err), (e32, e64, ref_err)
+    return grad_ok(got, z[f"{prefix}_{key}_f32"], z[f"{prefix}_{key}_f64"])
 
 
 def _fwd_error_ok(img, z):
-    """Forward bar; faded cases use an element-wise bar floored at 1e-3 of the image scale."""
-    e32 = rel_err(img, z["image_f32"])
-    if float(z["fade_alpha"]) > 0:
-        return e32 <= 5e-5
-    return e32 <= FWD_TOL
+    return fwd_ok(img, z["image_f32"], float(z["fade_alpha"]) > 0)
 
 
 @pytest.mark.parametrize("name", RENDER_CASES)

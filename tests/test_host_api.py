@@ -115,3 +115,26 @@ def test_codec_header_rejects_non_containers():
     from conftest import golden
     h = codec.blob_header(golden("codec_default_opacity.npz")["blob"].tobytes())
     assert h["n"] == 400 and h["H"] == 48 and h["W"] == 64 and h["has_opacity"]
+
+
+def test_reference_extension_shim_mirrors_the_extension_checks():
+    """The shim installed as the reference's _EXT raises the reference extension's RuntimeError
+    messages (render_ext.cpp:94-137) before anything reaches the GPU."""
+    from structsplat_b200.reference_ext import Extension
+    ext = Extension()
+    m, c, col, r = _cpu_field()
+    op = torch.empty(0)
+    gids = torch.zeros(1, dtype=torch.int32)
+    offs = torch.zeros(2, dtype=torch.int32)
+    with pytest.raises(RuntimeError, match="means must be a CUDA tensor"):
+        ext.forward_tiled(m, c, col, r, op, gids, offs, 10, 10, True, 1e-8, 16, False, 3.0)
+    with pytest.raises(RuntimeError, match="means must be a CUDA tensor"):
+        ext.forward(m, c, col, r, op, 10, 10, True, 1e-8, False, 3.0)
+    with pytest.raises(RuntimeError, match="must be CUDA tensors"):
+        ext.build_tile_index(m, c, r, 10, 10, 16, False, 3.0)
+    with pytest.raises(RuntimeError, match="means must be a CUDA tensor"):
+        ext.backward(torch.zeros(10, 10, 3), m, c, col, r.int(), op, torch.zeros(10, 10),
+                     torch.zeros(10, 10, 3), True, 1e-8, False, 3.0)
+    for name in ("build_tile_index", "forward", "forward_tiled", "backward",
+                 "backward_block_reduce", "backward_tiled"):
+        assert callable(getattr(ext, name)), name

@@ -42,10 +42,13 @@ def test_torch_oracle_reproduces_reference_render(name):
         m, c, col, r, int(z["H"]), int(z["W"]), torch.tensor(z["grad_out"]), op,
         bool(z["normalize"]), float(z["eps"]), float(z["sigma_cutoff"]), float(z["fade_alpha"]))
     assert _rel(img, z["image_f32"]) <= 1e-6
+    # float32 sums of ~1,000 terms per pixel (the streamed cases) depend on the summation order,
+    # which the oracle's single pass and the reference's chunked index_add do not share
+    gtol = 1e-5 if "streamed" in name else 2e-6
     for key in ("means", "conics", "colors"):
-        assert _rel(g[key], z[f"g_{key}_f32"]) <= 2e-6, key
+        assert _rel(g[key], z[f"g_{key}_f32"]) <= gtol, key
     if op is not None:
-        assert _rel(g["opacities"], z["g_opacities_f32"]) <= 2e-6
+        assert _rel(g["opacities"], z["g_opacities_f32"]) <= gtol
 
 
 @pytest.mark.parametrize("name", RENDER_CASES)
