@@ -146,7 +146,10 @@ def test_stress_field_render_step_matches_float64(deterministic, fused, tile_siz
     H, W, f, _, _ = case
     radii = field_ref.radii(torch.tensor(f.log_scales), torch.tensor(f.rotations), 3.0)
     _, offs = c_oracle.tile_index(f.means, radii, H, W, tile_size)
-    assert np.diff(offs).min() > 448 and np.diff(offs).max() > 512  # every list is streamed
+    # the lists are longer than the whole-list stages (512 records forward; 448 / 512 entries
+    # backward at 32- / 16-px tiles), so the streamed paths run on (nearly) every tile
+    lens = np.diff(offs)
+    assert (lens > 512).mean() >= (0.9 if tile_size == 32 else 0.6)
     assert int(((2 * radii + 1).max(1).values > 48).sum()) > 1000
     image, grads = _render_step(case, True, deterministic, fused, tile_size)
     _check(f"stress 256x256/15k det={deterministic} fused={fused} ts={tile_size}", image, grads,
