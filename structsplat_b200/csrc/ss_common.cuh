@@ -70,6 +70,21 @@ int launch(const char* what, void (*kern)(KArgs...), dim3 grid, dim3 block, size
   return SS_OK;
 }
 
+// Lets `kern` take `bytes` of dynamic shared memory (beyond the 48 KB default; the largest
+// size a kernel is launched with, set once per kernel and device).
+int allow_dynamic_smem(const void* kern, size_t bytes);
+
+// launch() of a kernel whose shared memory is dynamic: `smem` bytes, opted in first.
+template <typename... KArgs, typename... Args>
+int launch_smem(const char* what, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                cudaStream_t s, Args... args) {
+  if (smem > 48 * 1024) {
+    const int rc = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
+    if (rc) return rc;
+  }
+  return launch(what, kern, grid, block, smem, s, args...);
+}
+
 // 2^x on the SFU (PTX ex2.approx.ftz.f32: one MUFU operation, documented max relative error
 // 2^-22; results below 2^-126 flush to zero, which for a weight is an absolute error < 1.2e-38).
 __device__ __forceinline__ float fast_exp2(float x) {

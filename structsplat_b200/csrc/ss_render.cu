@@ -40,18 +40,14 @@
 namespace ss {
 namespace {
 
-constexpr int kChunk = 64;          // Gaussians per shared-memory stage (4 x 16 B each)
 constexpr int kEpilogueThreads = 256;
 
 template <int TS>
 struct Tiling {
-  static constexpr int kWarps = (TS / 8) * (TS / 8);  // forward: one 8x8 block per warp
-  static constexpr int kFwdThreads = 32 * kWarps;
+  // forward: one warp per 8x8 block of the tile
+  static constexpr int kFwdThreads = 32 * (TS / 8) * (TS / 8);
   // backward whole-list stage: what fits in 48 KB of static shared memory beside the pixels
   static constexpr int kBwdStageAll = TS == 16 ? 512 : 448;
-  // resident forward CTAs the register budget must allow: three 512-thread render CTAs per SM
-  // (at most 42 registers a thread); the loss variants keep two
-  static constexpr int fwd_min_blocks(int loss) { return TS == 32 && loss == 0 ? 3 : 1; }
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -88,47 +84,47 @@ __device__ __forceinline__ TileList tile_list(const int32_t* gids, const int32_t
   return L;
 }
 
-__device__ __forceinline__ int chunk_len(int64_t count, int64_t k0) {
-  const int64_t r = count - k0;
-  return r < kChunk ? (int)r : kChunk;
-}
-
-// Ballot of the staged entries [0, min(m, 32)) whose support rectangle touches the 8x8 block at
-// (sx0, sy0); lane l also gets entry l's cover of the block: bit c (c < 8) for block column c
-// inside [x0, x1), bit 8 + k for block row k inside [y0, y1).  A rectangle touches the block
-// exactly when both halves of its cover are non-zero.
 constexpr int kFarRect = 48;          // rectangle side (px) above which blocks are tested
 constexpr float kUnderflowQ = 230.0f;  // q beyond which every weight is +0 (174.7 + 30%)
 
-template <bool FAR>
+// Cover of the 8x8 block at (sx0, sy0) by staged record j (rectangle b): bit c (c < 8) for block
+// column c inside [x0, x1), bit 8 + k for block row k inside [y0, y1); 0 when the rectangle
+// misses the block.  A large rectangle (an elongated or wide Gaussian) may touch the block only
+// where every weight underflows: exp(-q/2) < 2^-126, which ex2.approx.ftz returns as +0, when
+// q > 174.7.  Such a block is not covered when the exact minimum of q over the covered pixels
+// exceeds kUnderflowQ, a margin of 30% for the rounding of q in either evaluation; adding the
+// zero weights would leave every sum unchanged.
+__device__ __forceinline__ unsigned block_cover(const float4 (*st)[4], int j, const int4& b,
+                                                int sx0, int sy0) {
+  const int x0 = min(max(b.x - sx0, 0), 8), x1 = min(max(b.z - sx0, 0), 8);
+  const int y0 = min(max(b.y - sy0, 0), 8), y1 = min(max(b.w - sy0, 0), 8);
+  const unsigned xm = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
+  const unsigned ym = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
+  if (!xm || !ym) return 0u;
+  if (b.z - b.x > kFarRect || b.w - b.y > kFarRect) {
+    const float4 p0 = st[j][0], p2 = st[j][2];  // (mx, my, ·, ·), (·, a, b, c)
+    const float qmin = rect_min_q(p0.x, p0.y, p2.y, p2.z, p2.w, (float)(sx0 + x0),
+                                  (float)(sx0 + x1 - 1), (float)(sy0 + y0),
+                                  (float)(sy0 + y1 - 1));
+    if (qmin > kUnderflowQ) return 0u;
+  }
+  return xm | (ym << 8);
+}
+
+// Ballot of the staged entries [0, min(m, 32)) covering the block at (sx0, sy0); lane l also
+// gets entry l's cover.
 __device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int sx0, int sy0,
                                               int lane, unsigned& cover) {
   cover = 0u;
   if (lane < m) {
     const int4 b = *reinterpret_cast<const int4*>(&st[lane][3]);
-    const int x0 = min(max(b.x - sx0, 0), 8), x1 = min(max(b.z - sx0, 0), 8);
-    const int y0 = min(max(b.y - sy0, 0), 8), y1 = min(max(b.w - sy0, 0), 8);
-    const unsigned xm = ((1u << x1) - 1u) & ~((1u << x0) - 1u);
-    const unsigned ym = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
-    if (xm && ym) cover = xm | (ym << 8);
-    // FAR: a large rectangle (an elongated or wide Gaussian) may touch the block only where every
-    // weight underflows: exp(-q/2) < 2^-126, which ex2.approx.ftz returns as +0, when
-    // q > 174.7.  Such a block is skipped when the exact minimum of q over the covered pixels
-    // exceeds kUnderflowQ, a margin of 30% for the rounding of q in either evaluation; adding
-    // the zero weights would leave every sum bitwise unchanged.
-    if (FAR && cover && (b.z - b.x > kFarRect || b.w - b.y > kFarRect)) {
-      const float4 p0 = st[lane][0], p2 = st[lane][2];  // (mx, my, ·, ·), (·, a, b, c)
-      const float qmin = rect_min_q(p0.x, p0.y, p2.y, p2.z, p2.w, (float)(sx0 + x0),
-                                    (float)(sx0 + x1 - 1), (float)(sy0 + y0),
-                                    (float)(sy0 + y1 - 1));
-      if (qmin > kUnderflowQ) cover = 0u;
-    }
+    cover = block_cover(st, lane, b, sx0, sy0);
   }
   return __ballot_sync(0xffffffffu, cover != 0u);
 }
 
 // Lists up to kStageAll Gaussians are staged whole (one barrier per tile; the warps then run
-// independently); longer lists stream through a double buffer of two kChunk-entry stages.
+// independently); longer lists stream through the two halves of the stage, double-buffered.
 constexpr int kStageAll = 512;
 
 // Issues the copies of entries [k0, k0+m) into `dst` with NT threads: 16-byte piece (q & 3) of
@@ -145,45 +141,184 @@ __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
   }
 }
 
-// Accumulates the staged entries [0, m) into one warp's two pixels per lane: lane l holds
-// block column l & 7 of block rows l >> 3 and (l >> 3) + 4; a pixel outside an entry's
-// rectangle (a clear bit of the entry's cover) adds a zero weight.
-template <bool FADE, bool FAR>
-__device__ __forceinline__ void forward_block(const float4 (*st)[4], int m, int sx0, int sy0,
-                                              int lane, int px, int py0, float fx, float fy0,
-                                              float tail, float (&acc0)[4], float (&acc1)[4]) {
-  const unsigned col = 1u << (lane & 7);
-  const unsigned need0 = col | (1u << (8 + (lane >> 3)));
-  const unsigned need1 = col | (1u << (12 + (lane >> 3)));
-  for (int base = 0; base < m; base += 32) {
-    unsigned cover;
-    unsigned hits = hit_cover<FAR>(st + base, m - base, sx0, sy0, lane, cover);
-    while (hits) {
-      const int src = __ffs(hits) - 1;
-      hits &= hits - 1;
-      const int j = base + src;
-      const unsigned cv = __shfl_sync(0xffffffffu, cover, src);
-      const float4 p0 = st[j][0], p1 = st[j][1];
-      const float cb = st[j][2].x;
-      const bool in0 = (cv & need0) == need0, in1 = (cv & need1) == need1;
-      const float dx = fx - p0.x, dy0 = fy0 - p0.y, dy1 = dy0 + 4.0f;
-      const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
-      const float raw0 = fast_exp2(fmaf(dy0, fmaf(p1.x, dy0, bdx), adx2));
-      const float raw1 = fast_exp2(fmaf(dy1, fmaf(p1.x, dy1, bdx), adx2));
-      const float vis0 = FADE ? fmaxf(raw0 - tail, 0.0f) : raw0;
-      const float vis1 = FADE ? fmaxf(raw1 - tail, 0.0f) : raw1;
-      const float w0 = in0 ? vis0 * p1.y : 0.0f;
-      const float w1 = in1 ? vis1 * p1.y : 0.0f;
-      acc0[0] = fmaf(w0, p1.z, acc0[0]);
-      acc0[1] = fmaf(w0, p1.w, acc0[1]);
-      acc0[2] = fmaf(w0, cb, acc0[2]);
-      acc0[3] += w0;
-      acc1[0] = fmaf(w1, p1.z, acc1[0]);
-      acc1[1] = fmaf(w1, p1.w, acc1[1]);
-      acc1[2] = fmaf(w1, cb, acc1[2]);
-      acc1[3] += w1;
+// ---------------------------------------------------------------------------------------------
+// Forward evaluation of one 8x8 pixel block by one warp, four Gaussians at a time.
+//
+// The block's hits (staged entries whose rectangle touches it and is not wholly underflowed, in
+// ascending list order) are listed per warp in shared memory; an entry is the staged slot
+// (bits 0-14) and its cover of the block (bits 16-23 block columns, 24-31 block rows).  The
+// lanes form four groups of eight: group g = lane >> 3 evaluates hit 4i + g, lane (c, g) the
+// eight pixels of block column c, so the setup of a Gaussian (record loads, dx terms) serves
+// eight pixels, and rows k and k + 4 share packed (f32x2) arithmetic.  Each lane keeps a
+// partial sum per pixel and channel; the k-th hit of a block always goes to partial k mod 4,
+// however its tile list was staged or chunked, and the partials are combined as
+// (p0 + p1) + (p2 + p3).  Every kernel that renders a tile (forward, fused render pass, fused
+// fit pass) evaluates its blocks this way, so their images agree bitwise.  A list is padded to
+// a multiple of four with the null record (opacity 0, no cover).
+constexpr int kQueueLen = 40;   // per-batch queue: ≥ 3 pending + 32 new hits + 3 padding
+constexpr int kCarrySlots = 4;  // per warp: staged slots for pending hits across a refill
+
+// Row offsets of the fast evaluation: kRowOff.v[rows][k] = (k, k + 4) for the rows of the
+// pair that the 8-bit row mask covers, and kRowMasked for the others.  Added to dy0, a masked
+// row's dy becomes so large that qc dy^2 overflows to -inf and its weight is exactly +0, so
+// the pair needs no per-pixel select.  Valid for regular records only (below).
+constexpr float kRowMasked = 1e30f;
+struct RowOffsets {
+  float2 v[256][4];
+};
+constexpr RowOffsets make_row_offsets() {
+  RowOffsets t{};
+  for (int m = 0; m < 256; ++m)
+    for (int k = 0; k < 4; ++k) {
+      t.v[m][k].x = ((m >> k) & 1) ? (float)k : kRowMasked;
+      t.v[m][k].y = ((m >> (k + 4)) & 1) ? (float)(k + 4) : kRowMasked;
     }
+  return t;
+}
+__device__ const RowOffsets kRowOff = make_row_offsets();
+
+// A record whose masked pixels the fast evaluation zeroes exactly: a positive-definite conic
+// (qa, qc < 0 with qb^2 < 4 qa qc, and qc not so small that dy = kRowMasked leaves q finite)
+// and a finite opacity and colour.  A tile staging any other record renders by select.
+__device__ __forceinline__ bool regular_record(const float4& p0, const float4& p1, float cb) {
+  return p0.z < 0.0f && p1.x < -1e-20f && p0.w * p0.w < 4.0f * p0.z * p1.x &&
+         fabsf(p1.y) + fabsf(p1.z) + fabsf(p1.w) + fabsf(cb) < 3.0e38f;
+}
+
+// Staged slots [0, m): true when every record is regular.  A CTA-wide barrier: every thread
+// of the CTA calls it.
+template <int NT>
+__device__ __forceinline__ bool all_regular(const float4 (*st)[4], int m) {
+  bool ok = true;
+  for (int t = threadIdx.x; t < m; t += NT) ok = ok && regular_record(st[t][0], st[t][1], st[t][2].x);
+  return __syncthreads_and(ok) != 0;
+}
+
+// The null record: zero opacity and colour, a unit conic, an empty rectangle.
+__device__ __forceinline__ void write_null_record(float4 (*st)[4], int slot) {
+  st[slot][0] = make_float4(0.f, 0.f, -1.f, 0.f);
+  st[slot][1] = make_float4(-1.f, 0.f, 0.f, 0.f);
+  st[slot][2] = make_float4(0.f, 0.f, 0.f, 0.f);
+  st[slot][3] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Hits q[0..4) of groups 0-3: lane (c, g) adds its eight pixels of hit q[g].  EXACT: masked
+// pixels by select (any record); otherwise by the row offsets (regular records).
+template <bool FADE, bool EXACT>
+__device__ __forceinline__ void eval4(const float4 (*st)[4], const uint32_t* q, int lane,
+                                      float fx, float fy0, float tail, float2 (&acc)[4][4]) {
+  const uint32_t e = q[lane >> 3];
+  const int j = (int)(e & 0x7fffu);
+  const uint32_t rows = (e & (1u << (16 + (lane & 7)))) ? (e >> 24) : 0u;
+  const float4 p0 = st[j][0], p1 = st[j][1];
+  const float cb = st[j][2].x;
+  const float dx = fx - p0.x, dy0 = fy0 - p0.y;
+  const float bdx = p0.w * dx, adx2 = p0.z * dx * dx;
+  const float2 bdx2 = make_float2(bdx, bdx), adx22 = make_float2(adx2, adx2);
+  const float2 qc2 = make_float2(p1.x, p1.x), op2 = make_float2(p1.y, p1.y);
+  const float2 dy02 = make_float2(dy0, dy0);
+  const float2 cr2 = make_float2(p1.z, p1.z), cg2 = make_float2(p1.w, p1.w);
+  const float2 cb2 = make_float2(cb, cb);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 off = EXACT ? make_float2((float)k, (float)(k + 4)) : kRowOff.v[rows][k];
+    const float2 dy = __fadd2_rn(dy02, off);
+    const float2 t = __ffma2_rn(qc2, dy, bdx2);
+    const float2 qq = __ffma2_rn(dy, t, adx22);
+    float2 v = make_float2(fast_exp2(qq.x), fast_exp2(qq.y));
+    if (FADE) v = make_float2(fmaxf(v.x - tail, 0.0f), fmaxf(v.y - tail, 0.0f));
+    float2 w = __fmul2_rn(v, op2);
+    if (EXACT) {
+      w.x = (rows & (1u << k)) ? w.x : 0.0f;
+      w.y = (rows & (1u << (k + 4))) ? w.y : 0.0f;
+    }
+    acc[k][0] = __ffma2_rn(w, cr2, acc[k][0]);
+    acc[k][1] = __ffma2_rn(w, cg2, acc[k][1]);
+    acc[k][2] = __ffma2_rn(w, cb2, acc[k][2]);
+    acc[k][3] = __fadd2_rn(acc[k][3], w);
   }
+}
+
+// Appends the hits among staged slots [slot0, slot0 + min(cnt, 32)) to the list q[0..qn).
+__device__ __forceinline__ int enqueue_hits(const float4 (*st)[4], int slot0, int cnt, int sx0,
+                                            int sy0, int lane, uint32_t* q, int qn) {
+  unsigned cover;
+  const unsigned hits = hit_cover(st + slot0, cnt, sx0, sy0, lane, cover);
+  if (cover) q[qn + __popc(hits & ((1u << lane) - 1u))] = (uint32_t)(slot0 + lane) | (cover << 16);
+  return qn + __popc(hits);
+}
+
+// Evaluates the listed hits four at a time.  `all`: the last partial group too, padded with the
+// null record (the list ends empty); otherwise the remainder (< 4) moves to the front.  Returns
+// the new length.  The list needs room for 3 entries of padding.
+template <bool FADE>
+__device__ __forceinline__ int drain(const float4 (*st)[4], uint32_t* q, int qn, bool all,
+                                     bool exact, int null_slot, int lane, float fx, float fy0,
+                                     float tail, float2 (&acc)[4][4]) {
+  if (all && (qn & 3)) {
+    if (lane < 4 && lane >= (qn & 3)) q[(qn & ~3) + lane] = (uint32_t)null_slot;
+    qn = (qn + 3) & ~3;
+  }
+  __syncwarp();
+  const int full = qn & ~3;
+  if (exact) {
+#pragma unroll 1
+    for (int i = 0; i < full; i += 4) eval4<FADE, true>(st, q + i, lane, fx, fy0, tail, acc);
+  } else {
+#pragma unroll 1
+    for (int i = 0; i < full; i += 4) eval4<FADE, false>(st, q + i, lane, fx, fy0, tail, acc);
+  }
+  const int r = qn - full;
+  if (r == 0) return 0;
+  const uint32_t keep = lane < r ? q[full + lane] : 0u;
+  __syncwarp();
+  if (lane < r) q[lane] = keep;
+  __syncwarp();
+  return r;
+}
+
+// Before a staged chunk is refilled: the records of the pending hits q[0..qn) (qn < 4) move to
+// the warp's carry slots carry0 + i (a hit already there stays), and the list points at them.
+__device__ __forceinline__ void carry_pending(float4 (*st)[4], uint32_t* q, int qn, int carry0,
+                                              int lane) {
+  if (lane < 3 * qn) {  // pieces 0-2 hold what the evaluation reads
+    const int i = lane / 3, piece = lane - 3 * i;
+    const int src = (int)(q[i] & 0x7fffu);
+    if (src != carry0 + i) st[carry0 + i][piece] = st[src][piece];
+  }
+  __syncwarp();
+  if (lane < qn) q[lane] = (q[lane] & 0xffff0000u) | (uint32_t)(carry0 + lane);
+  __syncwarp();
+}
+
+// The four group partials of a block combined as (p0 + p1) + (p2 + p3) by a two-level
+// reduce-scatter: lane (c, g) ends with block rows first_row(lane) and first_row(lane) + 1 of
+// column c.
+__device__ __forceinline__ int block_first_row(int lane) {
+  return ((lane & 8) ? 4 : 0) + ((lane & 16) ? 2 : 0);
+}
+__device__ __forceinline__ void combine_groups(const float2 (&acc)[4][4], int lane,
+                                               float (&v)[2][4]) {
+  // acc[r][ch].x is block row r, .y block row r + 4
+  float h[4][4];
+  const bool odd = lane & 8;
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const float send = odd ? acc[r][ch].x : acc[r][ch].y;
+      const float keep = odd ? acc[r][ch].y : acc[r][ch].x;
+      h[r][ch] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+  const bool hi = lane & 16;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+      const float send = hi ? h[r][ch] : h[r + 2][ch];
+      const float keep = hi ? h[r + 2][ch] : h[r][ch];
+      v[r][ch] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
 }
 
 // Pixel losses of fit.py:800-809 (mean over channels, then over the image's pixels).
@@ -206,9 +341,9 @@ __device__ __forceinline__ float4 finish_pixel(const float* a, int64_t p, float 
                                                float* den, const float* target, float& lp,
                                                float& sq) {
   float o[3];
-  const float denom = a[3] + eps;
+  const float denom = a[3] + eps, inv = 1.0f / denom;
 #pragma unroll
-  for (int ch = 0; ch < 3; ++ch) o[ch] = NORMALIZE ? a[ch] / denom : a[ch];
+  for (int ch = 0; ch < 3; ++ch) o[ch] = NORMALIZE ? a[ch] * inv : a[ch];
   if (LOSS == kNoLoss || den) den[p] = a[3];
   if (LOSS == kNoLoss || out) {
     out[3 * p] = o[0];
@@ -239,18 +374,100 @@ __device__ __forceinline__ float4 finish_pixel(const float* a, int64_t p, float 
     }
   }
   if (NORMALIZE)
-    return make_float4(g[0] / denom, g[1] / denom, g[2] / denom,
-                       -(g[0] * o[0] + g[1] * o[1] + g[2] * o[2]) / denom);
+    return make_float4(g[0] * inv, g[1] * inv, g[2] * inv,
+                       -(g[0] * o[0] + g[1] * o[1] + g[2] * o[2]) * inv);
   return make_float4(g[0], g[1], g[2], 0.f);
   }
 }
 
-// Forward of one tile.  LOSS == kNoLoss: writes out and den.  Otherwise (a fit iteration) it
-// also evaluates the pixel loss against target and writes the backward's per-pixel input
-// pixel_grad = (dL/dnum_rgb, dL/dden) (out and den only when given) and adds each image's loss
-// and mean squared error into loss[2 b], loss[2 b + 1] (finish_pixel).
+// Shared memory of the forward kernel (dynamic): the stage (whole lists up to kStageAll
+// records, or two halves of it for a streamed list) followed by every warp's carry slots and
+// the null record; every warp's hit list; and per warp an 8x8 tile of pixels (RGB rows, then
+// den) through which a block leaves as whole float4 image rows.  One warp per 8x8 block.
+template <int TS>
+struct FwdSmem {
+  static constexpr int kWarps = (TS / 8) * (TS / 8);
+  static constexpr int kNullSlot = kStageAll + kWarps * kCarrySlots;
+  static constexpr int kSlots = kNullSlot + 1;
+  static constexpr int kListLen = kStageAll + 4;  // a whole stage's hits and padding
+  static constexpr size_t kStageBytes = (size_t)kSlots * 4 * sizeof(float4);
+  static constexpr size_t kListBytes = (size_t)kWarps * kListLen * sizeof(uint32_t);
+  static constexpr size_t kTileBytes = (size_t)kWarps * 8 * 32 * sizeof(float);
+  static constexpr size_t kListOff = kStageBytes;
+  static constexpr size_t kTileOff = kListOff + kListBytes;
+  static constexpr size_t kBytes = kTileOff + kTileBytes;
+};
+
+// Accumulates one warp's 8x8 block over a tile's list, staged whole by the caller (who also
+// passed the barrier after it), or streamed here through two halves of the stage with the
+// pending hits carried across each refill (chunk 0 already in flight when `chunk0_issued`; the
+// stream ends with a barrier, after which the stage may be refilled).  `qcap` is the capacity
+// of the warp's list q: with room for a whole stage (or half) plus padding the hits are listed
+// first and evaluated in one run, otherwise batch by batch.  `exact`: the staged records were
+// checked (all_regular) and some is not regular.  Every thread of the CTA calls it: it holds
+// the CTA's barriers.
+template <int NT, bool FADE>
+__device__ __forceinline__ void accumulate_block(float4 (*stage)[4], int stage_slots,
+                                                 const Splat* __restrict__ rec,
+                                                 const TileList& L, uint32_t* q, int qcap,
+                                                 int carry0, int null_slot, bool active, int sx0,
+                                                 int sy0, int lane, float tail,
+                                                 float2 (&acc)[4][4], bool staged_whole,
+                                                 bool exact, bool chunk0_issued = false) {
+  const float fx = (float)(sx0 + (lane & 7)), fy0 = (float)sy0;
+  int qn = 0;
+  if (staged_whole) {  // the caller staged the list and passed the barrier
+    const int m = (int)L.count;
+    if (active) {
+      const bool listed = qcap >= m + 4;
+      for (int base = 0; base < m; base += 32) {
+        qn = enqueue_hits(stage, base, m - base, sx0, sy0, lane, q, qn);
+        if (!listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
+      }
+      drain<FADE>(stage, q, qn, true, exact, null_slot, lane, fx, fy0, tail, acc);
+    }
+    return;
+  }
+  const int half = stage_slots / 2;
+  const bool listed = qcap >= half + 8;
+  const int64_t count = L.count;
+  const int nchunks = (int)((count + half - 1) / half);
+  auto len = [&](int64_t k0) { return (int)(count - k0 < half ? count - k0 : half); };
+  if (!chunk0_issued) {
+    stage_range<NT>(stage, rec, L, 0, len(0));
+    cp_async_commit();
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    const int64_t k0 = (int64_t)c * half;
+    if (c + 1 < nchunks) stage_range<NT>(stage + ((c + 1) & 1) * half, rec, L, k0 + half,
+                                         len(k0 + half));
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    const int m = len(k0), s0 = (c & 1) * half;
+    exact = exact || !all_regular<NT>(stage + s0, m);
+    if (active) {
+      for (int base = 0; base < m; base += 32) {
+        qn = enqueue_hits(stage, s0 + base, m - base, sx0, sy0, lane, q, qn);
+        if (!listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
+      }
+      if (listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
+      if (c + 1 < nchunks) carry_pending(stage, q, qn, carry0, lane);
+    }
+    __syncthreads();
+  }
+  if (active) drain<FADE>(stage, q, qn, true, exact, null_slot, lane, fx, fy0, tail, acc);
+  __syncthreads();
+}
+
+// Forward of one tile, one warp per 8x8 block.  LOSS == kNoLoss: writes out and den.
+// Otherwise (a fit iteration) it also evaluates the pixel loss against target and writes the
+// backward's per-pixel input pixel_grad = (dL/dnum_rgb, dL/dden) (out and den only when given)
+// and adds each image's loss and mean squared error into loss[2 b], loss[2 b + 1]
+// (finish_pixel).  Each warp lists its block's hits (accumulate_block), per staged chunk when
+// the list streams.
 template <int TS, bool NORMALIZE, bool FADE, int LOSS>
-__global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, Tiling<TS>::fwd_min_blocks(LOSS))
+__global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
     forward_kernel(const Splat* __restrict__ rec, int64_t n, const int32_t* __restrict__ gids,
                    int64_t cap, const int32_t* __restrict__ offsets, Frames frames, float eps,
                    float tail, float* __restrict__ out, float* __restrict__ den,
@@ -258,8 +475,10 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, Tiling<TS>::fwd_min_b
                    float* __restrict__ loss, float charb_eps2) {
   pdl_wait();
   pdl_trigger();
+  using S = FwdSmem<TS>;
   constexpr int NT = Tiling<TS>::kFwdThreads;
-  __shared__ __align__(16) float4 stage[kStageAll][4];
+  extern __shared__ __align__(16) unsigned char fwd_smem[];
+  float4(*stage)[4] = reinterpret_cast<float4(*)[4]>(fwd_smem);
   const int tile = blockIdx.x;
   const Frame fr = frame_of_tile(frames, tile, n);
   const int local = tile - fr.first_tile;
@@ -267,48 +486,76 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, Tiling<TS>::fwd_min_b
   const int H = fr.H, W = fr.W;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sx0 = tx0 + (warp % (TS / 8)) * 8, sy0 = ty0 + (warp / (TS / 8)) * 8;
-  const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3), py1 = py0 + 4;
-  const float fx = (float)px, fy0 = (float)py0;
+  uint32_t* q = reinterpret_cast<uint32_t*>(fwd_smem + S::kListOff) + warp * S::kListLen;
   const TileList L = tile_list(gids, offsets, cap, fr, tile);
-
-  float acc0[4] = {0.f, 0.f, 0.f, 0.f}, acc1[4] = {0.f, 0.f, 0.f, 0.f};
-  if (L.count <= kStageAll) {
+  const bool whole = L.count <= kStageAll;
+  if (threadIdx.x == 0) write_null_record(stage, S::kNullSlot);
+  float2 acc[4][4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) acc[k][ch] = make_float2(0.f, 0.f);
+  bool exact = false;
+  if (whole) {
     stage_range<NT>(stage, rec, L, 0, (int)L.count);
     cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    forward_block<FADE, false>(stage, (int)L.count, sx0, sy0, lane, px, py0, fx, fy0, tail, acc0,
-                               acc1);
-  } else {
-    float4(*buf)[kChunk][4] = reinterpret_cast<float4(*)[kChunk][4]>(stage);
-    const int nchunks = (int)((L.count + kChunk - 1) / kChunk);
-    stage_range<NT>(buf[0], rec, L, 0, chunk_len(L.count, 0));
-    cp_async_commit();
-    for (int c = 0; c < nchunks; ++c) {
-      const int64_t k0 = (int64_t)c * kChunk;
-      if (c + 1 < nchunks)
-        stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kChunk, chunk_len(L.count, k0 + kChunk));
-      cp_async_commit();
-      cp_async_wait_one();
-      __syncthreads();
-      forward_block<FADE, true>(buf[c & 1], chunk_len(L.count, k0), sx0, sy0, lane, px, py0, fx,
-                                fy0, tail, acc0, acc1);
-      __syncthreads();
+    exact = !all_regular<NT>(stage, (int)L.count);
+  }
+  accumulate_block<NT, FADE>(stage, kStageAll, rec, L, q, S::kListLen,
+                             kStageAll + warp * kCarrySlots, S::kNullSlot, true, sx0, sy0, lane,
+                             tail, acc, whole, exact);
+  float v[2][4];
+  combine_groups(acc, lane, v);
+  const int cx = lane & 7, r0 = block_first_row(lane);
+  const int px = sx0 + cx;
+  if constexpr (LOSS == kNoLoss) {
+    // whole float4 rows when the block lies inside the image and its rows are 16-B aligned
+    const int64_t p_row0 = fr.pixel_base + (int64_t)sy0 * W + sx0;
+    const bool vec = sx0 + 8 <= W && sy0 + 8 <= H && (W & 3) == 0 && (p_row0 & 3) == 0 &&
+                     ((reinterpret_cast<uintptr_t>(out) | reinterpret_cast<uintptr_t>(den)) & 15) == 0;
+    if (vec) {
+      // the warp's 8 rows of 32 floats: 24 interleaved RGB, then 8 den
+      float* tb = reinterpret_cast<float*>(fwd_smem + S::kTileOff) + warp * 256;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const float inv = 1.0f / (v[k][3] + eps);
+        float* row = tb + (r0 + k) * 32;
+        row[3 * cx] = NORMALIZE ? v[k][0] * inv : v[k][0];
+        row[3 * cx + 1] = NORMALIZE ? v[k][1] * inv : v[k][1];
+        row[3 * cx + 2] = NORMALIZE ? v[k][2] * inv : v[k][2];
+        row[24 + cx] = v[k][3];
+      }
+      __syncwarp();
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {
+        const int idx = lane + 32 * it;  // 48 RGB float4s (8 rows x 6), then 16 den float4s
+        if (idx < 48) {
+          const int row = idx / 6, part = idx - 6 * row;
+          const float4 vv = reinterpret_cast<const float4*>(tb + row * 32)[part];
+          reinterpret_cast<float4*>(out + 3 * (p_row0 + (int64_t)row * W))[part] = vv;
+        } else {
+          const int d = idx - 48, row = d >> 1, part = d & 1;
+          const float4 vv = reinterpret_cast<const float4*>(tb + row * 32 + 24)[part];
+          reinterpret_cast<float4*>(den + p_row0 + (int64_t)row * W)[part] = vv;
+        }
+      }
+      return;
     }
   }
   float loss_sum = 0.f, sq_sum = 0.f;
   const float per_value = pixel_loss_scale(H, W);
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
-    const int py = k ? py1 : py0;
-    const float* a = k ? acc1 : acc0;
+    const int py = sy0 + r0 + k;
     if (px < W && py < H) {
       const int64_t p = fr.pixel_base + (int64_t)py * W + px;
       float lp, sq;
-      const float4 v = finish_pixel<NORMALIZE, LOSS>(a, p, eps, per_value, charb_eps2, out, den,
-                                                     target, lp, sq);
+      const float4 pg = finish_pixel<NORMALIZE, LOSS>(v[k], p, eps, per_value, charb_eps2, out,
+                                                      den, target, lp, sq);
       if (LOSS != kNoLoss) {
-        pixel_grad[p] = v;
+        pixel_grad[p] = pg;
         loss_sum += lp;
         sq_sum += sq;
       }
@@ -363,16 +610,17 @@ struct FusedFit {
 __device__ __forceinline__ float4 render_pixel_grad(int normalize, const float* a, int64_t p,
                                                     float eps, const float* __restrict__ go,
                                                     float* out, float* den) {
-  const float denom = a[3] + eps;
+  const float denom = a[3] + eps, inv = 1.0f / denom;
   float o[3];
 #pragma unroll
-  for (int ch = 0; ch < 3; ++ch) o[ch] = normalize ? a[ch] / denom : a[ch];
+  for (int ch = 0; ch < 3; ++ch) o[ch] = normalize ? a[ch] * inv : a[ch];
   den[p] = a[3];
   out[3 * p] = o[0];
   out[3 * p + 1] = o[1];
   out[3 * p + 2] = o[2];
   const float gr = go[3 * p], gg = go[3 * p + 1], gb = go[3 * p + 2];
   if (!normalize) return make_float4(gr, gg, gb, 0.f);
+  // the backward prologue's arithmetic (backward_kernel), so the pixel inputs agree bitwise
   return make_float4(gr / denom, gg / denom, gb / denom, -(gr * o[0] + gg * o[1] + gb * o[2]) / denom);
 }
 
@@ -393,6 +641,25 @@ __device__ __forceinline__ float4 finish_pixel_rt(int normalize, int loss_kind, 
 #undef SS_FIN
 }
 
+// Shared memory of the backward tile kernel (dynamic): the stage (plus, in the fused pass, every
+// warp's carry slots for the forward phase), the tile's per-pixel inputs, the staged ids, the
+// cost-class order and counters, and in the fused pass the warps' hit queues.
+template <int TS, int NT, bool FUSED>
+struct BwdSmem {
+  static constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
+  static constexpr int kWarps = NT / 32;
+  static constexpr int kNullSlot = kStageMax + kWarps * kCarrySlots;  // fused pass only
+  static constexpr int kSlots = kStageMax + (FUSED ? kWarps * kCarrySlots + 1 : 0);
+  static constexpr size_t kPixOff = (size_t)kSlots * 4 * sizeof(float4);
+  static constexpr size_t kGidOff = kPixOff + (size_t)TS * TS * sizeof(float4);
+  static constexpr size_t kOrderOff = kGidOff + (size_t)kStageMax * sizeof(int);
+  static constexpr size_t kClassOff = kOrderOff + (size_t)kStageMax * sizeof(int);
+  static constexpr size_t kNextOff = kClassOff + 64 * sizeof(int);
+  static constexpr size_t kQueueOff = kNextOff + 16;
+  static constexpr size_t kBytes =
+      kQueueOff + (FUSED ? (size_t)kWarps * kQueueLen * sizeof(uint32_t) : 0);
+};
+
 template <int TS, int NT>
 struct BackwardOccupancy {  // CTAs per SM the register budget is planned for
   static constexpr int kBlocks = TS == 16 ? (NT == 128 ? 6 : 4) : (NT == 256 ? 4 : 2);
@@ -410,14 +677,16 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
                     float* __restrict__ partials, uint32_t* status, FusedFit ff) {
   pdl_wait();
   pdl_trigger();
+  using S = BwdSmem<TS, NT, FUSED>;
   constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
   constexpr int kHalf = kStageMax / 2;  // entries per chunk when a long list streams through
-  __shared__ __align__(16) float4 stage[kStageMax][4];
-  __shared__ float4 pix[TS * TS];
-  __shared__ int stage_gid[kStageMax];
-  __shared__ int order[kStageMax];
-  __shared__ int class_count[64];
-  __shared__ int next_group;  // the next group a warp takes
+  extern __shared__ __align__(16) unsigned char bwd_smem[];
+  float4(*stage)[4] = reinterpret_cast<float4(*)[4]>(bwd_smem);
+  float4* pix = reinterpret_cast<float4*>(bwd_smem + S::kPixOff);
+  int* stage_gid = reinterpret_cast<int*>(bwd_smem + S::kGidOff);
+  int* order = reinterpret_cast<int*>(bwd_smem + S::kOrderOff);
+  int* class_count = reinterpret_cast<int*>(bwd_smem + S::kClassOff);
+  int& next_group = *reinterpret_cast<int*>(bwd_smem + S::kNextOff);  // the next group a warp takes
   const int tile = blockIdx.x;
   const Frame fr = frame_of_tile(frames, tile, n);
   const int local = tile - fr.first_tile;
@@ -611,78 +880,64 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     }
   };
   if constexpr (FUSED) {
-    // The tile's forward over the staged records, in forward_kernel's per-pixel order (so the
-    // image, the loss gradient and the moments are bitwise those of the two-kernel step), then
-    // each pixel's loss gradient straight into pix.  Warp w takes the 8x8 blocks w, w + NT/32, …
+    // The tile's forward over the staged records, evaluated block by block exactly as
+    // forward_kernel evaluates them (so the image, the loss gradient and the moments are bitwise
+    // those of the two-kernel step), then each pixel's loss gradient straight into pix.  Warp w
+    // takes the 8x8 blocks w, w + NT/32, … one pass each; a list longer than the stage streams
+    // through once per pass, and once more for the backward.
     constexpr int kBlocks = (TS / 8) * (TS / 8);
     constexpr int kWarps = NT / 32;
     constexpr int kPer = (kBlocks + kWarps - 1) / kWarps;
-    float acc[kPer][2][4];
-#pragma unroll
-    for (int i = 0; i < kPer; ++i)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][0][k] = acc[i][1][k] = 0.f;
-    auto accumulate = [&](const float4(*st)[4], int m) {
-#pragma unroll
-      for (int i = 0; i < kPer; ++i) {
-        const int b = warp + i * kWarps;
-        if (b < kBlocks) {
-          const int sx0 = tx0 + (b % (TS / 8)) * 8, sy0 = ty0 + (b / (TS / 8)) * 8;
-          const int px = sx0 + (lane & 7), py0 = sy0 + (lane >> 3);
-          forward_block<FADE, false>(st, m, sx0, sy0, lane, px, py0, (float)px, (float)py0, tail,
-                              acc[i][0], acc[i][1]);
-        }
-      }
-    };
-    if (L.count <= kStageMax) {
+    uint32_t* q = reinterpret_cast<uint32_t*>(bwd_smem + S::kQueueOff) + warp * kQueueLen;
+    const bool whole = L.count <= kStageMax;
+    if (threadIdx.x == 0) write_null_record(stage, S::kNullSlot);
+    bool exact = false;
+    if (whole) {
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
       __syncthreads();
-      accumulate(stage, (int)L.count);
-    } else {  // a long list streams through once for the forward, again for the backward
-      float4(*buf)[kHalf][4] = reinterpret_cast<float4(*)[kHalf][4]>(stage);
-      const int64_t count = L.count;
-      const int nchunks = (int)((count + kHalf - 1) / kHalf);
-      auto len = [&](int64_t k0) { return (int)(count - k0 < kHalf ? count - k0 : kHalf); };
-      for (int c = 0; c < nchunks; ++c) {
-        const int64_t k0 = (int64_t)c * kHalf;
-        if (c + 1 < nchunks)
-          stage_range<NT>(buf[(c + 1) & 1], rec, L, k0 + kHalf, len(k0 + kHalf),
-                          stage_gid + ((c + 1) & 1) * kHalf);
-        cp_async_commit();
-        cp_async_wait_one();
-        __syncthreads();
-        accumulate(buf[c & 1], len(k0));
-        __syncthreads();
-      }
-      stage_range<NT>(buf[0], rec, L, 0, len(0), stage_gid);  // chunk 0 for the backward
-      cp_async_commit();
+      exact = !all_regular<NT>(stage, (int)L.count);
     }
     const float per_value = pixel_loss_scale(H, W);
     float loss_sum = 0.f, sq_sum = 0.f;
-#pragma unroll
+#pragma unroll 1
     for (int i = 0; i < kPer; ++i) {
       const int b = warp + i * kWarps;
-      if (b < kBlocks) {
-        const int lx = (b % (TS / 8)) * 8 + (lane & 7), px = tx0 + lx;
+      const bool active = b < kBlocks;
+      const int bx = active ? (b % (TS / 8)) * 8 : 0, by = active ? (b / (TS / 8)) * 8 : 0;
+      float2 acc[4][4];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          const int ly = (b / (TS / 8)) * 8 + (lane >> 3) + 4 * k, py = ty0 + ly;
-          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-          if (px < W && py < H) {
-            const int64_t p = fr.pixel_base + (int64_t)py * W + px;
-            if (ff.grad_out) {
-              v = render_pixel_grad(normalize, acc[i][k], p, eps, ff.grad_out, ff.image, ff.den);
-            } else {
-              float lp, sq;
-              v = finish_pixel_rt(normalize, ff.loss_kind, acc[i][k], p, eps, per_value,
-                                  ff.charb_eps2, ff.image, ff.den, ff.target, lp, sq);
-              loss_sum += lp;
-              sq_sum += sq;
-            }
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) acc[k][ch] = make_float2(0.f, 0.f);
+      accumulate_block<NT, FADE>(stage, kStageMax, rec, L, q, kQueueLen,
+                                 kStageMax + warp * kCarrySlots, S::kNullSlot, active, tx0 + bx,
+                                 ty0 + by, lane, tail, acc, whole, exact, i == 0);
+      if (!active) continue;
+      float v[2][4];
+      combine_groups(acc, lane, v);
+      const int lx = bx + (lane & 7), px = tx0 + lx;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int ly = by + block_first_row(lane) + k, py = ty0 + ly;
+        float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (px < W && py < H) {
+          const int64_t p = fr.pixel_base + (int64_t)py * W + px;
+          if (ff.grad_out) {
+            pv = render_pixel_grad(normalize, v[k], p, eps, ff.grad_out, ff.image, ff.den);
+          } else {
+            float lp, sq;
+            pv = finish_pixel_rt(normalize, ff.loss_kind, v[k], p, eps, per_value, ff.charb_eps2,
+                                 ff.image, ff.den, ff.target, lp, sq);
+            loss_sum += lp;
+            sq_sum += sq;
           }
-          pix[ly * TS + lx] = v;
         }
+        pix[ly * TS + lx] = pv;
       }
+    }
+    if (!whole) {  // chunk 0 again, with its ids, for the backward
+      stage_range<NT>(stage, rec, L, 0, (int)(L.count < kHalf ? L.count : kHalf), stage_gid);
+      cp_async_commit();
     }
     if (ff.loss) {
 #pragma unroll
@@ -823,11 +1078,13 @@ __global__ void entry_keys_kernel(const int32_t* __restrict__ gids,
                                   int32_t* __restrict__ order) {
   pdl_wait();
   pdl_trigger();
-  const int64_t last = offsets[T];
+  // the entries of tiles [0, T): positions [offsets[0], offsets[T]) of the list (offsets[0] > 0
+  // for a window of an image's tile rows)
+  const int64_t first = offsets[0], last = offsets[T];
   const int64_t total = last < cap ? last : cap;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cap; e += stride) {
-    const int32_t id = e < total ? gids[e] : -1;
+    const int32_t id = e >= first && e < total ? gids[e] : -1;
     keys[e] = (id >= 0 && id < n) ? (uint32_t)id : (uint32_t)n;
     order[e] = (int32_t)e;
   }
@@ -903,8 +1160,9 @@ void launch_forward_loss(int loss_kind, unsigned T, cudaStream_t s, const Splat*
                          const float* target, float4* pixel_grad, float* loss, float ce2) {
   constexpr int NT = Tiling<TS>::kFwdThreads;
 #define SS_FWD(LOSS)                                                                          \
-  launch("forward_kernel", forward_kernel<TS, NORM, FADE, LOSS>, T, NT, 0, s, rec, n, gids,   \
-         cap, offsets, f, eps, tail, out, den, target, pixel_grad, loss, ce2)
+  launch_smem("forward_kernel", forward_kernel<TS, NORM, FADE, LOSS>, T, NT,                  \
+              FwdSmem<TS>::kBytes, s, rec, n, gids, cap, offsets, f, eps, tail, out, den,      \
+              target, pixel_grad, loss, ce2)
   switch (loss_kind) {
     case kL1: SS_FWD(kL1); break;
     case kL2: SS_FWD(kL2); break;
@@ -942,9 +1200,9 @@ void launch_backward_nt(unsigned T, cudaStream_t s, bool deterministic, const fl
                         float tail, float* ws, uint32_t* status) {
   const bool fade = tail > 0.0f;
 #define SS_BWD(FADE, DET)                                                                     \
-  launch("backward_kernel", backward_kernel<TS, NT, FADE, DET, PIXGRAD>, T, NT, 0, s, grad_out, \
-         rec, n, den, out, pixel_grad, gids, cap, offsets, f, normalize, eps, tail, ws, ws,    \
-         status, FusedFit{})
+  launch_smem("backward_kernel", backward_kernel<TS, NT, FADE, DET, PIXGRAD>, T, NT,         \
+              (BwdSmem<TS, NT, false>::kBytes), s, grad_out, rec, n, den, out, pixel_grad,   \
+              gids, cap, offsets, f, normalize, eps, tail, ws, ws, status, FusedFit{})
   if (deterministic) {
     if (fade) SS_BWD(true, true); else SS_BWD(false, true);
   } else {
@@ -979,9 +1237,9 @@ void launch_fused_nt(unsigned T, cudaStream_t s, bool deterministic, const Splat
                      const FusedFit& ff) {
   const bool fade = tail > 0.0f;
 #define SS_FUS(FADE, DET)                                                                       \
-  launch("fit_tile_kernel", backward_kernel<TS, NT, FADE, DET, false, true>, T, NT, 0, s,      \
-         nullptr, rec, n, nullptr, nullptr, nullptr, gids, cap, offsets, f, normalize, eps,    \
-         tail, ws, ws, status, ff)
+  launch_smem("fit_tile_kernel", backward_kernel<TS, NT, FADE, DET, false, true>, T, NT,     \
+              (BwdSmem<TS, NT, true>::kBytes), s, nullptr, rec, n, nullptr, nullptr, nullptr, \
+              gids, cap, offsets, f, normalize, eps, tail, ws, ws, status, ff)
   if (deterministic) {
     if (fade) SS_FUS(true, true); else SS_FUS(false, true);
   } else {

@@ -3,6 +3,9 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
+#include <utility>
+#include <vector>
 
 #include "ss_common.cuh"
 
@@ -37,10 +40,26 @@ int check_launch(const char* what) {
   return SS_OK;
 }
 
+int allow_dynamic_smem(const void* kern, size_t bytes) {
+  // (kernel, device) pairs already opted in; a handful of kernels use more than 48 KB
+  static std::mutex mu;
+  static std::vector<std::pair<const void*, int>> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return check_launch("cudaGetDevice");
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& d : done)
+    if (d.first == kern && d.second == dev) return SS_OK;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+      cudaSuccess)
+    return check_launch("dynamic shared memory attribute");
+  done.emplace_back(kern, dev);
+  return SS_OK;
+}
+
 int frames_of_batch(const ss_batch* batch, int64_t n, Frames* out) {
   if (!batch) return fail(SS_ERR_INVALID_ARGUMENT, "null batch");
   if (batch->images < 1) return fail(SS_ERR_INVALID_ARGUMENT, "batch needs at least one image");
-  if (batch->tile_size <= 0 || batch->tile_size * batch->tile_size > 1024)
+  if (batch->tile_size <= 0 || batch->tile_size > 32)  // ts^2 <= 1024, without overflow
     return fail(SS_ERR_INVALID_ARGUMENT, "batch tile_size must be positive with ts^2 <= 1024");
   if (batch->tiles < 0 || batch->tiles + 1 > (int64_t)INT32_MAX || batch->pixels < 0)
     return fail(SS_ERR_INVALID_ARGUMENT, "batch tile or pixel total out of range");

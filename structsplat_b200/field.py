@@ -13,9 +13,9 @@ from torch.autograd import Function
 from torch.autograd.function import once_differentiable
 
 from . import _native
-from .render import (DEFAULT_EPS, RECORD_FLOATS, RENDER_TILE, TileIndex, _backward, _forward, _p,
-                     _stream, fade_tail, index_from_records, resolve_fade_alpha, tile_grid,
-                     validate_eps)
+from .render import (DEFAULT_EPS, EAGER_PLANS, RECORD_FLOATS, RENDER_TILE, TileIndex, _backward,
+                     _forward, _p, _stream, fade_tail, index_from_records, resolve_fade_alpha,
+                     tile_grid, validate_eps)
 
 
 def project(means, log_scales, rotations, colors, opacity_logits, H: int, W: int,
@@ -43,35 +43,88 @@ class _B200RenderRS(Function):
         means, log_scales = means.contiguous(), log_scales.contiguous()
         rotations, colors = rotations.contiguous(), colors.contiguous()
         logits = None if logits is None else logits.contiguous()
+        ctx.meta = (n, H, W, bool(normalize), float(eps), int(tile_size), float(tail),
+                    logits is not None, float(dilation), bool(deterministic), bool(cull),
+                    float(sigma_cutoff))
+        if not deterministic and n and H * W:
+            # the fast path: the problem's buffers persist between calls (EagerPlan)
+            plan = EAGER_PLANS.get(n, H, W, tile_size, cull, sigma_cutoff, means.device)
+            _native.call("ss_project_rs_index_count", _p(means), _p(log_scales), _p(rotations),
+                         _p(colors), _p(logits), n, float(dilation), float(sigma_cutoff), H, W,
+                         tile_size, int(cull), _p(plan.records), _p(plan.offsets),
+                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.step_block),
+                         plan.step_block.numel(), _p(plan.status), _stream())
+            plan.ensure_capacity()
+            _native.call("ss_tile_index_fill", _p(plan.records), n, H, W, tile_size, int(cull),
+                         float(sigma_cutoff), _p(plan.offsets), _p(plan.gids), plan.capacity,
+                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), _stream())
+            out = torch.empty(H, W, 3, device=means.device, dtype=torch.float32)
+            den = torch.empty(H, W, device=means.device, dtype=torch.float32)
+            _native.call("ss_render_forward", _p(plan.records), n, _p(plan.gids), plan.capacity,
+                         _p(plan.offsets), H, W, tile_size, int(normalize), float(eps),
+                         float(tail), _p(out), _p(den), _p(plan.status), _stream())
+            plan.note_status()
+            plan.generation += 1
+            plan.moments_used = False
+            ctx.plan, ctx.generation = plan, plan.generation
+            ctx.save_for_backward(out, den, means, log_scales, rotations, colors, logits)
+            return out
         rec, _, _ = project(means, log_scales, rotations, colors, logits, H, W, sigma_cutoff,
                             dilation)
         index = index_from_records(rec, n, H, W, tile_size, cull, sigma_cutoff,
                                    exact=bool(deterministic))
         out, den = _forward(rec, n, index, H, W, normalize, eps, tail, means.device)
-        ctx.save_for_backward(rec, index.gids, index.offsets, index.status, out, den,
-                              log_scales, rotations, logits)
-        ctx.meta = (n, H, W, bool(normalize), float(eps), int(tile_size), float(tail),
-                    logits is not None, float(dilation), bool(deterministic))
+        ctx.plan = None
+        ctx.save_for_backward(out, den, means, log_scales, rotations, colors, logits, rec,
+                              index.gids, index.offsets, index.status)
         return out
 
     @staticmethod
     @once_differentiable
     def backward(ctx, grad_out):
-        rec, gids, offsets, status, out, den, log_scales, rotations, logits = ctx.saved_tensors
-        n, H, W, normalize, eps, ts, tail, has_op, dilation, det = ctx.meta
+        n, H, W, normalize, eps, ts, tail, has_op, dilation, det, cull, cutoff = ctx.meta
         if n == 0:
             return (None,) * 15
-        index = TileIndex(gids, offsets, ts, status)
-        g_means, g_conics, g_colors, g_opac = _backward(
-            grad_out.contiguous().to(torch.float32), rec, n, den, out, index, H, W, normalize,
-            eps, tail, has_op, det, grad_out.device)
-        g_ls = torch.empty_like(log_scales)
-        g_rot = torch.empty_like(rotations)
-        g_logits = torch.empty_like(logits) if has_op else None
-        _native.call("ss_project_rs_backward", _p(log_scales), _p(rotations), _p(logits), n,
-                     float(dilation), _p(g_conics), _p(g_opac), _p(g_ls), _p(g_rot),
-                     _p(g_logits), _stream())
+        saved = ctx.saved_tensors
+        out, den, means, log_scales, rotations, colors, logits = saved[:7]
+        grad_out = grad_out.contiguous().to(torch.float32)
         need = ctx.needs_input_grad
+        plan = ctx.plan
+        if plan is not None and plan.generation == ctx.generation:
+            dev = grad_out.device
+            if plan.moments_used:  # a second backward of the same forward
+                plan.bwd_ws.zero_()
+            plan.moments_used = True
+            _native.call("ss_render_backward_moments", _p(grad_out), None, _p(plan.records), n,
+                         _p(den), _p(out), _p(plan.gids), plan.capacity, _p(plan.offsets), H, W,
+                         ts, int(normalize), float(eps), float(tail), 0, _p(plan.bwd_ws),
+                         plan.bwd_ws_bytes, _p(plan.status), _stream())
+            flat = torch.empty(9 * n, device=dev, dtype=torch.float32)
+            g_means, g_ls = flat[:2 * n].view(n, 2), flat[2 * n:4 * n].view(n, 2)
+            g_rot, g_colors = flat[4 * n:5 * n], flat[5 * n:8 * n].view(n, 3)
+            g_logits = flat[8 * n:] if has_op else None
+            _native.call("ss_render_backward_finalize_rs", _p(plan.records), n, _p(plan.gids),
+                         plan.capacity, _p(plan.offsets), H, W, ts, 0, _p(plan.bwd_ws),
+                         _p(log_scales), _p(rotations), _p(logits), float(dilation),
+                         _p(g_means), _p(g_ls), _p(g_rot), _p(g_colors), _p(g_logits),
+                         _stream())
+        else:
+            if plan is not None:  # the plan moved on to a later forward: rebuild this one's
+                rec, _, _ = project(means, log_scales, rotations, colors, logits, H, W, cutoff,
+                                    dilation)
+                index = index_from_records(rec, n, H, W, ts, cull, cutoff, exact=True)
+            else:
+                rec, gids, offsets, status = saved[7:]
+                index = TileIndex(gids, offsets, ts, status)
+            g_means, g_conics, g_colors, g_opac = _backward(
+                grad_out, rec, n, den, out, index, H, W, normalize, eps, tail, has_op, det,
+                grad_out.device)
+            g_ls = torch.empty_like(log_scales)
+            g_rot = torch.empty_like(rotations)
+            g_logits = torch.empty_like(logits) if has_op else None
+            _native.call("ss_project_rs_backward", _p(log_scales), _p(rotations), _p(logits), n,
+                         float(dilation), _p(g_conics), _p(g_opac), _p(g_ls), _p(g_rot),
+                         _p(g_logits), _stream())
         return (g_means if need[0] else None, g_ls if need[1] else None,
                 g_rot if need[2] else None, g_colors if need[3] else None,
                 g_logits if (has_op and need[4]) else None) + (None,) * 10

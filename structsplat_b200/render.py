@@ -150,6 +150,94 @@ class _CapacityCache:
 CAPACITY = _CapacityCache()
 
 
+class EagerPlan:
+    """Buffers of one problem (device, N, H, W, tile size, cull) for the eager autograd path,
+    kept between calls: splat records, tile offsets and list, index workspace, and the fast
+    backward's moments and status word in one block that the step clears.  A fit loop renders
+    the same problem every iteration, so a forward + backward then allocates only its outputs
+    and makes five library calls.
+
+    The plan holds the state of the last forward that used it (``generation``).  A backward
+    whose forward has been followed by another forward on the same plan (two renders before one
+    backward) rebuilds its records and index from its saved inputs instead.  The list capacity
+    starts at the first call's entry total (one host read) with headroom; each call copies its
+    status word to pinned memory, and a later call that finds an overflow there re-reads the
+    total and grows the list (the overflowing call itself was exact: its truncated tiles scan
+    every Gaussian)."""
+
+    HEADROOM = 1.5
+
+    def __init__(self, n: int, H: int, W: int, tile_size: int, cull: bool, sigma_cutoff: float,
+                 device):
+        self.n, self.H, self.W, self.ts = n, H, W, tile_size
+        self.cull, self.cutoff = bool(cull), float(sigma_cutoff)
+        tiles_x, tiles_y = tile_grid(H, W, tile_size)
+        self.T = tiles_x * tiles_y
+        d = device
+        self.records = torch.empty(max(n, 1) * RECORD_FLOATS, device=d, dtype=torch.float32)
+        self.offsets = torch.zeros(self.T + 1, device=d, dtype=torch.int32)
+        self.idx_ws_bytes = _native.size_query("ss_tile_index_workspace_bytes", n, H, W,
+                                               tile_size)
+        self.idx_ws = torch.empty(max(self.idx_ws_bytes, 1), device=d, dtype=torch.uint8)
+        self.capacity = 0
+        self.gids = None
+        self.generation = 0
+        self.moments_used = False
+        self.host_status = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self.event = None
+        self._size_list(1)
+
+    def _size_list(self, capacity: int):
+        self.capacity = int(capacity)
+        d = self.records.device
+        self.gids = torch.empty(max(self.capacity, 1), device=d, dtype=torch.int32)
+        self.bwd_ws_bytes = _native.size_query("ss_render_backward_workspace_bytes", self.n,
+                                               self.capacity, self.H, self.W, 0)
+        ws_len = (max(self.bwd_ws_bytes, 16) + 255) // 256 * 256
+        self.step_block = torch.zeros(ws_len + 256, device=d, dtype=torch.uint8)
+        self.bwd_ws = self.step_block[:ws_len]
+        self.status = self.step_block[ws_len:ws_len + 4].view(torch.int32)
+
+    def ensure_capacity(self):
+        """After the count: size the list on first use, or grow it after an overflow seen in
+        an earlier call's status (both read the entry total back)."""
+        grow = self.gids is None or self.capacity <= 1
+        if not grow and self.event is not None and self.event.query():
+            grow = bool(int(self.host_status[0]) & 1)
+            self.event = None
+        if grow:
+            total = int(self.offsets[-1].item())
+            if total > self.capacity or self.capacity <= 1:
+                self._size_list(int(total * self.HEADROOM) + 4096)
+                self.step_block.zero_()
+
+    def note_status(self):
+        self.host_status.copy_(self.status, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self.event = ev
+
+
+class _EagerPlans:
+    """One EagerPlan per problem key; a handful of keys at most in a fit."""
+
+    def __init__(self, limit: int = 8):
+        self.plans = {}
+        self.limit = limit
+
+    def get(self, n, H, W, tile_size, cull, sigma_cutoff, device) -> EagerPlan:
+        key = (device.index, n, H, W, tile_size, bool(cull), float(sigma_cutoff))
+        plan = self.plans.get(key)
+        if plan is None:
+            if len(self.plans) >= self.limit:
+                self.plans.pop(next(iter(self.plans)))
+            plan = self.plans[key] = EagerPlan(n, H, W, tile_size, cull, sigma_cutoff, device)
+        return plan
+
+
+EAGER_PLANS = _EagerPlans()
+
+
 def index_from_records(records, n: int, H: int, W: int, tile_size: int = 16,
                        ellipse_cull: bool = False, sigma_cutoff: float = 3.0,
                        capacity: int | None = None, exact: bool = False) -> TileIndex:
@@ -232,27 +320,78 @@ class _B200Render(Function):
         radii = radii.contiguous()
         has_op = opacities is not None and opacities.numel() > 0
         op = opacities.contiguous() if has_op else None
+        ctx.meta = (n, H, W, bool(normalize), float(eps), int(tile_size), float(tail), has_op,
+                    bool(deterministic), bool(cull), float(sigma_cutoff))
+        if not deterministic and n and H * W:
+            # the fast path: the problem's buffers persist between calls (EagerPlan)
+            plan = EAGER_PLANS.get(n, H, W, tile_size, cull, sigma_cutoff, means.device)
+            plan.step_block.zero_()  # fast moments and the status word
+            _native.call("ss_pack_splats", _p(means), _p(conics), _p(colors), _p(radii), _p(op),
+                         n, H, W, _p(plan.records), _stream())
+            _native.call("ss_tile_index_count", _p(plan.records), n, H, W, tile_size, int(cull),
+                         float(sigma_cutoff), _p(plan.offsets), _p(plan.idx_ws),
+                         plan.idx_ws_bytes, _p(plan.status), _stream())
+            plan.ensure_capacity()
+            _native.call("ss_tile_index_fill", _p(plan.records), n, H, W, tile_size, int(cull),
+                         float(sigma_cutoff), _p(plan.offsets), _p(plan.gids), plan.capacity,
+                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), _stream())
+            out = torch.empty(H, W, 3, device=means.device, dtype=torch.float32)
+            den = torch.empty(H, W, device=means.device, dtype=torch.float32)
+            _native.call("ss_render_forward", _p(plan.records), n, _p(plan.gids), plan.capacity,
+                         _p(plan.offsets), H, W, tile_size, int(normalize), float(eps),
+                         float(tail), _p(out), _p(den), _p(plan.status), _stream())
+            plan.note_status()
+            plan.generation += 1
+            plan.moments_used = False
+            ctx.plan, ctx.generation = plan, plan.generation
+            ctx.save_for_backward(out, den, means, conics, colors, radii, op)
+            return out
         rec = pack_records(means, conics, colors, radii, op, H, W)
         index = index_from_records(rec, n, H, W, tile_size, cull, sigma_cutoff,
                                    exact=bool(deterministic))
         out, den = _forward(rec, n, index, H, W, normalize, eps, tail, means.device)
-        ctx.save_for_backward(rec, index.gids, index.offsets, index.status, out, den)
-        ctx.meta = (n, H, W, bool(normalize), float(eps), int(tile_size), float(tail), has_op,
-                    bool(deterministic))
+        ctx.plan = None
+        ctx.save_for_backward(out, den, means, conics, colors, radii, op, rec, index.gids,
+                              index.offsets, index.status)
         return out
 
     @staticmethod
     @once_differentiable
     def backward(ctx, grad_out):
-        rec, gids, offsets, status, out, den = ctx.saved_tensors
-        n, H, W, normalize, eps, ts, tail, has_op, det = ctx.meta
+        n, H, W, normalize, eps, ts, tail, has_op, det, cull, cutoff = ctx.meta
         need = ctx.needs_input_grad
         if not (need[0] or need[1] or need[2] or need[4]) or n == 0:
             return (None,) * 14
-        index = TileIndex(gids, offsets, ts, status)
-        g_means, g_conics, g_colors, g_opac = _backward(
-            grad_out.contiguous().to(torch.float32), rec, n, den, out, index, H, W, normalize,
-            eps, tail, has_op, det, grad_out.device)
+        saved = ctx.saved_tensors
+        out, den, means, conics, colors, radii, op = saved[:7]
+        grad_out = grad_out.contiguous().to(torch.float32)
+        dev = grad_out.device
+        plan = ctx.plan
+        if plan is not None and plan.generation == ctx.generation:
+            if plan.moments_used:  # a second backward of the same forward
+                plan.bwd_ws.zero_()
+            plan.moments_used = True
+            _native.call("ss_render_backward_moments", _p(grad_out), None, _p(plan.records), n,
+                         _p(den), _p(out), _p(plan.gids), plan.capacity, _p(plan.offsets), H, W,
+                         ts, int(normalize), float(eps), float(tail), 0, _p(plan.bwd_ws),
+                         plan.bwd_ws_bytes, _p(plan.status), _stream())
+            flat = torch.empty(9 * n, device=dev, dtype=torch.float32)
+            g_means, g_conics = flat[:2 * n].view(n, 2), flat[2 * n:5 * n].view(n, 3)
+            g_colors = flat[5 * n:8 * n].view(n, 3)
+            g_opac = flat[8 * n:] if has_op else None
+            _native.call("ss_render_backward_finalize", _p(plan.records), n, _p(plan.gids),
+                         plan.capacity, _p(plan.offsets), H, W, ts, int(has_op), 0,
+                         _p(plan.bwd_ws), _p(g_means), _p(g_conics), _p(g_colors), _p(g_opac),
+                         _stream())
+        else:
+            if plan is not None:  # the plan moved on to a later forward: rebuild this one's
+                rec = pack_records(means, conics, colors, radii, op, H, W)
+                index = index_from_records(rec, n, H, W, ts, cull, cutoff, exact=True)
+            else:
+                rec, gids, offsets, status = saved[7:]
+                index = TileIndex(gids, offsets, ts, status)
+            g_means, g_conics, g_colors, g_opac = _backward(
+                grad_out, rec, n, den, out, index, H, W, normalize, eps, tail, has_op, det, dev)
         return (g_means if need[0] else None, g_conics if need[1] else None,
                 g_colors if need[2] else None, None,
                 g_opac if (has_op and need[4]) else None) + (None,) * 9

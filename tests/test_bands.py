@@ -1,6 +1,7 @@
-"""One image split into bands of tile rows across two gloo ranks on the CPU (the oracle renders
-each band): the band images stack into the full image and the all-reduced band gradients are
-the full image's gradients."""
+"""One image split into bands of tile rows across two gloo ranks on the CPU (the oracle stands in
+for each rank's band: the full image's pixels of the band rows, and the gradients of those
+pixels alone): the band images stack into the full image and the all-reduced band gradients
+are the full image's gradients."""
 from __future__ import annotations
 
 import os
@@ -31,12 +32,15 @@ def _inputs():
 
 
 def _band(rank, world):
+    """A rank's band as the library computes it: the full image's records and tile lists,
+    rendered and differentiated over the band's rows only."""
     means, conics, colors, radii, opac, grad_out = _inputs()
     y0, y1 = band_rows(H, W, rank, world, TS)
-    shifted = means - torch.tensor([0.0, float(y0)], dtype=means.dtype)
-    img, _, grads = render_ref.render_with_grads(shifted, conics, colors, radii, y1 - y0, W,
-                                                 grad_out[y0:y1], opacities=opac)
-    return (y0, y1), img, grads
+    band_grad = torch.zeros_like(grad_out)
+    band_grad[y0:y1] = grad_out[y0:y1]
+    img, _, grads = render_ref.render_with_grads(means, conics, colors, radii, H, W, band_grad,
+                                                 opacities=opac)
+    return (y0, y1), img[y0:y1], grads
 
 
 def test_bands_cover_the_tile_rows():

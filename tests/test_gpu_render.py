@@ -195,8 +195,11 @@ def test_zero_sized_image():
 @pytest.mark.parametrize("name", ["render_synthetic_64_256.npz", "render_elongated_fade.npz",
                                   "render_matrix_add_op_d3_f1.npz"])
 def test_render_tile_sizes_agree(name):
-    """16x16 and 32x32 render tiles visit each pixel's Gaussians in the same (ascending) order:
-    identical images, gradients equal to rounding."""
+    """16x16 and 32x32 render tiles give every 8x8 block the same hits in the same order, so the
+    images are identical.  With the full support fade the ellipse cull drops each tile's
+    zero-weight pairs, which differ between the tile sizes: a block may then list a Gaussian
+    that contributes exact zeros in one tiling and not in the other, which moves the later hits
+    to other partial sums; those images agree to float rounding.  Gradients agree to rounding."""
     require_cuda()
     z = golden(name)
     outs = []
@@ -210,7 +213,10 @@ def test_render_tile_sizes_agree(name):
                           normalize=bool(z["normalize"]), eps=float(z["eps"]),
                           support_fade=alpha > 0, support_fade_alpha=alpha, tile_size=ts)
         outs.append((img.detach(), torch.autograd.grad(img, leaves, cuda(z["grad_out"]))))
-    assert torch.equal(outs[0][0], outs[1][0])
+    if float(z["fade_alpha"]) >= 1.0:
+        assert rel_err(outs[0][0], outs[1][0]) <= 1e-6
+    else:
+        assert torch.equal(outs[0][0], outs[1][0])
     for a, b in zip(outs[0][1], outs[1][1]):
         assert rel_err(a, b) <= 1e-5
 
