@@ -110,10 +110,24 @@ def make_inputs(dev, wl=WORKLOAD):
     return host
 
 
-def pair_count(host, wl=WORKLOAD):
-    from oracle import c_oracle, field_ref
-    r = field_ref.radii(torch.tensor(host["log_scales"]), torch.tensor(host["rotations"]), 3.0)
-    return c_oracle.pair_count(host["means"], r, wl["H"], wl["W"])
+def pair_count(host, wl=WORKLOAD, dev=None):
+    """P = sum over Gaussians of the pixels in their clipped support rectangle (the work unit of
+    the roofline): radii from the library's RS projection, rectangles as render.py:62-78 clips
+    them (centre rounded half to even, int64)."""
+    from structsplat_b200.field import project
+    dev = dev or torch.device("cuda")
+    t = {k: torch.as_tensor(host[k]).to(dev) for k in ("means", "log_scales", "rotations")}
+    n = t["means"].shape[0]
+    _, _, radii = project(t["means"], t["log_scales"], t["rotations"],
+                          torch.zeros(n, 3, device=dev), None, wl["H"], wl["W"],
+                          want_conics=True)
+    m = t["means"].double()
+    ok = torch.isfinite(m).all(dim=1)
+    c = torch.round(torch.where(ok[:, None], m, torch.zeros_like(m))).long()
+    lo = torch.clamp(c - radii, min=0)
+    hi = torch.minimum(c + radii, torch.tensor([wl["W"] - 1, wl["H"] - 1], device=dev))
+    side = torch.clamp(hi - lo + 1, min=0)
+    return int((side[:, 0] * side[:, 1] * ok).sum())
 
 
 def flush_l2(buf):
@@ -284,6 +298,9 @@ def run_ours(args, rank, world, dev):
             raise RuntimeError(f"e2e step gradient {k} differs from the captured step ({err:.2e})")
     del graphs
 
+    step.replay()
+    torch.cuda.synchronize()
+    step_out = {"image": plan.image.clone(), "grads": {k: v.clone() for k, v in grads.items()}}
     stats = torch.tensor([total_ms, e2e_total, e2e_serial_total], dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
@@ -292,7 +309,7 @@ def run_ours(args, rank, world, dev):
             "fused": plan.use_fused(), "additive_ms": statistics.median(additive_ms),
             "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
             "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
-            "clocks": clocks.summary(), "host": host}
+            "clocks": clocks.summary(), "host": host, "step_out": step_out}
 
 
 KERNELS_PER_CALL = {
@@ -399,6 +416,66 @@ def ref_cuda_baseline(host, dev, steps=10, normalize=True):
     return res
 
 
+def _rel(a, b) -> float:
+    a = torch.as_tensor(a).detach().double().cpu()
+    b = torch.as_tensor(b).detach().double().cpu()
+    return float((a - b).abs().max() / b.abs().max().clamp_min(1e-30))
+
+
+def parity_object(host, dev, image, grads, normalize=True):
+    """Errors of the timed step's image and RS-field gradients against the reference on the same
+    field: its CUDA extension's float32 result (tiled arm, through its own GaussianField and
+    render_cuda_exact) and its own renderer evaluated in float64 on the CPU
+    (GaussianField.from_numpy(dtype=float64) semantics, render.py:180-235), as max |d| / max |ref|.
+    """
+    names = ("means", "log_scales", "rotations", "colors", "opacity_logits")
+    H, W = WORKLOAD["H"], WORKLOAD["W"]
+    out = {"metric": "max |ours - ref| / max |ref| over the image and each gradient"}
+    ref_root = REPO / "baseline" / "_ref"
+    if not (ref_root / "structsplat" / "render.py").is_file():
+        return {"unavailable": "the reference package is not installed under baseline/_ref"}
+    if str(ref_root) not in sys.path:
+        sys.path.insert(0, str(ref_root))
+    from structsplat.gaussians import GaussianField
+    from structsplat.render import render_field
+
+    def reference(device, dtype, cuda_ext):
+        f = GaussianField(*[torch.tensor(host[k], dtype=dtype, device=device) for k in names])
+        f.trainable()
+        params = [f.means, f.log_scales, f.rotations, f.colors, f.opacities]
+        go = torch.tensor(host["grad_out"], dtype=dtype, device=device)
+        if cuda_ext is not None:
+            img = cuda_ext.render_cuda_exact(f.means, f.conics(), f.colors, f.radii(3.0), H, W,
+                                             opacities=f.opacity_values(), normalize=normalize,
+                                             tiled=True)
+        else:
+            img = render_field(f.means, f.conics(), f.colors, f.radii(3.0), H, W,
+                               mode="normalized" if normalize else "additive",
+                               opacities=f.opacity_values())
+        g = torch.autograd.grad(img, params, go)
+        return img.detach(), dict(zip(names, g))
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    img64, g64 = reference("cpu", torch.float64, None)
+    ours = {"image": image, **grads}
+    ref64 = {"image": img64, **g64}
+    out["vs_reference_float64"] = {k: round(_rel(ours[k], ref64[k]), 9) for k in ours}
+    try:
+        sys.path.insert(0, str(REPO / "baseline"))
+        from build_ref_cuda import load_reference_extension
+        ext = load_reference_extension()
+    except Exception as exc:
+        out["vs_reference_cuda_float32"] = {"unavailable": str(exc)[:200]}
+        return out
+    img32, g32 = reference(dev, torch.float32, ext)
+    ref32 = {"image": img32, **g32}
+    out["vs_reference_cuda_float32"] = {k: round(_rel(ours[k], ref32[k]), 9) for k in ours}
+    out["reference_cuda_float32_vs_float64"] = {k: round(_rel(ref32[k], ref64[k]), 9)
+                                                for k in ours}
+    out["bars"] = {"image": 1e-5, "gradients": 1e-4}
+    return out
+
+
 BATCH_SIZES = [(256, 256), (512, 512), (512, 768), (1024, 1024), (1536, 2048)]  # (H, W)
 BATCH_IMAGES, BATCH_DENSITY, BATCH_SEED = 64, 0.1, 7
 
@@ -490,9 +567,10 @@ def run_batched(args, dev, workload):
     for p in plans:
         _, loss = p.render()
         psnr_l.append(psnr_from_mse(float(loss[0, 1])))
-    # per-image loop with every image's step captured in its own graph
+    # per-image loop with every image's step captured in its own graph (timing only)
+    Kg = min(K, 100)
     graphs = [GraphStep(p) for p in plans]
-    t_loop_graph = timed(lambda: [g.replay() for g in graphs], K)
+    t_loop_graph = timed(lambda: [g.replay() for g in graphs], Kg) * K / Kg
     del graphs, plans
 
     # ranks fit disjoint shares of the images: the job is as slow as its slowest rank
@@ -500,8 +578,9 @@ def run_batched(args, dev, workload):
     t_batch, t_loop, t_loop_graph, dpsnr = max_over_ranks(
         [t_batch, t_loop, t_loop_graph,
          float(np.max(np.abs(np.array(psnr_b) - np.array(psnr_l))))], device=dev)
-    B_all, px_all, g_all, e_all, psum = sum_over_ranks(
-        [B, batch.pixels, batch.n, entries, float(np.sum(psnr_b))], device=dev)
+    B_all, px_all, g_all, e_all, psum, psum_loop = sum_over_ranks(
+        [B, batch.pixels, batch.n, entries, float(np.sum(psnr_b)), float(np.sum(psnr_l))],
+        device=dev)
     B_all = int(B_all)
     res = {
         "workload": f"{B_all} images, sizes uniform over {{256x256, 512x512, 768x512, 1024x1024, "
@@ -516,11 +595,46 @@ def run_batched(args, dev, workload):
         "loop_eager_img_s": round(B_all * K / (t_loop * 1e-3), 1),
         "loop_graph_img_s": round(B_all * K / (t_loop_graph * 1e-3), 1),
         "psnr_batched_mean": round(psum / max(B_all, 1), 4),
+        "psnr_loop_mean": round(psum_loop / max(B_all, 1), 4),
         "psnr_max_abs_diff_vs_loop": round(dpsnr, 6),
         "psnr_after_steps": Wm + K, "index_overflow": overflow,
         "gpu_launches_per_step": 8, "peak_mem_gb": round(mem_gb, 2), "clocks": clocks.summary(),
     }
     res["speedup_vs_loop_eager"] = round(res["batched_img_s"] / res["loop_eager_img_s"], 3)
+    res["loop_graph_steps"] = Kg
+    # Fast mode sums the moments with float atomics, so two runs of the same fit drift apart by
+    # rounding over the steps; the deterministic mode's batched and per-image fits are bitwise
+    # the same iteration, so their PSNRs are equal (checked here over Kd steps, both timed).
+    Kd = min(K, 100)
+    dset = FitSettings(deterministic=True)
+    fdet = fresh()
+    dplan = FitPlan(batch, Batch.concat_fields(fdet), batch.concat_images(targets), dset)
+    dstep = GraphStep(dplan)
+    t_det = timed(dstep.replay, Kd)
+    _, dloss = dplan.render()
+    del dstep, dplan
+    fdl = fresh()
+    dplans = [FitPlan(Batch([sizes[b]], [counts[b]], device=dev), fdl[b],
+                      targets[b].reshape(-1, 3), dset) for b in range(B)]
+    t_det_loop = timed(lambda: [p.step() for p in dplans], Kd)
+    dl = [float(p.render()[1][0, 1]) for p in dplans]
+    del dplans
+    ddiff = float(np.max(np.abs(np.array([psnr_from_mse(m) for m in dloss[:, 1].tolist()]) -
+                                np.array([psnr_from_mse(m) for m in dl]))))
+    t_det, t_det_loop, ddiff = max_over_ranks([t_det, t_det_loop, ddiff], device=dev)
+    res["deterministic"] = {"steps": Kd, "batched_img_s": round(B_all * Kd / (t_det * 1e-3), 1),
+                            "loop_eager_img_s": round(B_all * Kd / (t_det_loop * 1e-3), 1),
+                            "psnr_max_abs_diff_vs_loop": round(ddiff, 9)}
+    # the fit step's work: the in-rectangle pairs of every image (forward + backward slots)
+    pairs = sum(pair_count({"means": f.means, "log_scales": f.log_scales,
+                            "rotations": f.rotations}, {"H": h, "W": w}, dev=dev)
+                for f, (h, w) in zip(fields_np, sizes))
+    (pairs,) = sum_over_ranks([float(pairs)], device=dev)
+    f_mhz = measured_peaks().get("sm_max_mhz") or 1965.0
+    peak_slots = SM_COUNT * FP32_LANES * f_mhz * 1e6
+    res["pairs_per_step"] = int(pairs)
+    res["step_roofline_frac"] = round(
+        pairs * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / peak_slots / (t_batch / K * 1e-3), 4)
     world = torch.distributed.get_world_size() if torch.distributed.is_initialized() else 1
     if not args.no_ref_cuda and world == 1:
         res["reference_loop"] = ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev,
@@ -535,12 +649,13 @@ def run_batched(args, dev, workload):
     step = GraphStep(plan)
     for _ in range(Wm):
         step.replay()
-    t_ssim = timed(step.replay, K)
+    Ks = min(K, 200)
+    t_ssim = timed(step.replay, Ks)
     (t_ssim,) = max_over_ranks([t_ssim], device=dev)
     del step, plan
-    res["ssim_loss"] = {"loss": "0.7 l1 + 0.3 (1 - SSIM), 11-tap window",
-                        "batched_img_s": round(B_all * K / (t_ssim * 1e-3), 1),
-                        "batched_ms_per_step": round(t_ssim / K, 3)}
+    res["ssim_loss"] = {"loss": "0.7 l1 + 0.3 (1 - SSIM), 11-tap window", "steps": Ks,
+                        "batched_img_s": round(B_all * Ks / (t_ssim * 1e-3), 1),
+                        "batched_ms_per_step": round(t_ssim / Ks, 3)}
     if not args.no_ref_cuda and world == 1:
         ref = ref_cuda_fit_loop(sizes, counts, targets, fields_np, dev,
                                 steps=args.ref_batch_steps, ssim_weight=0.3)
@@ -640,6 +755,59 @@ def run_ssim_profile(dev, H=2048, W=2048, calls=13):
     e.record()
     torch.cuda.synchronize()
     return {"image": f"{W}x{H}", "ms_per_call": round(s.elapsed_time(e) / (calls - 3), 4)}
+
+
+ST_CASES = (  # (name, H, W, tensor sigma): the structure tensors the workloads compute
+    ("plain_fit_256", 256, 256, 2.0), ("stress_2048", 2048, 2048, 3.0),
+    ("placement_1920x1080", 1080, 1920, 2.0))
+
+
+def run_structure_tensor(dev, calls=20):
+    """J = G_rho * (grad I grad I^T) and its eigen-analysis (structure_tensor.compute) on the
+    workloads' targets: ms per call, replayed from a CUDA graph (two shared-memory tile kernels,
+    the radix select of the energy's median and 99th percentile, the labels), against the
+    compulsory HBM traffic (12 B per pixel in, five float32 maps and a uint8 label out: 33 B per
+    pixel); the reference's NumPy computation on the host for the 256x256 and 1920x1080
+    targets."""
+    from structsplat_b200 import structure_tensor as st
+    from structsplat_b200.fit import CapturedStep
+    from structsplat_b200.synthetic import make_target
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
+    out = {"bytes_per_pixel": 33, "peak_gbs": peak}
+    ref_root = REPO / "baseline" / "_ref"
+    ref_st = None
+    if (ref_root / "structsplat" / "structure_tensor.py").is_file():
+        if str(ref_root) not in sys.path:
+            sys.path.insert(0, str(ref_root))
+        from structsplat import structure_tensor as ref_st
+    for name, H, W, rho in ST_CASES:
+        tgt = make_target(H, W, seed=61, n_polygons=60 if W == 1920 else 20)
+        img = torch.tensor(tgt, device=dev)
+        cfg = st.StructureTensorConfig(grad_sigma=1.0, tensor_sigma=rho)
+        # captured once (the call's host-side preparation is not timed: a CUDA graph replays
+        # its kernels)
+        graph = CapturedStep(lambda: st.compute(img, cfg, sync_stats=False), warmup=3)
+        times = []
+        for _ in range(calls):
+            flush_l2(flush)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            graph.replay()
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        del graph
+        ms = statistics.median(times)
+        gbs = 33.0 * H * W / (ms * 1e-3) / 1e9
+        row = {"H": H, "W": W, "grad_sigma": 1.0, "tensor_sigma": rho, "ms": round(ms, 4),
+               "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+        if ref_st is not None and H * W <= 1920 * 1080:
+            t0 = time.perf_counter()
+            ref_st.compute(tgt, ref_st.StructureTensorConfig(grad_sigma=1.0, tensor_sigma=rho))
+            row["reference_numpy_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+        out[name] = row
+    return out
 
 
 def run_stress(args, dev):
@@ -758,12 +926,17 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-cuda", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the parity object (the reference's float32 and float64 results)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fit measurement")
-    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--ref-batch-steps", type=int, default=2)
     ap.add_argument("--batched-only", action="store_true")
     ap.add_argument("--stress", action="store_true", help="run only the stress workload")
-    ap.add_argument("--stress-steps", type=int, default=20)
+    ap.add_argument("--stress-steps", type=int, default=500)
+    ap.add_argument("--no-stress", action="store_true", help="skip the stress leg")
+    ap.add_argument("--no-e2e-fit", action="store_true",
+                    help="skip the placement + fit end-to-end leg")
     ap.add_argument("--e2e-fit", action="store_true",
                     help="run only the placement + fit end-to-end workload")
     ap.add_argument("--e2e-steps", type=int, default=2000)
@@ -847,8 +1020,9 @@ def main():
         return
     batched = run_batched(args, dev, workload) if workload is not None else None
     host = res.pop("host")
+    step_out = res.pop("step_out")
     peaks = measured_peaks()
-    P = pair_count(host) if rank == 0 else 0
+    P = pair_count(host, dev=dev) if rank == 0 else 0
     line = None
     if rank == 0:
         ms = res["total_ms"] / args.steps
@@ -921,6 +1095,17 @@ def main():
                                                                       normalize=False)
         if batched is not None:
             line["batched"] = batched
+        if world == 1 and not args.no_parity:
+            line["parity"] = parity_object(host, dev, step_out["image"], step_out["grads"])
+        del step_out
+        torch.cuda.empty_cache()
+        if world == 1:
+            line["structure_tensor"] = run_structure_tensor(dev)
+        if world == 1 and not args.no_stress:
+            line["stress"] = run_stress(args, dev)
+            torch.cuda.empty_cache()
+        if world == 1 and not args.no_e2e_fit:
+            line["e2e_fit"] = run_e2e_fit(args, dev)
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

@@ -7,10 +7,8 @@
 // or 3x3 Sobel / Scharr correlation with reflect padding), the outer products are summed over
 // channels and blurred again, and the closed-form eigen-analysis gives lam1, lam2, the
 // across-edge angle, coherence and energy.  The flat / edge / corner labels need the energy's
-// median and 99th percentile (float64, NumPy 'linear' interpolation): the energies are
-// radix-sorted on the device and one thread evaluates the statistics.
-#include <cub/device/device_radix_sort.cuh>
-
+// median and 99th percentile (float64, NumPy 'linear' interpolation): four order statistics of
+// the energies found by an exact radix select, then one thread evaluates the statistics.
 #include "ss_common.cuh"
 
 namespace ss {
@@ -115,6 +113,160 @@ __global__ void tensor_kernel(const float* __restrict__ maps, int chans, int H, 
   J[2 * HW + p] = jyy;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Tile kernels: one CTA per 32 x 32 block of output pixels, every intermediate in shared memory.
+//
+// st_tensor_tile: the source maps of the block and a halo (radius of the gradient blur plus one
+// pixel for the gradient stencil) are read once; the axis-0 blur, the axis-1 blur, the gradients
+// and the channel-summed outer products follow in shared memory; J (3 maps) is written.
+// st_eigen_tile: J of the block and a halo of the tensor blur's radius is read once, blurred
+// along axis 0 then axis 1, and the eigen-analysis writes the five maps.  Every value is the
+// same float32 arithmetic, in the same order, as the per-pass kernels above (reflect padding
+// per axis, taps accumulated in order with separately rounded products and sums).
+constexpr int kStTile = 32;
+constexpr int kStThreads = 256;
+constexpr int kStTileMaxRadius = 12;  // larger blurs take the per-pass kernels
+
+// Window of a tile along one axis: [lo, hi) of the image covering the tile [t0, t1) and `halo`
+// on either side (reflected indices of the halo fall inside it).
+struct Span {
+  int lo, hi;
+  __device__ __forceinline__ int len() const { return hi - lo; }
+};
+__device__ __forceinline__ Span span_of(int t0, int t1, int halo, int n) {
+  return Span{max(t0 - halo, 0), min(t1 + halo, n)};
+}
+
+// Blur along axis 0 (ALONG_Y) or axis 1 of a window-resident map: src covers rows sy and
+// columns sx, dst covers oy x ox; indices are image coordinates.  Threads are laid out 32 (x)
+// by 8 (y); reflection (per tap) only where the taps reach past the image edge.
+template <bool ALONG_Y>
+__device__ __forceinline__ void blur_window(const float* src, Span sy, Span sx, float* dst,
+                                            Span oy, Span ox, const Taps& taps, int H, int W) {
+  const int nx = ox.len(), sw = sx.len(), r = taps.r;
+  for (int y = oy.lo + threadIdx.y; y < oy.hi; y += blockDim.y) {
+    for (int x = ox.lo + threadIdx.x; x < ox.hi; x += blockDim.x) {
+      float acc = 0.0f;
+      const bool inside = ALONG_Y ? (y - r >= 0 && y + r < H) : (x - r >= 0 && x + r < W);
+      if (inside) {
+        const float* c = ALONG_Y ? src + (y - r - sy.lo) * sw + (x - sx.lo)
+                                 : src + (y - sy.lo) * sw + (x - r - sx.lo);
+        const int step = ALONG_Y ? sw : 1;
+        for (int k = 0; k <= 2 * r; ++k) acc = __fadd_rn(acc, __fmul_rn(taps.w[k], c[k * step]));
+      } else {
+        for (int k = -r; k <= r; ++k) {
+          const int yy = ALONG_Y ? reflect(y + k, H) : y;
+          const int xx = ALONG_Y ? x : reflect(x + k, W);
+          acc = __fadd_rn(acc, __fmul_rn(taps.w[k + r], src[(yy - sy.lo) * sw + (xx - sx.lo)]));
+        }
+      }
+      dst[(y - oy.lo) * nx + (x - ox.lo)] = acc;
+    }
+  }
+}
+
+template <int CH>
+__global__ void __launch_bounds__(kStThreads)
+    st_tensor_tile(const float* __restrict__ img, int H, int W, int C, int rgb, Taps tg, int op,
+                   float* __restrict__ J) {
+  pdl_wait();
+  pdl_trigger();
+  extern __shared__ float st_smem[];
+  const int x0 = blockIdx.x * kStTile, y0 = blockIdx.y * kStTile;
+  const int x1 = min(x0 + kStTile, W), y1 = min(y0 + kStTile, H);
+  const int rg = tg.r;
+  const Span wy = span_of(y0, y1, rg + 1, H), wx = span_of(x0, x1, rg + 1, W);  // sources
+  const Span gy = span_of(y0, y1, 1, H), gx = span_of(x0, x1, 1, W);            // smoothed
+  const int wn = wy.len() * wx.len(), bn = gy.len() * wx.len(), gn = gy.len() * gx.len();
+  float* S = st_smem;               // CH x window: sources, then the smoothed maps
+  float* B = st_smem + CH * wn;     // CH x (gy x wx): the axis-0 blur
+  const int64_t HW = (int64_t)H * W;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int i = tid; i < wn; i += kStThreads) {
+    const int y = wy.lo + i / wx.len(), x = wx.lo + i % wx.len();
+    const float* px = img + ((int64_t)y * W + x) * C;
+    if (CH == 3) {
+      S[i] = px[0];
+      S[wn + i] = px[1];
+      S[2 * wn + i] = px[2];
+    } else if (C == 1) {
+      S[i] = px[0];
+    } else {  // `img[..., :3] @ luma`: NumPy's float32 dot, a fused multiply-add chain
+      S[i] = __fmaf_rn(px[2], 0.0722f, __fmaf_rn(px[1], 0.7152f, __fmul_rn(px[0], 0.2126f)));
+    }
+  }
+  __syncthreads();
+  const float* G = S;  // the smoothed maps, (gy x gx) each, or the sources when rg == 0
+  Span sgy = wy, sgx = wx;
+  if (rg > 0) {
+#pragma unroll
+    for (int c = 0; c < CH; ++c) blur_window<true>(S + c * wn, wy, wx, B + c * bn, gy, wx, tg, H, W);
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < CH; ++c) blur_window<false>(B + c * bn, gy, wx, S + c * gn, gy, gx, tg, H, W);
+    __syncthreads();
+    sgy = gy;
+    sgx = gx;
+  }
+  const int gw = sgx.len(), gsz = sgy.len() * gw;
+  auto g = [&](int c, int y, int x) { return G[c * gsz + (y - sgy.lo) * gw + (x - sgx.lo)]; };
+  for (int y = y0 + threadIdx.y; y < y1; y += blockDim.y)
+  for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
+    float jxx = 0.f, jxy = 0.f, jyy = 0.f;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      float ix, iy;
+      if (op == 0) {  // np.gradient: central inside, one-sided at the border
+        if (x == 0) ix = __fsub_rn(g(c, y, 1), g(c, y, 0));
+        else if (x == W - 1) ix = __fsub_rn(g(c, y, x), g(c, y, x - 1));
+        else ix = __fsub_rn(g(c, y, x + 1), g(c, y, x - 1)) * 0.5f;
+        if (y == 0) iy = __fsub_rn(g(c, 1, x), g(c, 0, x));
+        else if (y == H - 1) iy = __fsub_rn(g(c, y, x), g(c, y - 1, x));
+        else iy = __fsub_rn(g(c, y + 1, x), g(c, y - 1, x)) * 0.5f;
+      } else {  // 3x3 correlation, reflect padding
+        const float e = op == 1 ? 0.125f : 0.09375f, m = op == 1 ? 0.25f : 0.3125f;
+        const float kx[3][3] = {{-e, 0.f, e}, {-m, 0.f, m}, {-e, 0.f, e}};
+        float ax = 0.f, ay = 0.f;
+        for (int dy = 0; dy < 3; ++dy) {
+          const int yy = reflect(y + dy - 1, H);
+          for (int dx = 0; dx < 3; ++dx) {
+            const float v = g(c, yy, reflect(x + dx - 1, W));
+            ax = __fadd_rn(ax, __fmul_rn(kx[dy][dx], v));
+            ay = __fadd_rn(ay, __fmul_rn(kx[dx][dy], v));
+          }
+        }
+        ix = ax;
+        iy = ay;
+      }
+      jxx = __fadd_rn(jxx, __fmul_rn(ix, ix));
+      jxy = __fadd_rn(jxy, __fmul_rn(ix, iy));
+      jyy = __fadd_rn(jyy, __fmul_rn(iy, iy));
+    }
+    const int64_t p = (int64_t)y * W + x;
+    J[p] = jxx;
+    J[HW + p] = jxy;
+    J[2 * HW + p] = jyy;
+  }
+}
+
+// The eigen-analysis of one pixel's tensor (structure_tensor.py:163-176).
+struct Eigen {
+  float l1, l2, angle, coherence, energy;
+};
+__device__ __forceinline__ Eigen eigen_of(float jxx, float jxy, float jyy) {
+  const float half = __fmul_rn(0.5f, __fadd_rn(jxx, jyy));
+  const float diff = __fmul_rn(0.5f, __fsub_rn(jxx, jyy));
+  const float r = __fsqrt_rn(__fadd_rn(__fmul_rn(diff, diff), __fmul_rn(jxy, jxy)));
+  Eigen e;
+  e.l1 = __fadd_rn(half, r);
+  e.l2 = fmaxf(__fsub_rn(half, r), 0.0f);
+  e.energy = __fadd_rn(e.l1, e.l2);
+  const float coh = __fdiv_rn(__fsub_rn(e.l1, e.l2), __fadd_rn(e.energy, 1e-12f));
+  e.angle = __fmul_rn(0.5f, atan2f(__fmul_rn(2.0f, jxy), __fsub_rn(jxx, jyy)));
+  e.coherence = __fmul_rn(coh, coh);
+  return e;
+}
+
 __global__ void eigen_kernel(const float* __restrict__ J, int64_t HW, float* __restrict__ lam1,
                              float* __restrict__ lam2, float* __restrict__ angle,
                              float* __restrict__ coherence, float* __restrict__ energy,
@@ -123,47 +275,188 @@ __global__ void eigen_kernel(const float* __restrict__ J, int64_t HW, float* __r
   pdl_trigger();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= HW) return;
-  const float jxx = J[p], jxy = J[HW + p], jyy = J[2 * HW + p];
-  const float half = __fmul_rn(0.5f, __fadd_rn(jxx, jyy));
-  const float diff = __fmul_rn(0.5f, __fsub_rn(jxx, jyy));
-  const float r = __fsqrt_rn(__fadd_rn(__fmul_rn(diff, diff), __fmul_rn(jxy, jxy)));
-  const float l1 = __fadd_rn(half, r);
-  const float l2 = fmaxf(__fsub_rn(half, r), 0.0f);
-  const float en = __fadd_rn(l1, l2);
-  const float coh = __fdiv_rn(__fsub_rn(l1, l2), __fadd_rn(en, 1e-12f));
-  lam1[p] = l1;
-  lam2[p] = l2;
-  angle[p] = __fmul_rn(0.5f, atan2f(__fmul_rn(2.0f, jxy), __fsub_rn(jxx, jyy)));
-  coherence[p] = __fmul_rn(coh, coh);
-  energy[p] = en;
-  energy_keys[p] = en;
+  const Eigen e = eigen_of(J[p], J[HW + p], J[2 * HW + p]);
+  lam1[p] = e.l1;
+  lam2[p] = e.l2;
+  angle[p] = e.angle;
+  coherence[p] = e.coherence;
+  energy[p] = e.energy;
+  energy_keys[p] = e.energy;
 }
 
-// NumPy 'linear' quantile of sorted float32 data, in float64 (index (n-1)q, lerp that switches
-// to b - (b-a)(1-t) for t >= 0.5).
-__device__ double quantile_sorted(const float* s, int64_t n, double q) {
-  const double v = (double)(n - 1) * q;
-  int64_t lo = (int64_t)floor(v);
-  if (lo < 0) lo = 0;
-  if (lo > n - 1) lo = n - 1;
-  const int64_t hi = lo + 1 < n ? lo + 1 : n - 1;
-  const double t = v - (double)lo;
-  const double a = fmax((double)s[lo], 0.0), b = fmax((double)s[hi], 0.0);
-  const double d = b - a;
-  return t >= 0.5 ? b - d * (1.0 - t) : a + d * t;
+__global__ void __launch_bounds__(kStThreads)
+    st_eigen_tile(const float* __restrict__ J, int H, int W, Taps tt, float* __restrict__ lam1,
+                  float* __restrict__ lam2, float* __restrict__ angle,
+                  float* __restrict__ coherence, float* __restrict__ energy,
+                  uint32_t* __restrict__ energy_keys) {
+  pdl_wait();
+  pdl_trigger();
+  extern __shared__ float st_smem[];
+  const int x0 = blockIdx.x * kStTile, y0 = blockIdx.y * kStTile;
+  const int x1 = min(x0 + kStTile, W), y1 = min(y0 + kStTile, H);
+  const int rt = tt.r;
+  const Span wy = span_of(y0, y1, rt, H), wx = span_of(x0, x1, rt, W);
+  const Span oy{y0, y1}, ox{x0, x1};
+  const int wn = wy.len() * wx.len(), bn = oy.len() * wx.len(), on = oy.len() * ox.len();
+  float* S = st_smem;              // 3 x window of J, then the blurred maps
+  float* B = st_smem + 3 * wn;     // 3 x (tile rows x window columns)
+  const int64_t HW = (int64_t)H * W;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int i = tid; i < wn; i += kStThreads) {
+    const int64_t p = (int64_t)(wy.lo + i / wx.len()) * W + wx.lo + i % wx.len();
+    S[i] = J[p];
+    S[wn + i] = J[HW + p];
+    S[2 * wn + i] = J[2 * HW + p];
+  }
+  __syncthreads();
+  const float* T = S;
+  Span sy = wy, sx = wx;
+  if (rt > 0) {
+    for (int c = 0; c < 3; ++c) blur_window<true>(S + c * wn, wy, wx, B + c * bn, oy, wx, tt, H, W);
+    __syncthreads();
+    for (int c = 0; c < 3; ++c) blur_window<false>(B + c * bn, oy, wx, S + c * on, oy, ox, tt, H, W);
+    __syncthreads();
+    sy = oy;
+    sx = ox;
+  }
+  const int tw = sx.len(), tsz = sy.len() * tw;
+  for (int y = y0 + threadIdx.y; y < y1; y += blockDim.y)
+  for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
+    const int q = (y - sy.lo) * tw + (x - sx.lo);
+    const Eigen e = eigen_of(T[q], T[tsz + q], T[2 * tsz + q]);
+    const int64_t p = (int64_t)y * W + x;
+    lam1[p] = e.l1;
+    lam2[p] = e.l2;
+    angle[p] = e.angle;
+    coherence[p] = e.coherence;
+    energy[p] = e.energy;
+    energy_keys[p] = __float_as_uint(e.energy);  // >= 0: the bits order like the values
+  }
 }
 
-__global__ void stats_kernel(const float* __restrict__ sorted, int64_t n, double flat_frac,
-                             double* stats) {
+size_t tensor_tile_smem(int rg, int chans) {
+  const int wn = (kStTile + 2 * (rg + 1)) * (kStTile + 2 * (rg + 1));
+  const int bn = (kStTile + 2) * (kStTile + 2 * (rg + 1));
+  return (size_t)chans * (wn + bn) * sizeof(float);
+}
+size_t eigen_tile_smem(int rt) {
+  const int wn = (kStTile + 2 * rt) * (kStTile + 2 * rt);
+  const int bn = kStTile * (kStTile + 2 * rt);
+  return (size_t)3 * (wn + bn) * sizeof(float);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Exact order statistics of the energies (all >= 0, so their float bits order like the values)
+// by a radix select: four passes over 8-bit digits from the top, each building one 256-bin
+// histogram per wanted rank among the keys that share that rank's digits so far, then one
+// thread descending into the bin holding the rank.  kRanks ranks: the median's one or two
+// middle elements and the two elements the 99th percentile interpolates.
+constexpr int kRanks = 4;
+struct SelectState {
+  uint32_t prefix[kRanks];   // digits found so far (high bits)
+  long long rank[kRanks];    // rank still to find among the keys with that prefix
+  uint32_t hist[kRanks][256];
+  unsigned int done;         // CTAs finished with the current pass
+};
+
+// One pass: the histograms of the current digit (keys >> shift & 255) of the keys sharing each
+// rank's prefix; identical digits of a warp are counted with one shared-memory atomic (the
+// energies cluster, so most keys of a pass share a few bins).  The last CTA to finish descends
+// into the bin holding each rank and clears the histograms for the next pass.
+__global__ void select_pass_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift,
+                                   SelectState* __restrict__ st) {
+  pdl_wait();
+  pdl_trigger();
+  __shared__ uint32_t h[kRanks][256];
+  __shared__ uint32_t prefix[kRanks];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
+  if (threadIdx.x < kRanks) prefix[threadIdx.x] = st->prefix[threadIdx.x];
+  __syncthreads();
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int64_t i = base + threadIdx.x;
+    const uint32_t k = i < n ? keys[i] : 0u;
+    const uint32_t high = shift >= 24 ? 0u : (k >> (shift + 8));
+    const uint32_t digit = (k >> shift) & 255u;
+#pragma unroll
+    for (int r = 0; r < kRanks; ++r) {
+      const uint32_t key = (i < n && high == prefix[r]) ? digit : 256u;
+      const unsigned same = __match_any_sync(0xffffffffu, key);
+      if (key < 256u && lane == __ffs(same) - 1) atomicAdd(&h[r][key], (uint32_t)__popc(same));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) {
+    const uint32_t v = (&h[0][0])[i];
+    if (v) atomicAdd(&(&st->hist[0][0])[i], v);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // the complete histograms (read past L1: the other CTAs added them in L2)
+  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x)
+    (&h[0][0])[i] = __ldcg(&(&st->hist[0][0])[i]);
+  __syncthreads();
+  if (threadIdx.x < kRanks) {
+    const int r = threadIdx.x;
+    long long want = st->rank[r];
+    int bin = 0;
+    for (; bin < 255; ++bin) {
+      const long long c = h[r][bin];
+      if (want < c) break;
+      want -= c;
+    }
+    st->prefix[r] = (st->prefix[r] << 8) | (uint32_t)bin;
+    st->rank[r] = want;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0u;
+  if (threadIdx.x == 0) st->done = 0u;
+}
+
+__global__ void select_init_kernel(SelectState* st, int64_t n) {
+  pdl_wait();
+  pdl_trigger();
+  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0u;
+  if (threadIdx.x == 0) {
+    const int64_t lo = (int64_t)floor((double)(n - 1) * 0.99);
+    const int64_t lo_c = lo < 0 ? 0 : (lo > n - 1 ? n - 1 : lo);
+    const long long want[kRanks] = {(long long)((n - 1) / 2), (long long)(n / 2), lo_c,
+                                    lo_c + 1 < n ? lo_c + 1 : n - 1};
+    for (int r = 0; r < kRanks; ++r) {
+      st->prefix[r] = 0u;
+      st->rank[r] = want[r];
+    }
+    st->done = 0u;
+  }
+}
+
+// The statistics from the four selected keys (the same float64 formulas as stats_kernel).
+__global__ void select_stats_kernel(const SelectState* __restrict__ st, int64_t n,
+                                    double flat_frac, double* stats) {
   pdl_wait();
   pdl_trigger();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double med = 0.0;
+  double med = 0.0, p99 = 0.0;
   if (n > 0) {
-    const double a = fmax((double)sorted[(n - 1) / 2], 0.0), b = fmax((double)sorted[n / 2], 0.0);
+    const double a = fmax((double)__uint_as_float(st->prefix[0]), 0.0);
+    const double b = fmax((double)__uint_as_float(st->prefix[1]), 0.0);
     med = (n & 1) ? b : (a + b) / 2.0;
+    const double v = (double)(n - 1) * 0.99;
+    int64_t lo = (int64_t)floor(v);
+    if (lo < 0) lo = 0;
+    if (lo > n - 1) lo = n - 1;
+    const double t = v - (double)lo;
+    const double pa = fmax((double)__uint_as_float(st->prefix[2]), 0.0);
+    const double pb = fmax((double)__uint_as_float(st->prefix[3]), 0.0);
+    const double d = pb - pa;
+    p99 = t >= 0.5 ? pb - d * (1.0 - t) : pa + d * t;
   }
-  const double p99 = n > 0 ? quantile_sorted(sorted, n, 0.99) : 0.0;
   const double ref = fmax(p99, 8.0 * med) + 1e-12;
   stats[0] = ref;
   stats[1] = fmax(flat_frac * ref, 1.5 * med);
@@ -188,20 +481,14 @@ __global__ void label_kernel(const float* __restrict__ energy, const float* __re
 }
 
 struct StWorkspace {
-  float *src, *tmp, *J, *keys;
-  void* sort_temp;
-  size_t sort_bytes;
+  float *src, *tmp, *J;
+  uint32_t* keys;
+  SelectState* select;
 };
-
-size_t sort_temp_bytes(int64_t n) {
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortKeys(nullptr, bytes, (const float*)nullptr, (float*)nullptr, (int)n);
-  return bytes;
-}
 
 size_t st_workspace_bytes(int64_t HW) {
   return 3 * align256(3 * HW * sizeof(float)) + align256(HW * sizeof(float)) +
-         align256(sort_temp_bytes(HW));
+         align256(sizeof(SelectState));
 }
 
 StWorkspace carve_st(void* base, int64_t HW) {
@@ -213,10 +500,9 @@ StWorkspace carve_st(void* base, int64_t HW) {
   p += align256(3 * HW * sizeof(float));
   w.J = reinterpret_cast<float*>(p);
   p += align256(3 * HW * sizeof(float));
-  w.keys = reinterpret_cast<float*>(p);
+  w.keys = reinterpret_cast<uint32_t*>(p);
   p += align256(HW * sizeof(float));
-  w.sort_temp = p;
-  w.sort_bytes = align256(sort_temp_bytes(HW));
+  w.select = reinterpret_cast<SelectState*>(p);
   return w;
 }
 
@@ -277,31 +563,55 @@ int ss_structure_tensor(const float* image, int height, int width, int channels,
   if ((rc = make_taps(taps_tensor, radius_tensor, &tt))) return rc;
   cudaStream_t s = as_stream(stream);
   StWorkspace w = carve_st(workspace, HW);
-  const dim3 blk(32, 8), grd((width + 31) / 32, (height + 7) / 8);
   const int rgb = (color_space == 1 && channels >= 3) ? 1 : 0;
   const int chans = rgb ? 3 : 1;
-  source_maps_kernel<<<grd, blk, 0, s>>>(image, height, width, channels, rgb, w.src);
-  if ((rc = check_launch("structure source maps"))) return rc;
-  const float* smoothed = w.src;
-  if (tg.r > 0) {
-    blur_kernel<true><<<dim3(grd.x, grd.y, chans), blk, 0, s>>>(w.src, w.tmp, height, width, tg);
-    blur_kernel<false><<<dim3(grd.x, grd.y, chans), blk, 0, s>>>(w.tmp, w.src, height, width, tg);
-  }
-  tensor_kernel<<<grd, blk, 0, s>>>(smoothed, chans, height, width, gradient_operator, w.J);
-  if ((rc = check_launch("structure gradients"))) return rc;
-  const float* Jb = w.J;
-  if (tt.r > 0) {
-    blur_kernel<true><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.J, w.tmp, height, width, tt);
-    blur_kernel<false><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.tmp, w.J, height, width, tt);
-  }
   const int lin = (int)((HW + 255) / 256);
-  eigen_kernel<<<lin, 256, 0, s>>>(Jb, HW, lam1, lam2, angle, coherence, energy, w.tmp);
-  if ((rc = check_launch("structure eigen"))) return rc;
-  size_t sb = w.sort_bytes;
-  cudaError_t e = cub::DeviceRadixSort::SortKeys(w.sort_temp, sb, w.tmp, w.keys, (int)HW, 0,
-                                                 32, s);
-  if (e != cudaSuccess) return fail(SS_ERR_CUDA, "energy sort: %s", cudaGetErrorString(e));
-  stats_kernel<<<1, 32, 0, s>>>(w.keys, HW, flat_frac, stats_dev);
+  if (tg.r <= kStTileMaxRadius && tt.r <= kStTileMaxRadius) {
+    // two tile kernels, every intermediate in shared memory
+    const dim3 tiles((width + kStTile - 1) / kStTile, (height + kStTile - 1) / kStTile);
+    const size_t sm1 = tensor_tile_smem(tg.r, chans), sm2 = eigen_tile_smem(tt.r);
+    if (rgb)
+      rc = launch_smem("st_tensor_tile", st_tensor_tile<3>, tiles, dim3(32, 8), sm1, s, image,
+                       height, width, channels, rgb, tg, gradient_operator, w.J);
+    else
+      rc = launch_smem("st_tensor_tile", st_tensor_tile<1>, tiles, dim3(32, 8), sm1, s, image,
+                       height, width, channels, rgb, tg, gradient_operator, w.J);
+    if (rc || (rc = check_launch("structure tensor tiles"))) return rc;
+    rc = launch_smem("st_eigen_tile", st_eigen_tile, tiles, dim3(32, 8), sm2, s,
+                     (const float*)w.J, height, width, tt, lam1, lam2, angle, coherence, energy,
+                     w.keys);
+    if (rc || (rc = check_launch("structure eigen tiles"))) return rc;
+  } else {  // blurs wider than the tiles' halo: one pass per axis in global memory
+    const dim3 blk(32, 8), grd((width + 31) / 32, (height + 7) / 8);
+    source_maps_kernel<<<grd, blk, 0, s>>>(image, height, width, channels, rgb, w.src);
+    if ((rc = check_launch("structure source maps"))) return rc;
+    if (tg.r > 0) {
+      blur_kernel<true><<<dim3(grd.x, grd.y, chans), blk, 0, s>>>(w.src, w.tmp, height, width, tg);
+      blur_kernel<false><<<dim3(grd.x, grd.y, chans), blk, 0, s>>>(w.tmp, w.src, height, width, tg);
+    }
+    tensor_kernel<<<grd, blk, 0, s>>>(w.src, chans, height, width, gradient_operator, w.J);
+    if ((rc = check_launch("structure gradients"))) return rc;
+    if (tt.r > 0) {
+      blur_kernel<true><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.J, w.tmp, height, width, tt);
+      blur_kernel<false><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.tmp, w.J, height, width, tt);
+    }
+    eigen_kernel<<<lin, 256, 0, s>>>(w.J, HW, lam1, lam2, angle, coherence, energy,
+                                     reinterpret_cast<float*>(w.keys));
+    if ((rc = check_launch("structure eigen"))) return rc;
+  }
+  // the energy's median and 99th percentile by an exact radix select
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t want = (HW + 255) / 256;
+  const unsigned hblocks = (unsigned)(want < (int64_t)sms * 4 ? want : (int64_t)sms * 4);
+  launch("select_init_kernel", select_init_kernel, 1, 256, 0, s, w.select, HW);
+  for (int shift = 24; shift >= 0; shift -= 8)
+    launch("select_pass_kernel", select_pass_kernel, hblocks, 256, 0, s,
+           (const uint32_t*)w.keys, HW, shift, w.select);
+  launch("select_stats_kernel", select_stats_kernel, 1, 32, 0, s,
+         (const SelectState*)w.select, HW, flat_frac, stats_dev);
+  if ((rc = check_launch("structure statistics"))) return rc;
   label_kernel<<<lin, 256, 0, s>>>(energy, lam2, HW, stats_dev, corner_frac, label);
   return check_launch("structure labels");
 }

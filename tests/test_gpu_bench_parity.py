@@ -195,3 +195,16 @@ def test_fit_iteration_gradients_match_float64(case_name, deterministic, fused):
         e = rel_err(grads[k], oracle[2][k])
         print(f"  {k}: grad err vs f64 {e:.2e}")
         assert e <= GRAD_TOL, (k, e)
+
+
+def test_benchmark_pair_count_matches_the_oracle():
+    """The benchmark's work unit (in-rectangle pairs, counted from the library's projection)
+    equals the oracle's count on the benchmark and stress fields."""
+    require_cuda()
+    import bench
+    for case in (_benchmark_case(), _stress_case()):
+        H, W, f, _, _ = case
+        host = {"means": f.means, "log_scales": f.log_scales, "rotations": f.rotations}
+        radii = field_ref.radii(torch.tensor(f.log_scales), torch.tensor(f.rotations), 3.0)
+        assert bench.pair_count(host, {"H": H, "W": W}) == c_oracle.pair_count(f.means, radii,
+                                                                              H, W)

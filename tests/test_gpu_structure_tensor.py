@@ -53,3 +53,29 @@ def test_torch_input_and_rgb_channels():
     t_rgb = compute(img, StructureTensorConfig(color_space="rgb"))
     t_luma = compute(img, StructureTensorConfig(color_space="luma"))
     assert float(t_rgb.energy.max()) > 50 * (float(t_luma.energy.max()) + 1e-9)
+
+
+@pytest.mark.parametrize("H, W, grad_sigma, tensor_sigma, op, space", [
+    (70, 97, 1.0, 2.0, "central", "luma"),    # tiles cut by both image edges
+    (129, 33, 1.0, 3.0, "sobel", "rgb"),      # the stress workload's tensor blur
+    (64, 80, 4.5, 2.0, "scharr", "luma"),     # a gradient blur wider than the tiles' halo
+    (40, 52, 0.0, 4.5, "central", "rgb"),     # no gradient blur, a wide tensor blur
+])
+def test_tile_and_per_pass_kernels_match_the_oracle(H, W, grad_sigma, tensor_sigma, op, space):
+    """The shared-memory tile kernels (blur radii up to 12) and the per-pass kernels (wider
+    blurs) against the CPU oracle's restatement of structure_tensor.compute on ragged images:
+    the maps to float32 rounding, the float64 statistics from the exact order statistics."""
+    require_cuda()
+    from oracle import structure_tensor_ref as ref
+    from structsplat_b200.synthetic import make_target
+    img = make_target(H, W, seed=H + W)
+    cfg = StructureTensorConfig(grad_sigma, tensor_sigma, op, space)
+    t = compute(img, cfg)
+    want = ref.compute(img, ref.TensorConfig(grad_sigma=grad_sigma, tensor_sigma=tensor_sigma,
+                                             gradient_operator=op, color_space=space))
+    scale = max(float(np.abs(want.energy).max()), 1e-30)
+    for attr in ("lam1", "lam2", "energy"):
+        err = np.abs(getattr(t, attr).cpu().numpy() - getattr(want, attr)).max() / scale
+        assert err <= 1e-6, (attr, err)
+    assert abs(t.energy_ref - float(want.energy_ref)) <= 1e-6 * float(want.energy_ref)
+    assert (t.label.cpu().numpy() != want.label).mean() <= 1e-3
