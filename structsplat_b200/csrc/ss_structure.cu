@@ -126,6 +126,7 @@ __global__ void tensor_kernel(const float* __restrict__ maps, int chans, int H, 
 constexpr int kStTile = 32;
 constexpr int kStThreads = 256;
 constexpr int kStTileMaxRadius = 12;  // larger blurs take the per-pass kernels
+static_assert(kStTile + 2 * (kStTileMaxRadius + 1) <= 64, "a window row fits two columns per lane");
 
 // Window of a tile along one axis: [lo, hi) of the image covering the tile [t0, t1) and `halo`
 // on either side (reflected indices of the halo fall inside it).
@@ -137,13 +138,32 @@ __device__ __forceinline__ Span span_of(int t0, int t1, int halo, int n) {
   return Span{max(t0 - halo, 0), min(t1 + halo, n)};
 }
 
+// Row pitch of a shared-memory plane whose rows hold n values: odd, so that the lanes of a warp
+// walking down different rows at the same column hit different banks.
+__host__ __device__ __forceinline__ int plane_pitch(int n) { return n | 1; }
+
+// Calls f(row, column) for every element of a window of at most 64 columns (window-relative
+// indices), threads laid out 32 (x) by 8 (y): a warp takes a row, each lane one or two columns.
+// Unrolled so that each thread has several rows' global loads in flight at once.
+template <typename F>
+__device__ __forceinline__ void for_window(Span wy, Span wx, F&& f) {
+  const int wxl = wx.len(), wyl = wy.len();
+  const int c0 = threadIdx.x, c1 = threadIdx.x + 32;
+#pragma unroll 4
+  for (int r = threadIdx.y; r < wyl; r += 8) {
+    if (c0 < wxl) f(r, c0);
+    if (c1 < wxl) f(r, c1);
+  }
+}
+
 // Blur along axis 0 (ALONG_Y) or axis 1 of a window-resident map: src covers rows sy and
-// columns sx, dst covers oy x ox; indices are image coordinates.  Threads are laid out 32 (x)
+// columns sx (row pitch sw), dst covers oy x ox (row pitch nx); indices are image coordinates.  Threads are laid out 32 (x)
 // by 8 (y); reflection (per tap) only where the taps reach past the image edge.
 template <bool ALONG_Y>
-__device__ __forceinline__ void blur_window(const float* src, Span sy, Span sx, float* dst,
-                                            Span oy, Span ox, const Taps& taps, int H, int W) {
-  const int nx = ox.len(), sw = sx.len(), r = taps.r;
+__device__ __forceinline__ void blur_window(const float* src, Span sy, Span sx, int sw,
+                                            float* dst, Span oy, Span ox, int nx,
+                                            const Taps& taps, int H, int W) {
+  const int r = taps.r;
   for (int y = oy.lo + threadIdx.y; y < oy.hi; y += blockDim.y) {
     for (int x = ox.lo + threadIdx.x; x < ox.hi; x += blockDim.x) {
       float acc = 0.0f;
@@ -165,6 +185,62 @@ __device__ __forceinline__ void blur_window(const float* src, Span sy, Span sx, 
   }
 }
 
+// The same blur for a compile-time radius R: each thread takes RO consecutive outputs along
+// the blur axis and holds the RO + 2R source values they need in registers (one load per
+// source value instead of one per tap); the taps are accumulated in the same order.
+template <bool ALONG_Y, int R, int RO>
+__device__ __forceinline__ void blur_window_sliding(const float* src, Span sy, Span sx, int sw,
+                                                    float* dst, Span oy, Span ox, int nx,
+                                                    const Taps& taps, int H, int W) {
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nline = ALONG_Y ? ox.len() : oy.len();
+  const int nalong = ALONG_Y ? oy.len() : ox.len();
+  const int nseg = (nalong + RO - 1) / RO;
+  const Span src_span = ALONG_Y ? sy : sx;
+  const int n_axis = ALONG_Y ? H : W;
+  for (int item = tid; item < nline * nseg; item += kStThreads) {
+    const int line = ALONG_Y ? item % nline : item / nseg;
+    const int seg = ALONG_Y ? item / nline : item % nseg;
+    const int a0 = (ALONG_Y ? oy.lo : ox.lo) + seg * RO;
+    const int a_end = (ALONG_Y ? oy.hi : ox.hi);
+    const int other = (ALONG_Y ? ox.lo : oy.lo) + line;  // the column (ALONG_Y) or the row
+    float win[RO + 2 * R];
+#pragma unroll
+    for (int j = 0; j < RO + 2 * R; ++j) {
+      int c = a0 - R + j;
+      if (c < 0 || c >= n_axis) c = reflect(c, n_axis);
+      c = min(c, src_span.hi - 1);  // sources only the unstored outputs past a_end would use
+      win[j] = ALONG_Y ? src[(c - sy.lo) * sw + (other - sx.lo)]
+                       : src[(other - sy.lo) * sw + (c - sx.lo)];
+    }
+#pragma unroll
+    for (int k = 0; k < RO; ++k) {
+      if (a0 + k < a_end) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(taps.w[j], win[k + j]));
+        const int y = ALONG_Y ? a0 + k : other, x = ALONG_Y ? other : a0 + k;
+        dst[(y - oy.lo) * nx + (x - ox.lo)] = acc;
+      }
+    }
+  }
+}
+
+// Blur dispatch: the register form for the workloads' radii (3: sigma 1; 6: rho 2; 9: rho 3).
+template <bool ALONG_Y>
+__device__ __forceinline__ void blur_any(const float* src, Span sy, Span sx, int sw, float* dst,
+                                         Span oy, Span ox, int nx, const Taps& taps, int H,
+                                         int W) {
+  if (taps.r == 3)
+    blur_window_sliding<ALONG_Y, 3, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+  else if (taps.r == 6)
+    blur_window_sliding<ALONG_Y, 6, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+  else if (taps.r == 9)
+    blur_window_sliding<ALONG_Y, 9, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+  else
+    blur_window<ALONG_Y>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+}
+
 template <int CH>
 __global__ void __launch_bounds__(kStThreads)
     st_tensor_tile(const float* __restrict__ img, int H, int W, int C, int rgb, Taps tg, int op,
@@ -177,14 +253,14 @@ __global__ void __launch_bounds__(kStThreads)
   const int rg = tg.r;
   const Span wy = span_of(y0, y1, rg + 1, H), wx = span_of(x0, x1, rg + 1, W);  // sources
   const Span gy = span_of(y0, y1, 1, H), gx = span_of(x0, x1, 1, W);            // smoothed
-  const int wn = wy.len() * wx.len(), bn = gy.len() * wx.len(), gn = gy.len() * gx.len();
+  const int pw = plane_pitch(wx.len()), pg = plane_pitch(gx.len());
+  const int wn = wy.len() * pw, bn = gy.len() * pw, gn = gy.len() * pg;
   float* S = st_smem;               // CH x window: sources, then the smoothed maps
   float* B = st_smem + CH * wn;     // CH x (gy x wx): the axis-0 blur
   const int64_t HW = (int64_t)H * W;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  for (int i = tid; i < wn; i += kStThreads) {
-    const int y = wy.lo + i / wx.len(), x = wx.lo + i % wx.len();
-    const float* px = img + ((int64_t)y * W + x) * C;
+  for_window(wy, wx, [&](int r, int c) {
+    const int i = r * pw + c;
+    const float* px = img + ((int64_t)(wy.lo + r) * W + wx.lo + c) * C;
     if (CH == 3) {
       S[i] = px[0];
       S[wn + i] = px[1];
@@ -194,21 +270,25 @@ __global__ void __launch_bounds__(kStThreads)
     } else {  // `img[..., :3] @ luma`: NumPy's float32 dot, a fused multiply-add chain
       S[i] = __fmaf_rn(px[2], 0.0722f, __fmaf_rn(px[1], 0.7152f, __fmul_rn(px[0], 0.2126f)));
     }
-  }
+  });
   __syncthreads();
   const float* G = S;  // the smoothed maps, (gy x gx) each, or the sources when rg == 0
   Span sgy = wy, sgx = wx;
+  int gw = pw, gsz = wn;
   if (rg > 0) {
 #pragma unroll
-    for (int c = 0; c < CH; ++c) blur_window<true>(S + c * wn, wy, wx, B + c * bn, gy, wx, tg, H, W);
+    for (int c = 0; c < CH; ++c)
+      blur_any<true>(S + c * wn, wy, wx, pw, B + c * bn, gy, wx, pw, tg, H, W);
     __syncthreads();
 #pragma unroll
-    for (int c = 0; c < CH; ++c) blur_window<false>(B + c * bn, gy, wx, S + c * gn, gy, gx, tg, H, W);
+    for (int c = 0; c < CH; ++c)
+      blur_any<false>(B + c * bn, gy, wx, pw, S + c * gn, gy, gx, pg, tg, H, W);
     __syncthreads();
     sgy = gy;
     sgx = gx;
+    gw = pg;
+    gsz = gn;
   }
-  const int gw = sgx.len(), gsz = sgy.len() * gw;
   auto g = [&](int c, int y, int x) { return G[c * gsz + (y - sgy.lo) * gw + (x - sgx.lo)]; };
   for (int y = y0 + threadIdx.y; y < y1; y += blockDim.y)
   for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
@@ -249,6 +329,13 @@ __global__ void __launch_bounds__(kStThreads)
   }
 }
 
+// The radix-select key of an energy (>= 0): its float bits, which order like the values, with
+// -0 read as +0.
+__device__ __forceinline__ uint32_t energy_key(float e) {
+  const uint32_t k = __float_as_uint(e);
+  return k == 0x80000000u ? 0u : k;
+}
+
 // The eigen-analysis of one pixel's tensor (structure_tensor.py:163-176).
 struct Eigen {
   float l1, l2, angle, coherence, energy;
@@ -269,8 +356,7 @@ __device__ __forceinline__ Eigen eigen_of(float jxx, float jxy, float jyy) {
 
 __global__ void eigen_kernel(const float* __restrict__ J, int64_t HW, float* __restrict__ lam1,
                              float* __restrict__ lam2, float* __restrict__ angle,
-                             float* __restrict__ coherence, float* __restrict__ energy,
-                             float* __restrict__ energy_keys) {
+                             float* __restrict__ coherence, float* __restrict__ energy) {
   pdl_wait();
   pdl_trigger();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,14 +367,13 @@ __global__ void eigen_kernel(const float* __restrict__ J, int64_t HW, float* __r
   angle[p] = e.angle;
   coherence[p] = e.coherence;
   energy[p] = e.energy;
-  energy_keys[p] = e.energy;
 }
 
 __global__ void __launch_bounds__(kStThreads)
     st_eigen_tile(const float* __restrict__ J, int H, int W, Taps tt, float* __restrict__ lam1,
                   float* __restrict__ lam2, float* __restrict__ angle,
                   float* __restrict__ coherence, float* __restrict__ energy,
-                  uint32_t* __restrict__ energy_keys) {
+                  uint32_t* __restrict__ level0_hist) {
   pdl_wait();
   pdl_trigger();
   extern __shared__ float st_smem[];
@@ -297,142 +382,244 @@ __global__ void __launch_bounds__(kStThreads)
   const int rt = tt.r;
   const Span wy = span_of(y0, y1, rt, H), wx = span_of(x0, x1, rt, W);
   const Span oy{y0, y1}, ox{x0, x1};
-  const int wn = wy.len() * wx.len(), bn = oy.len() * wx.len(), on = oy.len() * ox.len();
+  const int pw = plane_pitch(wx.len()), po = plane_pitch(ox.len());
+  const int wn = wy.len() * pw, bn = oy.len() * pw, on = oy.len() * po;
   float* S = st_smem;              // 3 x window of J, then the blurred maps
   float* B = st_smem + 3 * wn;     // 3 x (tile rows x window columns)
   const int64_t HW = (int64_t)H * W;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-  for (int i = tid; i < wn; i += kStThreads) {
-    const int64_t p = (int64_t)(wy.lo + i / wx.len()) * W + wx.lo + i % wx.len();
+  for_window(wy, wx, [&](int r, int c) {
+    const int i = r * pw + c;
+    const int64_t p = (int64_t)(wy.lo + r) * W + wx.lo + c;
     S[i] = J[p];
     S[wn + i] = J[HW + p];
     S[2 * wn + i] = J[2 * HW + p];
-  }
+  });
   __syncthreads();
   const float* T = S;
   Span sy = wy, sx = wx;
+  int tw = pw, tsz = wn;
   if (rt > 0) {
-    for (int c = 0; c < 3; ++c) blur_window<true>(S + c * wn, wy, wx, B + c * bn, oy, wx, tt, H, W);
+    for (int c = 0; c < 3; ++c)
+      blur_any<true>(S + c * wn, wy, wx, pw, B + c * bn, oy, wx, pw, tt, H, W);
     __syncthreads();
-    for (int c = 0; c < 3; ++c) blur_window<false>(B + c * bn, oy, wx, S + c * on, oy, ox, tt, H, W);
+    for (int c = 0; c < 3; ++c)
+      blur_any<false>(B + c * bn, oy, wx, pw, S + c * on, oy, ox, po, tt, H, W);
     __syncthreads();
     sy = oy;
     sx = ox;
+    tw = po;
+    tsz = on;
   }
-  const int tw = sx.len(), tsz = sy.len() * tw;
-  for (int y = y0 + threadIdx.y; y < y1; y += blockDim.y)
-  for (int x = x0 + threadIdx.x; x < x1; x += blockDim.x) {
-    const int q = (y - sy.lo) * tw + (x - sx.lo);
-    const Eigen e = eigen_of(T[q], T[tsz + q], T[2 * tsz + q]);
-    const int64_t p = (int64_t)y * W + x;
-    lam1[p] = e.l1;
-    lam2[p] = e.l2;
-    angle[p] = e.angle;
-    coherence[p] = e.coherence;
-    energy[p] = e.energy;
-    energy_keys[p] = __float_as_uint(e.energy);  // >= 0: the bits order like the values
+  __shared__ uint32_t h0[256];  // the energies' top key bytes (level 0 of the radix select)
+  for (int i = tid; i < 256; i += kStThreads) h0[i] = 0u;
+  __syncthreads();
+  const int x = x0 + threadIdx.x;
+  for (int y = y0 + threadIdx.y; y < y0 + kStTile; y += blockDim.y) {  // warp-uniform
+    const bool in = y < y1 && x < x1;
+    uint32_t digit = 256u;
+    if (in) {
+      const int q = (y - sy.lo) * tw + (x - sx.lo);
+      const Eigen e = eigen_of(T[q], T[tsz + q], T[2 * tsz + q]);
+      const int64_t p = (int64_t)y * W + x;
+      lam1[p] = e.l1;
+      lam2[p] = e.l2;
+      angle[p] = e.angle;
+      coherence[p] = e.coherence;
+      energy[p] = e.energy;
+      digit = energy_key(e.energy) >> 24;
+    }
+    // neighbouring energies share their top byte: one shared-memory atomic per distinct byte
+    const unsigned same = __match_any_sync(0xffffffffu, digit);
+    if (in && (threadIdx.x == __ffs(same) - 1)) atomicAdd(&h0[digit], (uint32_t)__popc(same));
   }
+  __syncthreads();
+  for (int i = tid; i < 256; i += kStThreads)
+    if (h0[i]) atomicAdd(&level0_hist[i], h0[i]);
 }
 
 size_t tensor_tile_smem(int rg, int chans) {
-  const int wn = (kStTile + 2 * (rg + 1)) * (kStTile + 2 * (rg + 1));
-  const int bn = (kStTile + 2) * (kStTile + 2 * (rg + 1));
+  const int side = kStTile + 2 * (rg + 1);
+  const int wn = side * plane_pitch(side), bn = (kStTile + 2) * plane_pitch(side);
   return (size_t)chans * (wn + bn) * sizeof(float);
 }
 size_t eigen_tile_smem(int rt) {
-  const int wn = (kStTile + 2 * rt) * (kStTile + 2 * rt);
-  const int bn = kStTile * (kStTile + 2 * rt);
+  const int side = kStTile + 2 * rt;
+  const int wn = side * plane_pitch(side), bn = kStTile * plane_pitch(side);
   return (size_t)3 * (wn + bn) * sizeof(float);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Exact order statistics of the energies (all >= 0, so their float bits order like the values)
-// by a radix select: four passes over 8-bit digits from the top, each building one 256-bin
-// histogram per wanted rank among the keys that share that rank's digits so far, then one
-// thread descending into the bin holding the rank.  kRanks ranks: the median's one or two
-// middle elements and the two elements the 99th percentile interpolates.
+// Exact order statistics of the energies by a radix select over their float bits (the energies
+// are >= 0, so the bits order like the values; -0 is read as +0).  Level l (0..3) is the 8-bit
+// digit (key >> (24 - 8 l)) & 255; the histogram of level l counts, for each wanted rank, the
+// level-l digits of the keys that share that rank's digits of levels < l (ranks whose prefixes
+// agree share one histogram, the one of the lowest such rank).  The level-0 histogram is built
+// by the eigen tile kernel as it writes the energies; every later pass and the statistics kernel
+// first re-derive the prefixes from the finished lower levels (one warp, a few hundred cycles),
+// so no CTA waits on another.  kRanks ranks: the median's one or two middle elements and the two
+// elements the 99th percentile interpolates.
 constexpr int kRanks = 4;
+constexpr int kLevels = 4;
 struct SelectState {
-  uint32_t prefix[kRanks];   // digits found so far (high bits)
-  long long rank[kRanks];    // rank still to find among the keys with that prefix
-  uint32_t hist[kRanks][256];
-  unsigned int done;         // CTAs finished with the current pass
+  long long want[kRanks];                // rank of each wanted element among all keys
+  uint32_t hist[kLevels][kRanks][256];
 };
 
-// One pass: the histograms of the current digit (keys >> shift & 255) of the keys sharing each
-// rank's prefix; identical digits of a warp are counted with one shared-memory atomic (the
-// energies cluster, so most keys of a pass share a few bins).  The last CTA to finish descends
-// into the bin holding each rank and clears the histograms for the next pass.
-__global__ void select_pass_kernel(const uint32_t* __restrict__ keys, int64_t n, int shift,
+// Copies the finished histograms of levels [0, levels) into shared memory (all threads of the
+// CTA; one batch of independent loads instead of a chain of dependent ones in select_descend).
+__device__ __forceinline__ void select_load(const SelectState* __restrict__ st, int levels,
+                                            uint32_t* hs, int tid, int nthreads) {
+  const uint32_t* src = &st->hist[0][0][0];
+  for (int i = tid; i < levels * kRanks * 256; i += nthreads) hs[i] = __ldcg(src + i);
+}
+
+// The digits of levels [0, levels) of every rank (prefix) and each rank's rank among the keys
+// with that prefix, from the histograms select_load copied to hs; run by one full warp, results
+// in the caller's shared arrays.
+__device__ void select_descend(const SelectState* __restrict__ st, const uint32_t* hs,
+                               int levels, uint32_t* prefix, long long* rank) {
+  const int lane = threadIdx.x & 31;
+  uint32_t pre[kRanks];
+  long long want[kRanks];
+#pragma unroll
+  for (int r = 0; r < kRanks; ++r) {
+    pre[r] = 0u;
+    want[r] = st->want[r];
+  }
+  for (int l = 0; l < levels; ++l) {
+    uint32_t next[kRanks];
+#pragma unroll
+    for (int r = 0; r < kRanks; ++r) {
+      int hr = r;  // the histogram this rank's keys were counted in (prefixes are monotone)
+#pragma unroll
+      for (int q = r - 1; q >= 0; --q)
+        if (pre[q] == pre[r]) hr = q;
+      // lane i holds bins [8 i, 8 i + 8)
+      const uint32_t* bins = hs + (l * kRanks + hr) * 256 + lane * 8;
+      uint32_t c[8];
+      long long sum = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        c[j] = bins[j];
+        sum += c[j];
+      }
+      long long incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const long long excl = incl - sum;
+      // the lane whose bins hold the rank (the last lane when the counts fall short)
+      const unsigned hit = __ballot_sync(0xffffffffu, want[r] < incl);
+      const int owner = hit ? __ffs(hit) - 1 : 31;
+      int bin = 0;
+      long long left = 0;
+      if (lane == owner) {
+        long long w = want[r] - excl;
+        int j = 0;
+        for (; j < 7; ++j) {
+          if (w < (long long)c[j]) break;
+          w -= c[j];
+        }
+        bin = lane * 8 + j;
+        left = w;
+      }
+      bin = __shfl_sync(0xffffffffu, bin, owner);
+      left = __shfl_sync(0xffffffffu, left, owner);
+      next[r] = (pre[r] << 8) | (uint32_t)bin;
+      want[r] = left;
+    }
+#pragma unroll
+    for (int r = 0; r < kRanks; ++r) pre[r] = next[r];
+  }
+  if (lane < kRanks) {
+#pragma unroll
+    for (int r = 0; r < kRanks; ++r)
+      if (lane == r) {
+        prefix[r] = pre[r];
+        rank[r] = want[r];
+      }
+  }
+}
+
+// Adds one key's level-`level` digit to the shared histograms h of every distinct prefix it
+// matches (prefix[] from select_descend; at level 0 every prefix is empty).
+__device__ __forceinline__ void select_count(uint32_t (*h)[256], const uint32_t* prefix,
+                                             int level, uint32_t k) {
+  const int shift = 24 - 8 * level;
+  const uint32_t high = level == 0 ? 0u : (k >> (shift + 8));
+  const uint32_t digit = (k >> shift) & 255u;
+#pragma unroll
+  for (int r = 0; r < kRanks; ++r) {
+    if (r > 0 && prefix[r] == prefix[r - 1]) continue;  // the same keys as rank r - 1
+    if (high == prefix[r]) atomicAdd(&h[r][digit], 1u);
+  }
+}
+
+// Adds a CTA's shared histograms into level `level` of the global state (non-zero bins only).
+__device__ __forceinline__ void select_flush(uint32_t (*h)[256], SelectState* st, int level,
+                                             int tid, int nthreads) {
+  for (int i = tid; i < kRanks * 256; i += nthreads) {
+    const uint32_t v = (&h[0][0])[i];
+    if (v) atomicAdd(&(&st->hist[level][0][0])[i], v);
+  }
+}
+
+__global__ void select_pass_kernel(const float* __restrict__ energy, int64_t n, int level,
                                    SelectState* __restrict__ st) {
   pdl_wait();
   pdl_trigger();
   __shared__ uint32_t h[kRanks][256];
+  __shared__ uint32_t hs[kLevels - 1][kRanks][256];
   __shared__ uint32_t prefix[kRanks];
-  __shared__ bool last;
-  const int lane = threadIdx.x & 31;
+  __shared__ long long rank[kRanks];
   for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
-  if (threadIdx.x < kRanks) prefix[threadIdx.x] = st->prefix[threadIdx.x];
+  select_load(st, level, &hs[0][0][0], threadIdx.x, blockDim.x);
   __syncthreads();
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const int64_t i = base + threadIdx.x;
-    const uint32_t k = i < n ? keys[i] : 0u;
-    const uint32_t high = shift >= 24 ? 0u : (k >> (shift + 8));
-    const uint32_t digit = (k >> shift) & 255u;
+  if (threadIdx.x < 32) select_descend(st, &hs[0][0][0], level, prefix, rank);
+  __syncthreads();
+  uint32_t pre[kRanks];
 #pragma unroll
-    for (int r = 0; r < kRanks; ++r) {
-      const uint32_t key = (i < n && high == prefix[r]) ? digit : 256u;
-      const unsigned same = __match_any_sync(0xffffffffu, key);
-      if (key < 256u && lane == __ffs(same) - 1) atomicAdd(&h[r][key], (uint32_t)__popc(same));
+  for (int r = 0; r < kRanks; ++r) pre[r] = prefix[r];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four keys per load where the energies are 16-byte aligned, two loads in flight
+  const int64_t n4 = (reinterpret_cast<uintptr_t>(energy) & 15) ? 0 : n / 4;
+  const float4* e4 = reinterpret_cast<const float4*>(energy);
+  for (int64_t i = first; i < n4; i += 2 * stride) {
+    const float4 a = __ldg(e4 + i);
+    const bool two = i + stride < n4;
+    const float4 b = two ? __ldg(e4 + i + stride) : make_float4(0.f, 0.f, 0.f, 0.f);
+    select_count(h, pre, level, energy_key(a.x));
+    select_count(h, pre, level, energy_key(a.y));
+    select_count(h, pre, level, energy_key(a.z));
+    select_count(h, pre, level, energy_key(a.w));
+    if (two) {
+      select_count(h, pre, level, energy_key(b.x));
+      select_count(h, pre, level, energy_key(b.y));
+      select_count(h, pre, level, energy_key(b.z));
+      select_count(h, pre, level, energy_key(b.w));
     }
   }
+  for (int64_t i = 4 * n4 + first; i < n; i += stride)
+    select_count(h, pre, level, energy_key(energy[i]));
   __syncthreads();
-  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) {
-    const uint32_t v = (&h[0][0])[i];
-    if (v) atomicAdd(&(&st->hist[0][0])[i], v);
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&st->done, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the complete histograms (read past L1: the other CTAs added them in L2)
-  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x)
-    (&h[0][0])[i] = __ldcg(&(&st->hist[0][0])[i]);
-  __syncthreads();
-  if (threadIdx.x < kRanks) {
-    const int r = threadIdx.x;
-    long long want = st->rank[r];
-    int bin = 0;
-    for (; bin < 255; ++bin) {
-      const long long c = h[r][bin];
-      if (want < c) break;
-      want -= c;
-    }
-    st->prefix[r] = (st->prefix[r] << 8) | (uint32_t)bin;
-    st->rank[r] = want;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0u;
-  if (threadIdx.x == 0) st->done = 0u;
+  select_flush(h, st, level, threadIdx.x, blockDim.x);
 }
 
 __global__ void select_init_kernel(SelectState* st, int64_t n) {
   pdl_wait();
   pdl_trigger();
-  for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&st->hist[0][0])[i] = 0u;
+  for (int i = threadIdx.x; i < kLevels * kRanks * 256; i += blockDim.x)
+    (&st->hist[0][0][0])[i] = 0u;
   if (threadIdx.x == 0) {
     const int64_t lo = (int64_t)floor((double)(n - 1) * 0.99);
     const int64_t lo_c = lo < 0 ? 0 : (lo > n - 1 ? n - 1 : lo);
     const long long want[kRanks] = {(long long)((n - 1) / 2), (long long)(n / 2), lo_c,
                                     lo_c + 1 < n ? lo_c + 1 : n - 1};
-    for (int r = 0; r < kRanks; ++r) {
-      st->prefix[r] = 0u;
-      st->rank[r] = want[r];
-    }
-    st->done = 0u;
+    for (int r = 0; r < kRanks; ++r) st->want[r] = want[r];
   }
 }
 
@@ -441,19 +628,26 @@ __global__ void select_stats_kernel(const SelectState* __restrict__ st, int64_t 
                                     double flat_frac, double* stats) {
   pdl_wait();
   pdl_trigger();
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ uint32_t hs[kLevels][kRanks][256];
+  __shared__ uint32_t key[kRanks];
+  __shared__ long long rank[kRanks];
+  select_load(st, kLevels, &hs[0][0][0], threadIdx.x, blockDim.x);
+  __syncthreads();
+  if (threadIdx.x < 32) select_descend(st, &hs[0][0][0], kLevels, key, rank);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   double med = 0.0, p99 = 0.0;
   if (n > 0) {
-    const double a = fmax((double)__uint_as_float(st->prefix[0]), 0.0);
-    const double b = fmax((double)__uint_as_float(st->prefix[1]), 0.0);
+    const double a = fmax((double)__uint_as_float(key[0]), 0.0);
+    const double b = fmax((double)__uint_as_float(key[1]), 0.0);
     med = (n & 1) ? b : (a + b) / 2.0;
     const double v = (double)(n - 1) * 0.99;
     int64_t lo = (int64_t)floor(v);
     if (lo < 0) lo = 0;
     if (lo > n - 1) lo = n - 1;
     const double t = v - (double)lo;
-    const double pa = fmax((double)__uint_as_float(st->prefix[2]), 0.0);
-    const double pb = fmax((double)__uint_as_float(st->prefix[3]), 0.0);
+    const double pa = fmax((double)__uint_as_float(key[2]), 0.0);
+    const double pb = fmax((double)__uint_as_float(key[3]), 0.0);
     const double d = pb - pa;
     p99 = t >= 0.5 ? pb - d * (1.0 - t) : pa + d * t;
   }
@@ -469,26 +663,37 @@ __global__ void label_kernel(const float* __restrict__ energy, const float* __re
                              uint8_t* __restrict__ label) {
   pdl_wait();
   pdl_trigger();
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= HW) return;
   // The thresholds are Python floats compared against float32 arrays: NumPy casts them to
   // float32 first.
   const float flat_thr = (float)stats[1];
   const float corner_thr = (float)(corner_frac * stats[0]);
-  const bool flat = energy[p] < flat_thr;
-  const bool corner = lam2[p] > corner_thr && !flat;
-  label[p] = flat ? 0 : (corner ? 2 : 1);
+  auto lab = [&](float e, float l2) -> uint8_t {
+    const bool flat = e < flat_thr;
+    const bool corner = l2 > corner_thr && !flat;
+    return flat ? 0 : (corner ? 2 : 1);
+  };
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t first = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // four pixels per thread where every buffer allows it (16-byte loads, a 4-byte store)
+  const bool vec = ((reinterpret_cast<uintptr_t>(energy) | reinterpret_cast<uintptr_t>(lam2)) &
+                    15) == 0 && (reinterpret_cast<uintptr_t>(label) & 3) == 0;
+  const int64_t n4 = vec ? HW / 4 : 0;
+  for (int64_t i = first; i < n4; i += stride) {
+    const float4 e = __ldg(reinterpret_cast<const float4*>(energy) + i);
+    const float4 l = __ldg(reinterpret_cast<const float4*>(lam2) + i);
+    reinterpret_cast<uchar4*>(label)[i] =
+        make_uchar4(lab(e.x, l.x), lab(e.y, l.y), lab(e.z, l.z), lab(e.w, l.w));
+  }
+  for (int64_t p = 4 * n4 + first; p < HW; p += stride) label[p] = lab(energy[p], lam2[p]);
 }
 
 struct StWorkspace {
   float *src, *tmp, *J;
-  uint32_t* keys;
   SelectState* select;
 };
 
 size_t st_workspace_bytes(int64_t HW) {
-  return 3 * align256(3 * HW * sizeof(float)) + align256(HW * sizeof(float)) +
-         align256(sizeof(SelectState));
+  return 3 * align256(3 * HW * sizeof(float)) + align256(sizeof(SelectState));
 }
 
 StWorkspace carve_st(void* base, int64_t HW) {
@@ -500,8 +705,6 @@ StWorkspace carve_st(void* base, int64_t HW) {
   p += align256(3 * HW * sizeof(float));
   w.J = reinterpret_cast<float*>(p);
   p += align256(3 * HW * sizeof(float));
-  w.keys = reinterpret_cast<uint32_t*>(p);
-  p += align256(HW * sizeof(float));
   w.select = reinterpret_cast<SelectState*>(p);
   return w;
 }
@@ -566,6 +769,8 @@ int ss_structure_tensor(const float* image, int height, int width, int channels,
   const int rgb = (color_space == 1 && channels >= 3) ? 1 : 0;
   const int chans = rgb ? 3 : 1;
   const int lin = (int)((HW + 255) / 256);
+  launch("select_init_kernel", select_init_kernel, 1, 256, 0, s, w.select, HW);
+  int first_level = 0;  // the first radix-select level not yet counted
   if (tg.r <= kStTileMaxRadius && tt.r <= kStTileMaxRadius) {
     // two tile kernels, every intermediate in shared memory
     const dim3 tiles((width + kStTile - 1) / kStTile, (height + kStTile - 1) / kStTile);
@@ -579,8 +784,9 @@ int ss_structure_tensor(const float* image, int height, int width, int channels,
     if (rc || (rc = check_launch("structure tensor tiles"))) return rc;
     rc = launch_smem("st_eigen_tile", st_eigen_tile, tiles, dim3(32, 8), sm2, s,
                      (const float*)w.J, height, width, tt, lam1, lam2, angle, coherence, energy,
-                     w.keys);
+                     &w.select->hist[0][0][0]);
     if (rc || (rc = check_launch("structure eigen tiles"))) return rc;
+    first_level = 1;
   } else {  // blurs wider than the tiles' halo: one pass per axis in global memory
     const dim3 blk(32, 8), grd((width + 31) / 32, (height + 7) / 8);
     source_maps_kernel<<<grd, blk, 0, s>>>(image, height, width, channels, rgb, w.src);
@@ -595,8 +801,7 @@ int ss_structure_tensor(const float* image, int height, int width, int channels,
       blur_kernel<true><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.J, w.tmp, height, width, tt);
       blur_kernel<false><<<dim3(grd.x, grd.y, 3), blk, 0, s>>>(w.tmp, w.J, height, width, tt);
     }
-    eigen_kernel<<<lin, 256, 0, s>>>(w.J, HW, lam1, lam2, angle, coherence, energy,
-                                     reinterpret_cast<float*>(w.keys));
+    eigen_kernel<<<lin, 256, 0, s>>>(w.J, HW, lam1, lam2, angle, coherence, energy);
     if ((rc = check_launch("structure eigen"))) return rc;
   }
   // the energy's median and 99th percentile by an exact radix select
@@ -605,14 +810,15 @@ int ss_structure_tensor(const float* image, int height, int width, int channels,
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int64_t want = (HW + 255) / 256;
   const unsigned hblocks = (unsigned)(want < (int64_t)sms * 4 ? want : (int64_t)sms * 4);
-  launch("select_init_kernel", select_init_kernel, 1, 256, 0, s, w.select, HW);
-  for (int shift = 24; shift >= 0; shift -= 8)
-    launch("select_pass_kernel", select_pass_kernel, hblocks, 256, 0, s,
-           (const uint32_t*)w.keys, HW, shift, w.select);
-  launch("select_stats_kernel", select_stats_kernel, 1, 32, 0, s,
+  for (int level = first_level; level < kLevels; ++level)
+    launch("select_pass_kernel", select_pass_kernel, hblocks, 256, 0, s, (const float*)energy,
+           HW, level, w.select);
+  launch("select_stats_kernel", select_stats_kernel, 1, 256, 0, s,
          (const SelectState*)w.select, HW, flat_frac, stats_dev);
   if ((rc = check_launch("structure statistics"))) return rc;
-  label_kernel<<<lin, 256, 0, s>>>(energy, lam2, HW, stats_dev, corner_frac, label);
+  const unsigned lblocks = (unsigned)((HW / 4 + 255) / 256 < (int64_t)sms * 8
+                                          ? (HW / 4 + 255) / 256 + 1 : (int64_t)sms * 8);
+  label_kernel<<<lblocks, 256, 0, s>>>(energy, lam2, HW, stats_dev, corner_frac, label);
   return check_launch("structure labels");
 }
 
