@@ -944,6 +944,8 @@ def main():
     ap.add_argument("--psnr-thresholds", default="30,33,35,36,37,38,39")
     ap.add_argument("--ssim-profile", action="store_true",
                     help="only time the SSIM term on one 2048x2048 image (for ncu)")
+    ap.add_argument("--structure-tensor", action="store_true",
+                    help="only time the structure tensor on its three workloads")
     ap.add_argument("--fused", type=int, default=-1, choices=[-1, 0, 1],
                     help="fit legs: forward, loss and backward in one tile pass (1), two (0), "
                          "or the plan's choice (-1: fused in fast mode); the fwd+bwd step: "
@@ -994,6 +996,11 @@ def main():
         dev = torch.device(f"cuda:{local}")
         torch.cuda.set_device(dev)
         print(json.dumps({"ssim_profile": run_ssim_profile(dev)}))
+        return
+    if args.structure_tensor:
+        dev = torch.device(f"cuda:{local}")
+        torch.cuda.set_device(dev)
+        print(json.dumps({"structure_tensor": run_structure_tensor(dev)}), flush=True)
         return
     if args.stress or args.e2e_fit:
         dev = torch.device(f"cuda:{local}")
