@@ -288,6 +288,28 @@ def run_ours(args, rank, world, dev):
 
     e2e_serial_total = e2e_time(False)
     e2e_total = e2e_time(True)
+
+    # the copies alone (the same bytes, the same streams, nothing else running): the host link's
+    # share of the end-to-end step
+    def copies_ms(direction, reps=10):
+        times = []
+        stream = h2d if direction == "h2d" else d2h
+        for _ in range(reps):
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            with torch.cuda.stream(stream):
+                if direction == "h2d":
+                    for k in names:
+                        slots[0][0][k].copy_(pinned[k], non_blocking=True)
+                    slots[0][1].copy_(pinned["grad_out"], non_blocking=True)
+                else:
+                    for k in names:
+                        host_grads[k].copy_(grads[k], non_blocking=True)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            times.append(t0.elapsed_time(t1))
+        return statistics.median(times)
+    h2d_ms, d2h_ms = copies_ms("h2d"), copies_ms("d2h")
     # the split, overlapped steps give the gradients of the one-graph step
     step.replay()
     torch.cuda.synchronize()
@@ -301,11 +323,13 @@ def run_ours(args, rank, world, dev):
     step.replay()
     torch.cuda.synchronize()
     step_out = {"image": plan.image.clone(), "grads": {k: v.clone() for k, v in grads.items()}}
-    stats = torch.tensor([total_ms, e2e_total, e2e_serial_total], dtype=torch.float64, device=dev)
+    stats = torch.tensor([total_ms, e2e_total, e2e_serial_total, h2d_ms, d2h_ms],
+                         dtype=torch.float64, device=dev)
     if world > 1:
         torch.distributed.all_reduce(stats, op=torch.distributed.ReduceOp.MAX)
     return {"total_ms": float(stats[0]), "e2e_total_ms": float(stats[1]),
-            "e2e_serial_total_ms": float(stats[2]), "step_ms": step_ms,
+            "e2e_serial_total_ms": float(stats[2]), "h2d_ms": float(stats[3]),
+            "d2h_ms": float(stats[4]), "step_ms": step_ms,
             "fused": plan.use_fused(), "additive_ms": statistics.median(additive_ms),
             "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
             "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
@@ -533,8 +557,20 @@ def run_batched(args, dev, workload):
         torch.cuda.synchronize()
         return s.elapsed_time(e)
 
+    # the launch shape (tile size, backward warps) by the autotuner, timed on this workload; the
+    # batched plan and the per-image loops below all use it
+    tuned = None
+    if not args.no_tune:
+        from structsplat_b200 import autotune
+        fp = fresh()
+        tuned = autotune.tune_fit(sizes, counts, Batch.concat_fields(fp),
+                                  Batch(sizes, counts, device=dev).concat_images(targets),
+                                  settings, use_cache=False)
+        del fp
+    ts = tuned.tile_size if tuned else 32
+
     # batched: one plan for every image, one graph per step
-    batch = Batch(sizes, counts, device=dev)
+    batch = Batch(sizes, counts, tile_size=ts, device=dev)
     fb = fresh()
     plan = FitPlan(batch, Batch.concat_fields(fb), batch.concat_images(targets), settings)
     step = GraphStep(plan)
@@ -554,7 +590,7 @@ def run_batched(args, dev, workload):
     fl = fresh()
     plans = []
     for b in range(B):
-        bb = Batch([sizes[b]], [counts[b]], device=dev)
+        bb = Batch([sizes[b]], [counts[b]], tile_size=ts, device=dev)
         plans.append(FitPlan(bb, fl[b], targets[b].reshape(-1, 3), settings))
 
     def loop_step():
@@ -601,6 +637,11 @@ def run_batched(args, dev, workload):
         "gpu_launches_per_step": 8, "peak_mem_gb": round(mem_gb, 2), "clocks": clocks.summary(),
     }
     res["speedup_vs_loop_eager"] = round(res["batched_img_s"] / res["loop_eager_img_s"], 3)
+    if tuned is not None:
+        from structsplat_b200 import autotune
+        res["autotune"] = autotune.describe(tuned)
+    else:
+        res["autotune"] = "off (--no-tune): 32-px tiles, default backward warps"
     res["loop_graph_steps"] = Kg
     # Fast mode sums the moments with float atomics, so two runs of the same fit drift apart by
     # rounding over the steps; the deterministic mode's batched and per-image fits are bitwise
@@ -614,7 +655,7 @@ def run_batched(args, dev, workload):
     _, dloss = dplan.render()
     del dstep, dplan
     fdl = fresh()
-    dplans = [FitPlan(Batch([sizes[b]], [counts[b]], device=dev), fdl[b],
+    dplans = [FitPlan(Batch([sizes[b]], [counts[b]], tile_size=ts, device=dev), fdl[b],
                       targets[b].reshape(-1, 3), dset) for b in range(B)]
     t_det_loop = timed(lambda: [p.step() for p in dplans], Kd)
     dl = [float(p.render()[1][0, 1]) for p in dplans]
@@ -931,6 +972,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-fit measurement")
     ap.add_argument("--batch-steps", type=int, default=1000)
     ap.add_argument("--ref-batch-steps", type=int, default=2)
+    ap.add_argument("--no-tune", action="store_true",
+                    help="batched leg: fixed 32-px tiles instead of the autotuner's shape")
     ap.add_argument("--batched-only", action="store_true")
     ap.add_argument("--stress", action="store_true", help="run only the stress workload")
     ap.add_argument("--stress-steps", type=int, default=500)
@@ -1090,7 +1133,15 @@ def main():
                               "copy stream into one of two device input slots (step i+1's "
                               "copies run under step i), the forward waits for the field, the "
                               "backward for grad_out; gradients D2H on a third stream",
-                    "serial_ms_per_step": round(res["e2e_serial_total_ms"] / args.steps, 4)},
+                    "serial_ms_per_step": round(res["e2e_serial_total_ms"] / args.steps, 4),
+                    "h2d_alone_ms": round(res["h2d_ms"], 4),
+                    "d2h_alone_ms": round(res["d2h_ms"], 4),
+                    "h2d_gbs": round(res["bi"] / (res["h2d_ms"] * 1e-3) / 1e9, 2),
+                    "d2h_gbs": round(res["bo"] / (res["d2h_ms"] * 1e-3) / 1e9, 2),
+                    # the slowest of the three overlapped legs bounds a step
+                    "bound_ms": round(max(res["h2d_ms"], res["d2h_ms"], ms), 4),
+                    "frac_of_bound": round(max(res["h2d_ms"], res["d2h_ms"], ms) /
+                                           (res["e2e_total_ms"] / args.steps), 4)},
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(host)

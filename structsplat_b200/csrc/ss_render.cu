@@ -93,7 +93,8 @@ constexpr float kUnderflowQ = 230.0f;  // q beyond which every weight is +0 (174
 // where every weight underflows: exp(-q/2) < 2^-126, which ex2.approx.ftz returns as +0, when
 // q > 174.7.  Such a block is not covered when the exact minimum of q over the covered pixels
 // exceeds kUnderflowQ, a margin of 30% for the rounding of q in either evaluation; adding the
-// zero weights would leave every sum unchanged.
+// zero weights would leave every sum unchanged.  Only for a finite opacity and colour: an
+// infinite one times a zero weight is NaN, which the full evaluation keeps.
 __device__ __forceinline__ unsigned block_cover(const float4 (*st)[4], int j, const int4& b,
                                                 int sx0, int sy0) {
   const int x0 = min(max(b.x - sx0, 0), 8), x1 = min(max(b.z - sx0, 0), 8);
@@ -102,22 +103,24 @@ __device__ __forceinline__ unsigned block_cover(const float4 (*st)[4], int j, co
   const unsigned ym = ((1u << y1) - 1u) & ~((1u << y0) - 1u);
   if (!xm || !ym) return 0u;
   if (b.z - b.x > kFarRect || b.w - b.y > kFarRect) {
-    const float4 p0 = st[j][0], p2 = st[j][2];  // (mx, my, ·, ·), (·, a, b, c)
+    // (mx, my, ·, ·), (·, op, r, g), (b, a, b, c)
+    const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
     const float qmin = rect_min_q(p0.x, p0.y, p2.y, p2.z, p2.w, (float)(sx0 + x0),
                                   (float)(sx0 + x1 - 1), (float)(sy0 + y0),
                                   (float)(sy0 + y1 - 1));
-    if (qmin > kUnderflowQ) return 0u;
+    const bool finite = isfinite(p1.y) && isfinite(p1.z) && isfinite(p1.w) && isfinite(p2.x);
+    if (qmin > kUnderflowQ && finite) return 0u;
   }
   return xm | (ym << 8);
 }
 
 // Ballot of the staged entries [0, min(m, 32)) covering the block at (sx0, sy0); lane l also
-// gets entry l's cover.
-__device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int sx0, int sy0,
-                                              int lane, unsigned& cover) {
+// gets entry l's cover.  The rectangles come from `rects` when given, else from the records.
+__device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], const int4* rects, int m,
+                                              int sx0, int sy0, int lane, unsigned& cover) {
   cover = 0u;
   if (lane < m) {
-    const int4 b = *reinterpret_cast<const int4*>(&st[lane][3]);
+    const int4 b = rects ? rects[lane] : *reinterpret_cast<const int4*>(&st[lane][3]);
     cover = block_cover(st, lane, b, sx0, sy0);
   }
   return __ballot_sync(0xffffffffu, cover != 0u);
@@ -128,15 +131,20 @@ __device__ __forceinline__ unsigned hit_cover(const float4 (*st)[4], int m, int 
 constexpr int kStageAll = 512;
 
 // Issues the copies of entries [k0, k0+m) into `dst` with NT threads: 16-byte piece (q & 3) of
-// entry (q >> 2) for q = threadIdx.x, threadIdx.x + NT, …
+// entry (q >> 2) for q = threadIdx.x, threadIdx.x + NT, …  With `rect_dst` the rectangles
+// (piece 3) go to that packed array instead: the lanes of a warp reading 32 consecutive
+// entries' rectangles then hit distinct banks (at the 64-byte record stride every fourth
+// entry shares a bank group).
 template <int NT>
 __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
                                             const TileList& L, int64_t k0, int m,
-                                            int* gid_dst = nullptr) {
+                                            int* gid_dst = nullptr, int4* rect_dst = nullptr) {
   for (int q = threadIdx.x; q < 4 * m; q += NT) {
     const int slot = q >> 2, piece = q & 3;
     const int g = L.gid(k0 + slot);
-    cp_async16(&dst[slot][piece], reinterpret_cast<const float4*>(rec + g) + piece);
+    void* to = (rect_dst && piece == 3) ? static_cast<void*>(&rect_dst[slot])
+                                        : static_cast<void*>(&dst[slot][piece]);
+    cp_async16(to, reinterpret_cast<const float4*>(rec + g) + piece);
     if (gid_dst && piece == 0) gid_dst[slot] = g;  // the backward's atomics need the id
   }
 }
@@ -240,10 +248,12 @@ __device__ __forceinline__ void eval4(const float4 (*st)[4], const uint32_t* q, 
 }
 
 // Appends the hits among staged slots [slot0, slot0 + min(cnt, 32)) to the list q[0..qn).
-__device__ __forceinline__ int enqueue_hits(const float4 (*st)[4], int slot0, int cnt, int sx0,
-                                            int sy0, int lane, uint32_t* q, int qn) {
+__device__ __forceinline__ int enqueue_hits(const float4 (*st)[4], const int4* rects, int slot0,
+                                            int cnt, int sx0, int sy0, int lane, uint32_t* q,
+                                            int qn) {
   unsigned cover;
-  const unsigned hits = hit_cover(st + slot0, cnt, sx0, sy0, lane, cover);
+  const unsigned hits = hit_cover(st + slot0, rects ? rects + slot0 : nullptr, cnt, sx0, sy0,
+                                  lane, cover);
   if (cover) q[qn + __popc(hits & ((1u << lane) - 1u))] = (uint32_t)(slot0 + lane) | (cover << 16);
   return qn + __popc(hits);
 }
@@ -382,8 +392,9 @@ __device__ __forceinline__ float4 finish_pixel(const float* a, int64_t p, float 
 
 // Shared memory of the forward kernel (dynamic): the stage (whole lists up to kStageAll
 // records, or two halves of it for a streamed list) followed by every warp's carry slots and
-// the null record; every warp's hit list; and per warp an 8x8 tile of pixels (RGB rows, then
-// den) through which a block leaves as whole float4 image rows.  One warp per 8x8 block.
+// the null record; the staged records' rectangles, packed; and every warp's hit list, which
+// after the block's last evaluation holds the block's 8x8 pixels (RGB rows, then den) on their
+// way out as whole float4 image rows.  One warp per 8x8 block.
 template <int TS>
 struct FwdSmem {
   static constexpr int kWarps = (TS / 8) * (TS / 8);
@@ -391,11 +402,13 @@ struct FwdSmem {
   static constexpr int kSlots = kNullSlot + 1;
   static constexpr int kListLen = kStageAll + 4;  // a whole stage's hits and padding
   static constexpr size_t kStageBytes = (size_t)kSlots * 4 * sizeof(float4);
+  static constexpr size_t kRectBytes = (size_t)kStageAll * sizeof(int4);
   static constexpr size_t kListBytes = (size_t)kWarps * kListLen * sizeof(uint32_t);
-  static constexpr size_t kTileBytes = (size_t)kWarps * 8 * 32 * sizeof(float);
-  static constexpr size_t kListOff = kStageBytes;
-  static constexpr size_t kTileOff = kListOff + kListBytes;
-  static constexpr size_t kBytes = kTileOff + kTileBytes;
+  static constexpr size_t kRectOff = kStageBytes;
+  static constexpr size_t kListOff = kRectOff + kRectBytes;
+  static constexpr size_t kBytes = kListOff + kListBytes;
+  static_assert(kListLen * sizeof(uint32_t) >= 8 * 32 * sizeof(float), "a block's pixels fit");
+  static_assert(kListLen * sizeof(uint32_t) % 16 == 0 && kListOff % 16 == 0, "float4 rows");
 };
 
 // Accumulates one warp's 8x8 block over a tile's list, staged whole by the caller (who also
@@ -413,7 +426,8 @@ __device__ __forceinline__ void accumulate_block(float4 (*stage)[4], int stage_s
                                                  int carry0, int null_slot, bool active, int sx0,
                                                  int sy0, int lane, float tail,
                                                  float2 (&acc)[4][4], bool staged_whole,
-                                                 bool exact, bool chunk0_issued = false) {
+                                                 bool exact, bool chunk0_issued = false,
+                                                 int4* rects = nullptr) {
   const float fx = (float)(sx0 + (lane & 7)), fy0 = (float)sy0;
   int qn = 0;
   if (staged_whole) {  // the caller staged the list and passed the barrier
@@ -421,7 +435,7 @@ __device__ __forceinline__ void accumulate_block(float4 (*stage)[4], int stage_s
     if (active) {
       const bool listed = qcap >= m + 4;
       for (int base = 0; base < m; base += 32) {
-        qn = enqueue_hits(stage, base, m - base, sx0, sy0, lane, q, qn);
+        qn = enqueue_hits(stage, rects, base, m - base, sx0, sy0, lane, q, qn);
         if (!listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
       }
       drain<FADE>(stage, q, qn, true, exact, null_slot, lane, fx, fy0, tail, acc);
@@ -434,13 +448,14 @@ __device__ __forceinline__ void accumulate_block(float4 (*stage)[4], int stage_s
   const int nchunks = (int)((count + half - 1) / half);
   auto len = [&](int64_t k0) { return (int)(count - k0 < half ? count - k0 : half); };
   if (!chunk0_issued) {
-    stage_range<NT>(stage, rec, L, 0, len(0));
+    stage_range<NT>(stage, rec, L, 0, len(0), nullptr, rects);
     cp_async_commit();
   }
   for (int c = 0; c < nchunks; ++c) {
     const int64_t k0 = (int64_t)c * half;
-    if (c + 1 < nchunks) stage_range<NT>(stage + ((c + 1) & 1) * half, rec, L, k0 + half,
-                                         len(k0 + half));
+    if (c + 1 < nchunks)
+      stage_range<NT>(stage + ((c + 1) & 1) * half, rec, L, k0 + half, len(k0 + half), nullptr,
+                      rects ? rects + ((c + 1) & 1) * half : nullptr);
     cp_async_commit();
     cp_async_wait_one();
     __syncthreads();
@@ -448,7 +463,7 @@ __device__ __forceinline__ void accumulate_block(float4 (*stage)[4], int stage_s
     exact = exact || !all_regular<NT>(stage + s0, m);
     if (active) {
       for (int base = 0; base < m; base += 32) {
-        qn = enqueue_hits(stage, s0 + base, m - base, sx0, sy0, lane, q, qn);
+        qn = enqueue_hits(stage, rects, s0 + base, m - base, sx0, sy0, lane, q, qn);
         if (!listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
       }
       if (listed) qn = drain<FADE>(stage, q, qn, false, exact, null_slot, lane, fx, fy0, tail, acc);
@@ -487,6 +502,7 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sx0 = tx0 + (warp % (TS / 8)) * 8, sy0 = ty0 + (warp / (TS / 8)) * 8;
   uint32_t* q = reinterpret_cast<uint32_t*>(fwd_smem + S::kListOff) + warp * S::kListLen;
+  int4* rects = reinterpret_cast<int4*>(fwd_smem + S::kRectOff);
   const TileList L = tile_list(gids, offsets, cap, fr, tile);
   const bool whole = L.count <= kStageAll;
   if (threadIdx.x == 0) write_null_record(stage, S::kNullSlot);
@@ -497,7 +513,7 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
     for (int ch = 0; ch < 4; ++ch) acc[k][ch] = make_float2(0.f, 0.f);
   bool exact = false;
   if (whole) {
-    stage_range<NT>(stage, rec, L, 0, (int)L.count);
+    stage_range<NT>(stage, rec, L, 0, (int)L.count, nullptr, rects);
     cp_async_commit();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
@@ -505,7 +521,7 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
   }
   accumulate_block<NT, FADE>(stage, kStageAll, rec, L, q, S::kListLen,
                              kStageAll + warp * kCarrySlots, S::kNullSlot, true, sx0, sy0, lane,
-                             tail, acc, whole, exact);
+                             tail, acc, whole, exact, false, rects);
   float v[2][4];
   combine_groups(acc, lane, v);
   const int cx = lane & 7, r0 = block_first_row(lane);
@@ -516,8 +532,10 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
     const bool vec = sx0 + 8 <= W && sy0 + 8 <= H && (W & 3) == 0 && (p_row0 & 3) == 0 &&
                      ((reinterpret_cast<uintptr_t>(out) | reinterpret_cast<uintptr_t>(den)) & 15) == 0;
     if (vec) {
-      // the warp's 8 rows of 32 floats: 24 interleaved RGB, then 8 den
-      float* tb = reinterpret_cast<float*>(fwd_smem + S::kTileOff) + warp * 256;
+      // the warp's 8 rows of 32 floats: 24 interleaved RGB, then 8 den, in the warp's list
+      // (every lane has read its last hit: the reduce-scatter above is warp-synchronous)
+      __syncwarp();
+      float* tb = reinterpret_cast<float*>(q);
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const float inv = 1.0f / (v[k][3] + eps);
@@ -621,7 +639,7 @@ __device__ __forceinline__ float4 render_pixel_grad(int normalize, const float* 
   const float gr = go[3 * p], gg = go[3 * p + 1], gb = go[3 * p + 2];
   if (!normalize) return make_float4(gr, gg, gb, 0.f);
   // the backward prologue's arithmetic (backward_kernel), so the pixel inputs agree bitwise
-  return make_float4(gr / denom, gg / denom, gb / denom, -(gr * o[0] + gg * o[1] + gb * o[2]) / denom);
+  return make_float4(gr * inv, gg * inv, gb * inv, -(gr * o[0] + gg * o[1] + gb * o[2]) * inv);
 }
 
 // finish_pixel with the loss kind and normalisation chosen at run time (uniform per launch).
@@ -738,12 +756,12 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       if (!PIXGRAD && normalize) {
         const int x = tx0 + (q % TS), y = ty0 + (q / TS);
         if (x < W && y < H) {
-          const float denom = dn[i] + eps;
+          const float inv = 1.0f / (dn[i] + eps);
           const float gr = v.x, gg = v.y, gb = v.z;
-          v.x = gr / denom;
-          v.y = gg / denom;
-          v.z = gb / denom;
-          v.w = -(gr * o0[i] + gg * o1[i] + gb * o2[i]) / denom;
+          v.x = gr * inv;
+          v.y = gg * inv;
+          v.z = gb * inv;
+          v.w = -(gr * o0[i] + gg * o1[i] + gb * o2[i]) * inv;
         }
       }
       pix[q] = v;

@@ -475,26 +475,28 @@ __device__ __forceinline__ void select_load(const SelectState* __restrict__ st, 
 }
 
 // The digits of levels [0, levels) of every rank (prefix) and each rank's rank among the keys
-// with that prefix, from the histograms select_load copied to hs; run by one full warp, results
-// in the caller's shared arrays.
+// with that prefix, from the histograms select_load copied to hs.  Warp r takes rank r; the
+// ranks' prefixes meet in the shared arrays after each level (a rank counted in the histogram
+// of the lowest rank sharing its prefix).  Every thread of the CTA calls it (at least kRanks
+// warps); results in the caller's shared arrays prefix and rank.
 __device__ void select_descend(const SelectState* __restrict__ st, const uint32_t* hs,
                                int levels, uint32_t* prefix, long long* rank) {
-  const int lane = threadIdx.x & 31;
-  uint32_t pre[kRanks];
-  long long want[kRanks];
-#pragma unroll
-  for (int r = 0; r < kRanks; ++r) {
-    pre[r] = 0u;
-    want[r] = st->want[r];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x < kRanks) {
+    prefix[threadIdx.x] = 0u;
+    rank[threadIdx.x] = st->want[threadIdx.x];
   }
+  __syncthreads();
   for (int l = 0; l < levels; ++l) {
-    uint32_t next[kRanks];
-#pragma unroll
-    for (int r = 0; r < kRanks; ++r) {
+    uint32_t next = 0u;
+    long long left = 0;
+    if (warp < kRanks) {
+      const int r = warp;
+      const uint32_t pre = prefix[r];
+      const long long want = rank[r];
       int hr = r;  // the histogram this rank's keys were counted in (prefixes are monotone)
-#pragma unroll
       for (int q = r - 1; q >= 0; --q)
-        if (pre[q] == pre[r]) hr = q;
+        if (prefix[q] == pre) hr = q;
       // lane i holds bins [8 i, 8 i + 8)
       const uint32_t* bins = hs + (l * kRanks + hr) * 256 + lane * 8;
       uint32_t c[8];
@@ -512,12 +514,11 @@ __device__ void select_descend(const SelectState* __restrict__ st, const uint32_
       }
       const long long excl = incl - sum;
       // the lane whose bins hold the rank (the last lane when the counts fall short)
-      const unsigned hit = __ballot_sync(0xffffffffu, want[r] < incl);
+      const unsigned hit = __ballot_sync(0xffffffffu, want < incl);
       const int owner = hit ? __ffs(hit) - 1 : 31;
       int bin = 0;
-      long long left = 0;
       if (lane == owner) {
-        long long w = want[r] - excl;
+        long long w = want - excl;
         int j = 0;
         for (; j < 7; ++j) {
           if (w < (long long)c[j]) break;
@@ -528,19 +529,14 @@ __device__ void select_descend(const SelectState* __restrict__ st, const uint32_
       }
       bin = __shfl_sync(0xffffffffu, bin, owner);
       left = __shfl_sync(0xffffffffu, left, owner);
-      next[r] = (pre[r] << 8) | (uint32_t)bin;
-      want[r] = left;
+      next = (pre << 8) | (uint32_t)bin;
     }
-#pragma unroll
-    for (int r = 0; r < kRanks; ++r) pre[r] = next[r];
-  }
-  if (lane < kRanks) {
-#pragma unroll
-    for (int r = 0; r < kRanks; ++r)
-      if (lane == r) {
-        prefix[r] = pre[r];
-        rank[r] = want[r];
-      }
+    __syncthreads();  // every rank has read this level's prefixes
+    if (warp < kRanks && lane == 0) {
+      prefix[warp] = next;
+      rank[warp] = left;
+    }
+    __syncthreads();
   }
 }
 
@@ -578,8 +574,7 @@ __global__ void select_pass_kernel(const float* __restrict__ energy, int64_t n, 
   for (int i = threadIdx.x; i < kRanks * 256; i += blockDim.x) (&h[0][0])[i] = 0u;
   select_load(st, level, &hs[0][0][0], threadIdx.x, blockDim.x);
   __syncthreads();
-  if (threadIdx.x < 32) select_descend(st, &hs[0][0][0], level, prefix, rank);
-  __syncthreads();
+  select_descend(st, &hs[0][0][0], level, prefix, rank);
   uint32_t pre[kRanks];
 #pragma unroll
   for (int r = 0; r < kRanks; ++r) pre[r] = prefix[r];
@@ -633,8 +628,7 @@ __global__ void select_stats_kernel(const SelectState* __restrict__ st, int64_t 
   __shared__ long long rank[kRanks];
   select_load(st, kLevels, &hs[0][0][0], threadIdx.x, blockDim.x);
   __syncthreads();
-  if (threadIdx.x < 32) select_descend(st, &hs[0][0][0], kLevels, key, rank);
-  __syncthreads();
+  select_descend(st, &hs[0][0][0], kLevels, key, rank);
   if (threadIdx.x != 0) return;
   double med = 0.0, p99 = 0.0;
   if (n > 0) {

@@ -184,6 +184,43 @@ def test_nonfinite_means_are_dropped():
     assert torch.isfinite(img).all() and torch.equal(img, one)
 
 
+@pytest.mark.parametrize("normalize", [True, False])
+def test_infinite_colour_on_a_large_rectangle_gives_the_reference_nans(normalize):
+    """An elongated Gaussian (rectangle > 48 px) with an infinite colour channel: where its
+    weight underflows to 0 the reference's product 0 * inf is NaN, so the block skip for
+    underflowed weights must not drop it.  NaN pattern and finite values as the oracle."""
+    require_cuda()
+    from oracle import render_ref
+    H = W = 96
+    ang = np.float32(np.pi / 4)
+    sx, sy = np.float32(30.0), np.float32(1.2)  # standard deviations along / across
+    c, s = np.cos(ang), np.sin(ang)
+    cov = np.array([[c * c * sx * sx + s * s * sy * sy, c * s * (sx * sx - sy * sy)],
+                    [c * s * (sx * sx - sy * sy), s * s * sx * sx + c * c * sy * sy]])
+    inv = np.linalg.inv(cov)
+    conic = np.array([[inv[0, 0], inv[0, 1], inv[1, 1]]], np.float32)
+    rad = np.ceil(3.0 * np.sqrt(np.diag(cov))).astype(np.int64)[None, :]
+    means = np.array([[48.3, 47.6]], np.float32)
+    colors = np.array([[np.inf, 0.5, 0.25]], np.float32)
+    img = render_b200(cuda(means), cuda(conic), cuda(colors), cuda(rad), H, W,
+                      normalize=normalize).cpu()
+    ref = render_ref.render(torch.tensor(means), torch.tensor(conic), torch.tensor(colors),
+                            torch.tensor(rad), H, W, normalize=normalize)
+    assert int(rad.max()) > 24  # a rectangle wider than 48 px
+    nan_ref, nan_img = torch.isnan(ref), torch.isnan(img)
+    assert nan_ref.sum() > 1000
+    assert not (nan_ref & ~nan_img).any()  # every NaN of the reference
+    # the only other NaNs: pixels whose reference weight is subnormal (inf there), which the
+    # flush-to-zero exponential returns as 0 (0 * inf)
+    extra = nan_img & ~nan_ref
+    assert torch.isinf(ref[extra]).all() and extra.sum() <= 0.1 * nan_ref.sum()
+    fin = torch.isfinite(ref) & torch.isfinite(img)
+    assert torch.equal(fin, torch.isfinite(ref))  # the finite channels stay finite
+    # along the major axis the conic's terms (~150 each 30 px out) cancel to q ~ 1, so both
+    # float32 evaluations carry ~1e-5 relative error in the weight there
+    assert rel_err(img[fin], ref[fin]) <= 1e-4
+
+
 def test_zero_sized_image():
     require_cuda()
     m = torch.tensor([[1.0, 1.0]], device="cuda")
