@@ -166,20 +166,24 @@ __device__ __forceinline__ void stage_range(float4 (*dst)[4], const Splat* rec,
 constexpr int kQueueLen = 40;   // per-batch queue: ≥ 3 pending + 32 new hits + 3 padding
 constexpr int kCarrySlots = 4;  // per warp: staged slots for pending hits across a refill
 
-// Row offsets of the fast evaluation: kRowOff.v[rows][k] = (k, k + 4) for the rows of the
-// pair that the 8-bit row mask covers, and kRowMasked for the others.  Added to dy0, a masked
+// Row offsets of the fast evaluation: for row pair k (rows k and k + 4) the row's index when
+// the 8-bit row mask covers it, and kRowMasked when not.  Added to dy0, a masked
 // row's dy becomes so large that qc dy^2 overflows to -inf and its weight is exactly +0, so
 // the pair needs no per-pixel select.  Valid for regular records only (below).
 constexpr float kRowMasked = 1e30f;
 struct RowOffsets {
-  float2 v[256][4];
+  // v[rows][h] = the pairs k = 2h and 2h + 1 as (k, k + 4, k + 1, k + 5): two 16-byte loads
+  float4 v[256][2];
 };
+constexpr float row_offset(int m, int row) { return ((m >> row) & 1) ? (float)row : kRowMasked; }
 constexpr RowOffsets make_row_offsets() {
   RowOffsets t{};
   for (int m = 0; m < 256; ++m)
-    for (int k = 0; k < 4; ++k) {
-      t.v[m][k].x = ((m >> k) & 1) ? (float)k : kRowMasked;
-      t.v[m][k].y = ((m >> (k + 4)) & 1) ? (float)(k + 4) : kRowMasked;
+    for (int h = 0; h < 2; ++h) {
+      t.v[m][h].x = row_offset(m, 2 * h);
+      t.v[m][h].y = row_offset(m, 2 * h + 4);
+      t.v[m][h].z = row_offset(m, 2 * h + 1);
+      t.v[m][h].w = row_offset(m, 2 * h + 5);
     }
   return t;
 }
@@ -227,9 +231,12 @@ __device__ __forceinline__ void eval4(const float4 (*st)[4], const uint32_t* q, 
   const float2 dy02 = make_float2(dy0, dy0);
   const float2 cr2 = make_float2(p1.z, p1.z), cg2 = make_float2(p1.w, p1.w);
   const float2 cb2 = make_float2(cb, cb);
+  float4 o4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const float2 off = EXACT ? make_float2((float)k, (float)(k + 4)) : kRowOff.v[rows][k];
+    if (!EXACT && (k & 1) == 0) o4 = kRowOff.v[rows][k >> 1];
+    const float2 off = EXACT ? make_float2((float)k, (float)(k + 4))
+                             : ((k & 1) ? make_float2(o4.z, o4.w) : make_float2(o4.x, o4.y));
     const float2 dy = __fadd2_rn(dy02, off);
     const float2 t = __ffma2_rn(qc2, dy, bdx2);
     const float2 qq = __ffma2_rn(dy, t, adx22);
