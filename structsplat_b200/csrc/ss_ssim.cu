@@ -327,14 +327,27 @@ __global__ void __launch_bounds__(kTileThreads)
   const int c = blockIdx.y;  // one channel per CTA: a single load phase each
   float ssum = 0.f;
   {
-    for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
+    // the tile and its halo: a fixed trip count, unrolled, so that every load of a thread is
+    // in flight before the first is used
+    constexpr int kIters = (R * R + kTileThreads - 1) / kTileThreads;
+    float v[kIters], t[kIters];
+#pragma unroll
+    for (int k = 0; k < kIters; ++k) {
+      const int i = threadIdx.x + k * kTileThreads;
       const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
-      const bool in = x >= 0 && x < W && y >= 0 && y < H;
+      const bool in = i < R * R && x >= 0 && x < W && y >= 0 && y < H;
       const int64_t q = fr.pixel_base + (int64_t)y * W + x;
-      const float v = in ? img[3 * q + c] : 0.f, t = in ? tgt[3 * q + c] : 0.f;
-      src[0][i] = v;
-      src[1][i] = v * v;
-      src[2][i] = v * t;
+      v[k] = in ? img[3 * q + c] : 0.f;
+      t[k] = in ? tgt[3 * q + c] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kIters; ++k) {
+      const int i = threadIdx.x + k * kTileThreads;
+      if (i < R * R) {
+        src[0][i] = v[k];
+        src[1][i] = v[k] * v[k];
+        src[2][i] = v[k] * t[k];
+      }
     }
     __syncthreads();
     for (int w = threadIdx.x; w < R * kGroups; w += kTileThreads) {
@@ -404,12 +417,27 @@ __global__ void __launch_bounds__(kTileThreads)
   const int H = fr.H, W = fr.W;
   const int c = blockIdx.y;
   const float inv_n = 1.0f / (float)(3 * (int64_t)H * W);
-  for (int i = threadIdx.x; i < R * R; i += kTileThreads) {
-    const int xx = tx0 - kRadius + i % R, yy = ty0 - kRadius + i / R;
-    const bool in = xx >= 0 && xx < W && yy >= 0 && yy < H;
-    const int64_t q = fr.pixel_base + (int64_t)yy * W + xx;
+  {
+    // unrolled like the maps kernel's staging: every load in flight before the first store
+    constexpr int kIters = (R * R + kTileThreads - 1) / kTileThreads;
+    float a[kIters][3];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) sm[m][i] = in ? abc[(int64_t)(3 * c + m) * P + q] : 0.f;
+    for (int k = 0; k < kIters; ++k) {
+      const int i = threadIdx.x + k * kTileThreads;
+      const int xx = tx0 - kRadius + i % R, yy = ty0 - kRadius + i / R;
+      const bool in = i < R * R && xx >= 0 && xx < W && yy >= 0 && yy < H;
+      const int64_t q = fr.pixel_base + (int64_t)yy * W + xx;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) a[k][m] = in ? abc[(int64_t)(3 * c + m) * P + q] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kIters; ++k) {
+      const int i = threadIdx.x + k * kTileThreads;
+      if (i < R * R) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) sm[m][i] = a[k][m];
+      }
+    }
   }
   __syncthreads();
   for (int w = threadIdx.x; w < R * kGroups; w += kTileThreads) {
