@@ -205,6 +205,29 @@ def run_ours(args, rank, world, dev):
         eager()
     eager_ms = timed_loop(eager, args.steps, flush)
 
+    # ---- render_field(mode="b200") on precomputed conics / radii / opacities: the call the
+    # reference's fit loop makes (fit.py:1043-1056), against its render_cuda_exact arms ----
+    from structsplat_b200 import render_field
+    from structsplat_b200.field import project
+    n = params["means"].shape[0]
+    _, conics0, radii0 = project(params["means"], params["log_scales"], params["rotations"],
+                                 params["colors"], params["opacity_logits"], H, W,
+                                 want_conics=True)
+    rf_leaves = [params["means"].clone().requires_grad_(True), conics0.requires_grad_(True),
+                 params["colors"].clone().requires_grad_(True),
+                 torch.sigmoid(params["opacity_logits"]).requires_grad_(True)]
+
+    def eager_rf():
+        img = render_field(rf_leaves[0], rf_leaves[1], rf_leaves[2], radii0, H, W,
+                           mode="b200" if normalize else "b200_additive",
+                           opacities=rf_leaves[3])
+        return torch.autograd.grad(img, rf_leaves, grad_out)
+
+    for _ in range(args.warmup):
+        eager_rf()
+    eager_rf_ms = timed_loop(eager_rf, args.steps, flush)
+    del rf_leaves, conics0, radii0, n
+
     # ---- dominant kernels alone, CUDA events on the launching stream ----
     kt = {}
     for name, fn in (("forward", plan.render), ("backward_kernel", lambda: plan.backward_tiles(grad_out)),
@@ -331,7 +354,8 @@ def run_ours(args, rank, world, dev):
             "e2e_serial_total_ms": float(stats[2]), "h2d_ms": float(stats[3]),
             "d2h_ms": float(stats[4]), "step_ms": step_ms,
             "fused": plan.use_fused(), "additive_ms": statistics.median(additive_ms),
-            "eager_ms": statistics.median(eager_ms), "kernels_ms": kt, "entries": entries,
+            "eager_ms": statistics.median(eager_ms),
+            "eager_rf_ms": statistics.median(eager_rf_ms), "kernels_ms": kt, "entries": entries,
             "launches": launches_per_step * args.steps, "bi": bi, "bo": bo,
             "clocks": clocks.summary(), "host": host, "step_out": step_out}
 
@@ -798,6 +822,16 @@ def run_ssim_profile(dev, H=2048, W=2048, calls=13):
     return {"image": f"{W}x{H}", "ms_per_call": round(s.elapsed_time(e) / (calls - 3), 4)}
 
 
+def st_fp32_slots_per_pixel(grad_sigma: float, tensor_sigma: float) -> int:
+    """FP32 issue slots per pixel of the structure tensor of a luma image with central
+    gradients: blur taps are a separately rounded multiply and add each (NumPy's order), radii
+    round(3 sigma) as structure_tensor.py:61-65 sizes them."""
+    rg = max(1, int(round(3.0 * grad_sigma))) if grad_sigma > 0 else 0
+    rt = max(1, int(round(3.0 * tensor_sigma))) if tensor_sigma > 0 else 0
+    luma, grads, products, eigen = 3, 4, 6, 50
+    return luma + 2 * (2 * rg + 1) * 2 + grads + products + 3 * 2 * (2 * rt + 1) * 2 + eigen
+
+
 ST_CASES = (  # (name, H, W, tensor sigma): the structure tensors the workloads compute
     ("plain_fit_256", 256, 256, 2.0), ("stress_2048", 2048, 2048, 3.0),
     ("placement_1920x1080", 1080, 1920, 2.0))
@@ -814,8 +848,14 @@ def run_structure_tensor(dev, calls=20):
     from structsplat_b200.fit import CapturedStep
     from structsplat_b200.synthetic import make_target
     peak = measured_peaks().get("hbm_gbs") or 6650.0
+    f_mhz = measured_peaks().get("sm_max_mhz") or 1965.0
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)
-    out = {"bytes_per_pixel": 33, "peak_gbs": peak}
+    out = {"bytes_per_pixel": 33, "peak_gbs": peak,
+           "fp32_work": "separately rounded multiply and add per blur tap (NumPy's order), per "
+                        "pixel of a luma image: luma 3, sigma blur 2x(2r+1)x2, central "
+                        "gradients 4, products 6, rho blur 3x2x(2r+1)x2, eigen-analysis ~50 "
+                        "(square root, division, atan2f); peak 148 SMs x 128 FP32 lanes x "
+                        "sm_max_mhz"}
     ref_root = REPO / "baseline" / "_ref"
     ref_st = None
     if (ref_root / "structsplat" / "structure_tensor.py").is_file():
@@ -841,8 +881,14 @@ def run_structure_tensor(dev, calls=20):
         del graph
         ms = statistics.median(times)
         gbs = 33.0 * H * W / (ms * 1e-3) / 1e9
+        slots = st_fp32_slots_per_pixel(1.0, rho)
+        fp32_ms = slots * H * W / (SM_COUNT * FP32_LANES * f_mhz * 1e6) * 1e3
+        hbm_ms = 33.0 * H * W / (peak * 1e9) * 1e3
         row = {"H": H, "W": W, "grad_sigma": 1.0, "tensor_sigma": rho, "ms": round(ms, 4),
-               "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4)}
+               "achieved_gbs": round(gbs, 1), "hbm_frac": round(gbs / peak, 4),
+               "fp32_slots_per_pixel": slots, "fp32_frac": round(fp32_ms / ms, 4),
+               "bound": "fp32" if fp32_ms > hbm_ms else "hbm",
+               "roofline_frac": round(max(fp32_ms, hbm_ms) / ms, 4)}
         if ref_st is not None and H * W <= 1920 * 1080:
             t0 = time.perf_counter()
             ref_st.compute(tgt, ref_st.StructureTensorConfig(grad_sigma=1.0, tensor_sigma=rho))
@@ -1123,6 +1169,7 @@ def main():
             "backward_kernel_roofline_frac": round(bwd_ach / peak_slots, 4),
             "kernels_ms": {k: round(v, 4) for k, v in kt.items()},
             "eager_autograd_ms_per_step": round(res["eager_ms"], 4),
+            "eager_render_field_ms_per_step": round(res["eager_rf_ms"], 4),
             "forward_roofline_frac": round(fwd_ach / peak_slots, 4),
             "step_roofline_frac": round(t_bound_ms / ms, 4),
             "clocks": clk,
