@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kThreads)
   const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t first = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x - lane);
-  if (DETERMINISTIC) {
+  if constexpr (DETERMINISTIC) {
     for (int64_t base = first; base < n; base += stride) {
       const int64_t g = base + lane;
       const bool active = g < n;
@@ -120,8 +120,7 @@ __global__ void __launch_bounds__(kThreads)
       load_grad_in(rec, log_scales, rotations, logits, g, in);
       store_grads(in, g, dilation, logits != nullptr, grad);
     }
-    return;
-  }
+  } else {
   for (int64_t base = first; base < n; base += 2 * stride) {
     const int64_t g[2] = {base + lane, base + stride + lane};
     GradIn in[2];
@@ -139,6 +138,7 @@ __global__ void __launch_bounds__(kThreads)
       for (int k = 0; k < kMoments; ++k) moments[k * n + g[u]] = 0.0f;
       store_grads(in[u], g[u], dilation, logits != nullptr, grad);
     }
+  }
   }
 }
 

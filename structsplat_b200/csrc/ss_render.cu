@@ -673,7 +673,7 @@ template <int TS, int NT, bool FUSED>
 struct BwdSmem {
   static constexpr int kStageMax = Tiling<TS>::kBwdStageAll;
   static constexpr int kWarps = NT / 32;
-  static constexpr int kNullSlot = kStageMax + kWarps * kCarrySlots;  // fused pass only
+  // fused pass only: every warp's carry slots, then the null record (slot kSlots - 1)
   static constexpr int kSlots = kStageMax + (FUSED ? kWarps * kCarrySlots + 1 : 0);
   static constexpr size_t kPixOff = (size_t)kSlots * 4 * sizeof(float4);
   static constexpr size_t kGidOff = kPixOff + (size_t)TS * TS * sizeof(float4);
@@ -915,7 +915,8 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     constexpr int kPer = (kBlocks + kWarps - 1) / kWarps;
     uint32_t* q = reinterpret_cast<uint32_t*>(bwd_smem + S::kQueueOff) + warp * kQueueLen;
     const bool whole = L.count <= kStageMax;
-    if (threadIdx.x == 0) write_null_record(stage, S::kNullSlot);
+    constexpr int kNullSlot = S::kSlots - 1;
+    if (threadIdx.x == 0) write_null_record(stage, kNullSlot);
     bool exact = false;
     if (whole) {
       asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -935,7 +936,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
 #pragma unroll
         for (int ch = 0; ch < 4; ++ch) acc[k][ch] = make_float2(0.f, 0.f);
       accumulate_block<NT, FADE>(stage, kStageMax, rec, L, q, kQueueLen,
-                                 kStageMax + warp * kCarrySlots, S::kNullSlot, active, tx0 + bx,
+                                 kStageMax + warp * kCarrySlots, kNullSlot, active, tx0 + bx,
                                  ty0 + by, lane, tail, acc, whole, exact, i == 0);
       if (!active) continue;
       float v[2][4];
