@@ -1041,6 +1041,8 @@ def main():
                          "one tile pass only with 1")
     ap.add_argument("--dependent-launch", type=int, default=1, choices=[0, 1],
                     help="programmatic dependent launch of the library's kernels (1: on)")
+    ap.add_argument("--forward-chunk", type=int, default=0, choices=[0, 64, 128, 256],
+                    help="records per streamed forward chunk (0: the library's default)")
     ap.add_argument("--profile", action="store_true",
                     help="only replay the captured step (for ncu launch lists)")
     args = ap.parse_args()
@@ -1048,6 +1050,8 @@ def main():
     if args.impl == "ours":
         from structsplat_b200 import _native
         _native.call("ss_set_dependent_launch", args.dependent_launch)
+        for ts in (16, 32):
+            _native.call("ss_set_forward_chunk", ts, args.forward_chunk)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -203,6 +203,13 @@ int ss_render_forward(const void* records, int64_t n, const int32_t* tile_gids,
 int ss_set_backward_warps(int tile_size, int warps);
 int ss_get_backward_warps(int tile_size);
 
+/* Launch tuning (process-wide): records per streamed chunk of the forward for a render tile
+ * size — 64, 128 or 256, 0 restores the default (256).  Only tile lists longer than the
+ * forward's 512-record stage stream; images do not depend on it.  ss_get_forward_chunk returns
+ * the value in effect (-1 for an unsupported tile size). */
+int ss_set_forward_chunk(int tile_size, int records);
+int ss_get_forward_chunk(int tile_size);
+
 /* Workspace of ss_render_backward: per-Gaussian moment accumulators (36 B per Gaussian) or,
  * deterministic, per-entry partials (48 B per entry of capacity); height and width are unused. */
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,

@@ -68,6 +68,8 @@ SIGNATURES = {
     "ss_set_dependent_launch": [_int],
     "ss_get_dependent_launch": [],
     "ss_get_backward_warps": [_int],
+    "ss_set_forward_chunk": [_int, _int],
+    "ss_get_forward_chunk": [_int],
     "ss_render_backward_workspace_bytes": [_i64, _i64, _int, _int, _int, _szp],
     "ss_render_backward": [_vp, _vp, _i64, _vp, _vp, _vp, _i64, _vp, _int, _int, _int, _int,
                            _f32, _f32, _int, _vp, _vp, _vp, _vp, _int, _vp, ctypes.c_size_t, _vp,

@@ -6,7 +6,10 @@ workload picks, by timing on the GPU it runs on, among
 * render tile 16 or 32 (pixels per CTA; also the staging depth: a 32x32 tile stages its whole
   list up to 512 Gaussians for the forward and 448 for the backward, a 16x16 tile up to 512,
   longer lists stream through 64-record chunks), and
-* warps per backward CTA (4 or 8 for tile 16, 8 or 16 for tile 32).
+* warps per backward CTA (4 or 8 for tile 16, 8 or 16 for tile 32), and
+* when the workload's longest tile list is longer than the forward's 512-record stage (the
+  list then streams through two chunks), the forward's chunk depth: 64, 128 or 256 records,
+  timed at the chosen shape.
 
 The forward's threads follow the tile (one warp per 8x8 block).  Timing runs the render forward
 and backward of the actual workload (the field and images in hand), median of a few CUDA-event
@@ -29,6 +32,8 @@ import torch
 from . import _native
 
 CANDIDATES = ((16, 4), (16, 8), (32, 8), (32, 16))
+CHUNKS = (64, 128, 256)  # forward records per streamed chunk
+STAGE_RECORDS = 512      # the forward's whole-list stage
 
 
 @dataclass
@@ -38,10 +43,12 @@ class TuneResult:
     key: str
     times_ms: dict = field(default_factory=dict)
     cached: bool = False
+    forward_chunk: int = 0  # 0: the library's default (lists short enough not to stream)
 
     def apply(self):
-        """Make this shape the one the library launches (the warps knob is process-wide)."""
+        """Make this shape the one the library launches (the knobs are process-wide)."""
         _native.call("ss_set_backward_warps", self.tile_size, self.backward_warps)
+        _native.call("ss_set_forward_chunk", self.tile_size, self.forward_chunk)
         return self
 
 
@@ -60,7 +67,7 @@ def _load():
 def _store(key, result: TuneResult):
     data = _load()
     data[key] = {"tile_size": result.tile_size, "backward_warps": result.backward_warps,
-                 "times_ms": result.times_ms}
+                 "forward_chunk": result.forward_chunk, "times_ms": result.times_ms}
     try:
         p = cache_path()
         p.parent.mkdir(parents=True, exist_ok=True)
@@ -104,27 +111,44 @@ def _time(fn, repeats: int) -> float:
     return statistics.median(times)
 
 
-def _pick(key, candidates, build, repeats, use_cache) -> TuneResult:
+def _pick(key, candidates, build, repeats, use_cache, longest=None) -> TuneResult:
+    """The fastest (tile, warps) candidate; then, when ``longest(ts)`` (the longest tile list
+    at that tile size) exceeds the forward's stage, the fastest forward chunk at that shape."""
     if use_cache:
         hit = _load().get(key)
         if hit and (hit["tile_size"], hit["backward_warps"]) in set(candidates):
             return TuneResult(hit["tile_size"], hit["backward_warps"], key, hit["times_ms"],
-                              cached=True).apply()
-    before = {ts: _native.lib().ss_get_backward_warps(ts) for ts in (16, 32)}
+                              cached=True, forward_chunk=hit.get("forward_chunk", 0)).apply()
+    before = {ts: (_native.lib().ss_get_backward_warps(ts),
+                   _native.lib().ss_get_forward_chunk(ts)) for ts in (16, 32)}
     times = {}
+    chunk = 0
     try:
         for ts, warps in candidates:
             _native.call("ss_set_backward_warps", ts, warps)
             times[f"{ts}x{warps}"] = round(_time(build(ts), repeats), 4)
+        best = min(times, key=times.get)
+        ts, warps = (int(v) for v in best.split("x"))
+        if longest is not None and longest(ts) > STAGE_RECORDS:
+            _native.call("ss_set_backward_warps", ts, warps)
+            chunk_times = {}
+            for c in CHUNKS:
+                _native.call("ss_set_forward_chunk", ts, c)
+                chunk_times[c] = round(_time(build(ts), repeats), 4)
+                times[f"{ts}x{warps}/chunk{c}"] = chunk_times[c]
+            chunk = min(chunk_times, key=chunk_times.get)
     finally:
-        for ts, w in before.items():
-            _native.call("ss_set_backward_warps", ts, w)
-    best = min(times, key=times.get)
-    ts, warps = (int(v) for v in best.split("x"))
-    result = TuneResult(ts, warps, key, times).apply()
+        for t, (w, c) in before.items():
+            _native.call("ss_set_backward_warps", t, w)
+            _native.call("ss_set_forward_chunk", t, c)
+    result = TuneResult(ts, warps, key, times, forward_chunk=chunk).apply()
     if use_cache:
         _store(key, result)
     return result
+
+
+def _longest(offsets: torch.Tensor) -> int:
+    return int((offsets[1:] - offsets[:-1]).max().item()) if offsets.numel() > 1 else 0
 
 
 def tune_render(params: dict, H: int, W: int, grad_out: torch.Tensor, normalize: bool = True,
@@ -146,7 +170,8 @@ def tune_render(params: dict, H: int, W: int, grad_out: torch.Tensor, normalize:
     entries = int(plans[candidates[0][0]].offsets[-1].item())
     key = workload_key(H * W, params["means"].shape[0], entries, 1, normalize, False,
                        deterministic, fit=False)
-    return _pick(key, candidates, build, repeats, use_cache)
+    return _pick(key, candidates, build, repeats, use_cache,
+                 longest=lambda ts: _longest(plans[ts].offsets))
 
 
 def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
@@ -181,7 +206,9 @@ def tune_fit(sizes, counts, params: dict, target: torch.Tensor, settings=None,
         key = workload_key(pixels, sum(counts), entries, len(sizes), settings.normalize,
                            settings.fade_alpha > 0, settings.deterministic, fit=True,
                            fused=settings.use_fused())
-        return _pick(key, candidates, build, repeats, use_cache)
+        # the fused fit pass streams through the backward's stage, which has no chunk knob
+        longest = None if settings.use_fused() else (lambda ts: _longest(plans[ts].offsets))
+        return _pick(key, candidates, build, repeats, use_cache, longest=longest)
     finally:
         for plan in plans.values():  # the probe backward added into the moments: clear them
             plan.bwd_ws.zero_()

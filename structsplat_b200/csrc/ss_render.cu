@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
                    int64_t cap, const int32_t* __restrict__ offsets, Frames frames, float eps,
                    float tail, float* __restrict__ out, float* __restrict__ den,
                    const float* __restrict__ target, float4* __restrict__ pixel_grad,
-                   float* __restrict__ loss, float charb_eps2) {
+                   float* __restrict__ loss, float charb_eps2, int chunk) {
   pdl_wait();
   pdl_trigger();
   using S = FwdSmem<TS>;
@@ -526,7 +526,8 @@ __global__ void __launch_bounds__(Tiling<TS>::kFwdThreads, 2)
     __syncthreads();
     exact = !all_regular<NT>(stage, (int)L.count);
   }
-  accumulate_block<NT, FADE>(stage, kStageAll, rec, L, q, S::kListLen,
+  // a streamed list moves through two chunks of `chunk` records (at most half the stage)
+  accumulate_block<NT, FADE>(stage, 2 * chunk, rec, L, q, S::kListLen,
                              kStageAll + warp * kCarrySlots, S::kNullSlot, true, sx0, sy0, lane,
                              tail, acc, whole, exact, false, rects);
   float v[2][4];
@@ -1179,16 +1180,22 @@ int check_render_args(int64_t n, int H, int W, int ts, float eps) {
   return SS_OK;
 }
 
+// Records per streamed chunk of the forward (lists longer than the stage): a process-wide
+// tuning knob per tile size (0 = half the stage).  Results do not depend on it.
+std::atomic<int> g_forward_chunk[2] = {{0}, {0}};
+
 template <int TS, bool NORM, bool FADE>
 void launch_forward_loss(int loss_kind, unsigned T, cudaStream_t s, const Splat* rec, int64_t n,
                          const int32_t* gids, int64_t cap, const int32_t* offsets,
                          const Frames& f, float eps, float tail, float* out, float* den,
                          const float* target, float4* pixel_grad, float* loss, float ce2) {
   constexpr int NT = Tiling<TS>::kFwdThreads;
+  const int c = g_forward_chunk[TS == 16 ? 0 : 1].load(std::memory_order_relaxed);
+  const int chunk = c ? c : kStageAll / 2;
 #define SS_FWD(LOSS)                                                                          \
   launch_smem("forward_kernel", forward_kernel<TS, NORM, FADE, LOSS>, T, NT,                  \
               FwdSmem<TS>::kBytes, s, rec, n, gids, cap, offsets, f, eps, tail, out, den,      \
-              target, pixel_grad, loss, ce2)
+              target, pixel_grad, loss, ce2, chunk)
   switch (loss_kind) {
     case kL1: SS_FWD(kL1); break;
     case kL2: SS_FWD(kL2); break;
@@ -1462,6 +1469,22 @@ int ss_get_backward_warps(int tile_size) {
   if (tile_size != 16 && tile_size != 32) return -1;
   const int w = g_backward_warps[tile_size == 16 ? 0 : 1].load(std::memory_order_relaxed);
   return w ? w : 8;
+}
+
+int ss_set_forward_chunk(int tile_size, int records) {
+  if (tile_size != 16 && tile_size != 32)
+    return fail(SS_ERR_UNSUPPORTED, "render tile_size must be 16 or 32, got %d", tile_size);
+  if (records != 0 && records != 64 && records != 128 && records != kStageAll / 2)
+    return fail(SS_ERR_INVALID_ARGUMENT, "forward chunk must be 0, 64, 128 or %d records, got %d",
+                kStageAll / 2, records);
+  g_forward_chunk[tile_size == 16 ? 0 : 1].store(records, std::memory_order_relaxed);
+  return SS_OK;
+}
+
+int ss_get_forward_chunk(int tile_size) {
+  if (tile_size != 16 && tile_size != 32) return -1;
+  const int c = g_forward_chunk[tile_size == 16 ? 0 : 1].load(std::memory_order_relaxed);
+  return c ? c : kStageAll / 2;
 }
 
 int ss_render_backward_workspace_bytes(int64_t n, int64_t gid_capacity, int height, int width,

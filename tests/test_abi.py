@@ -153,6 +153,17 @@ def test_backward_warps_knob_validation(lib):
     assert lib.ss_get_backward_warps(7) == -1
 
 
+def test_forward_chunk_knob_validation(lib):
+    rc, msg = _status(lib, "ss_set_forward_chunk", 8, 64)
+    assert rc == 4 and "tile_size" in msg
+    rc, msg = _status(lib, "ss_set_forward_chunk", 32, 100)
+    assert rc == 1 and "0, 64, 128 or 256" in msg
+    assert lib.ss_get_forward_chunk(16) == 256 and lib.ss_get_forward_chunk(32) == 256
+    assert lib.ss_set_forward_chunk(32, 64) == 0 and lib.ss_get_forward_chunk(32) == 64
+    assert lib.ss_set_forward_chunk(32, 0) == 0 and lib.ss_get_forward_chunk(32) == 256
+    assert lib.ss_get_forward_chunk(7) == -1
+
+
 def test_dependent_launch_switch(lib):
     """Programmatic dependent launch is on by default; the switch takes 0 or 1 only."""
     assert lib.ss_get_dependent_launch() == 1

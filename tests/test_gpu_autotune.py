@@ -89,3 +89,53 @@ def test_dependent_launch_does_not_change_results():
     assert torch.equal(runs[0][0], runs[1][0])
     for k in runs[0][1]:
         assert torch.equal(runs[0][1][k], runs[1][1][k]), k
+
+
+def test_forward_chunk_depth_does_not_change_the_image():
+    """A streamed list (longer than the 512-record stage) renders bitwise the same image at
+    every chunk depth: a block's k-th hit always goes to partial k mod 4, however the list is
+    chunked, and the hits carried across a refill keep their order."""
+    require_cuda()
+    import numpy as np
+    from structsplat_b200.synthetic import make_stress_field
+    H = W = 192
+    angle = np.random.default_rng(3).uniform(0, np.pi, (H, W)).astype(np.float32)
+    f = make_stress_field(H, W, 9000, seed=4, along_edge_angle=angle)
+    params = {k: torch.tensor(getattr(f, k), device="cuda") for k in PARAM_NAMES}
+    images = []
+    try:
+        for ts in (16, 32):
+            for chunk in autotune.CHUNKS:
+                _native.call("ss_set_forward_chunk", ts, chunk)
+                plan = RenderPlan.for_field(params, H, W, tile_size=ts)
+                img = plan.forward(params).clone()
+                torch.cuda.synchronize()
+                assert not plan.overflowed()
+                assert autotune._longest(plan.offsets) > autotune.STAGE_RECORDS
+                images.append((ts, img))
+    finally:
+        for ts in (16, 32):
+            _native.call("ss_set_forward_chunk", ts, 0)
+    for ts in (16, 32):
+        same = [img for t, img in images if t == ts]
+        assert all(torch.equal(same[0], img) for img in same[1:]), ts
+
+
+def test_tuner_picks_a_forward_chunk_for_streamed_lists():
+    require_cuda()
+    import numpy as np
+    from structsplat_b200.synthetic import make_stress_field
+    H = W = 192
+    angle = np.random.default_rng(3).uniform(0, np.pi, (H, W)).astype(np.float32)
+    f = make_stress_field(H, W, 9000, seed=4, along_edge_angle=angle)
+    params = {k: torch.tensor(getattr(f, k), device="cuda") for k in PARAM_NAMES}
+    go = torch.randn(H, W, 3, device="cuda", generator=torch.Generator("cuda").manual_seed(2))
+    try:
+        r = autotune.tune_render(params, H, W, go, repeats=2, use_cache=False)
+        assert r.forward_chunk in autotune.CHUNKS
+        assert _native.lib().ss_get_forward_chunk(r.tile_size) == r.forward_chunk
+        assert any("/chunk" in k for k in r.times_ms)
+    finally:
+        for ts in (16, 32):
+            _native.call("ss_set_forward_chunk", ts, 0)
+            _native.call("ss_set_backward_warps", ts, 0)
