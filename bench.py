@@ -944,6 +944,10 @@ def run_stress(args, dev):
             "step_roofline_frac": round(pairs * (PAIR_SLOTS_FWD + PAIR_SLOTS_BWD) / (
                 SM_COUNT * FP32_LANES * (measured_peaks().get("sm_max_mhz") or 1965.0) * 1e6)
                 / (ms * 1e-3), 4),
+            "roofline_note": "pairs counts every in-rectangle pair, as the reference evaluates "
+                             "them; the forward skips 8x8 blocks and the backward skips tile "
+                             "entries where every weight underflows to +0 (the elongated "
+                             "Gaussians' rectangles), so the fraction can exceed 1",
             "tile_entries": entries, "tile_list_max": int(counts.max()),
             "tile_list_median": float(counts.float().median()),
             "psnr_start": round(psnr_from_mse(float(loss0[0, 1])), 3),

@@ -729,6 +729,8 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   else
     stage_range<NT>(stage, rec, L, 0, (int)(L.count < kHalf ? L.count : kHalf), stage_gid);
   cp_async_commit();
+  // every pixel input this thread wrote is finite (the underflowed-entry skip below needs it)
+  bool pix_ok = true;
   // Per-pixel inputs of the tile: every load is issued before the first is used.
   constexpr int kPx = TS * TS / NT;
   static_assert(TS * TS % NT == 0, "pixels per thread");
@@ -772,6 +774,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
           v.w = -(gr * o0[i] + gg * o1[i] + gb * o2[i]) * inv;
         }
       }
+      pix_ok = pix_ok && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w);
       pix[q] = v;
     }
   }
@@ -782,7 +785,8 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   // same loop trip counts and the heaviest groups start first.  The order within a class comes
   // from shared-memory atomics and varies from run to run; no result depends on it (every
   // entry's moments are computed by its own four lanes).
-  auto prepare = [&](const float4(*st)[4], int m, int* ord) {
+  bool tile_finite = false;  // set once the pixel inputs are in shared memory
+  auto prepare = [&](float4(*st)[4], int m, int* ord) {
     constexpr int kPer = (kStageMax + NT - 1) / NT;  // entries per thread
     int code[kPer];
     if (threadIdx.x < 64) class_count[threadIdx.x] = 0;
@@ -793,7 +797,22 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       const int t = threadIdx.x + i * NT;
       code[i] = -1;
       if (t < m) {
-        const int4 r = *reinterpret_cast<const int4*>(&st[t][3]);
+        int4 r = *reinterpret_cast<const int4*>(&st[t][3]);
+        // An entry whose every pixel in the tile has q > kUnderflowQ adds exactly +0 to every
+        // moment (weight +0 times finite inputs): its rectangle is emptied so that its four
+        // lanes skip the walk (the forward's block test, at the scale of the entry).
+        if (tile_finite && (r.z - r.x > kFarRect || r.w - r.y > kFarRect)) {
+          const float4 p0 = st[t][0], p1 = st[t][1], p2 = st[t][2];
+          const int rx0 = max(r.x, tx0), rx1 = min(r.z, tx0 + TS) - 1;
+          const int ry0 = max(r.y, ty0), ry1 = min(r.w, ty0 + TS) - 1;
+          if (rx1 >= rx0 && ry1 >= ry0 && isfinite(p1.y) && isfinite(p1.z) && isfinite(p1.w) &&
+              isfinite(p2.x) &&
+              rect_min_q(p0.x, p0.y, p2.y, p2.z, p2.w, (float)rx0, (float)rx1, (float)ry0,
+                         (float)ry1) > kUnderflowQ) {
+            r.z = r.x;
+            reinterpret_cast<int4*>(&st[t][3])->z = r.x;
+          }
+        }
         const int w = min(r.z - tx0, TS) - max(r.x - tx0, 0);
         const int h = min(r.w - ty0, TS) - max(r.y - ty0, 0);
         const int passes = w > 0 && h > 0 ? min((w + 3) >> 2, 8) : 0;
@@ -831,6 +850,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     float acc[kMoments];
 #pragma unroll
     for (int k = 0; k < kMoments; ++k) acc[k] = 0.f;
+    bool walked = false;  // an empty walk leaves every moment +0: fast mode adds nothing
     if (active) {
       const float4 p0 = st[j][0], p1 = st[j][1], p2 = st[j][2];
       const int4 r = *reinterpret_cast<const int4*>(&st[j][3]);
@@ -838,6 +858,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       const int cy0 = max(r.y - ty0, 0), cy1 = min(r.w - ty0, TS);
       const int rows = cy1 - cy0;
       const int passes = (cx1 - cx0 + 3) >> 2;
+      walked = passes > 0 && rows > 0;
       const float dy0 = (float)(ty0 + cy0) - p0.y;
       for (int pass = 0; pass < passes; ++pass) {
         const int cx = cx0 + quad + 4 * pass;
@@ -877,7 +898,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     float a[5], b[3];
     scatter_level<9, 5>(acc, a, lane & 2, 2);
     scatter_level<5, 3>(a, b, lane & 1, 1);
-    if (active) {
+    if (active && (DETERMINISTIC || walked)) {
       const int base = ((quad & 2) ? 5 : 0) + ((quad & 1) ? 3 : 0);
       const int cnt = (quad & 1) ? 2 : 3;
 #pragma unroll
@@ -892,7 +913,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
       }
     }
   };
-  auto run = [&](const float4(*st)[4], int m, int* ord, const int* gsm, int64_t k0) {
+  auto run = [&](float4(*st)[4], int m, int* ord, const int* gsm, int64_t k0) {
     prepare(st, m, ord);
     // Groups go to warps as they become free (heaviest first, by the class order), so the
     // warps of a CTA finish close together instead of idling behind a round-robin share.
@@ -959,6 +980,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
             sq_sum += sq;
           }
         }
+        pix_ok = pix_ok && isfinite(pv.x) && isfinite(pv.y) && isfinite(pv.z) && isfinite(pv.w);
         pix[ly * TS + lx] = pv;
       }
     }
@@ -979,6 +1001,7 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
     }
     // the barrier before the first group (below) orders these pix writes before their reads
   }
+  tile_finite = __syncthreads_and(pix_ok) != 0;
   if (L.count <= kStageMax) {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
