@@ -49,20 +49,21 @@ class _B200RenderRS(Function):
         if not deterministic and n and H * W:
             # the fast path: the problem's buffers persist between calls (EagerPlan)
             plan = EAGER_PLANS.get(n, H, W, tile_size, cull, sigma_cutoff, means.device)
+            stream = _stream()
             _native.call("ss_project_rs_index_count", _p(means), _p(log_scales), _p(rotations),
                          _p(colors), _p(logits), n, float(dilation), float(sigma_cutoff), H, W,
                          tile_size, int(cull), _p(plan.records), _p(plan.offsets),
                          _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.step_block),
-                         plan.step_block.numel(), _p(plan.status), _stream())
+                         plan.step_block.numel(), _p(plan.status), stream)
             plan.ensure_capacity()
             _native.call("ss_tile_index_fill", _p(plan.records), n, H, W, tile_size, int(cull),
                          float(sigma_cutoff), _p(plan.offsets), _p(plan.gids), plan.capacity,
-                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), _stream())
+                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), stream)
             out = torch.empty(H, W, 3, device=means.device, dtype=torch.float32)
             den = torch.empty(H, W, device=means.device, dtype=torch.float32)
             _native.call("ss_render_forward", _p(plan.records), n, _p(plan.gids), plan.capacity,
                          _p(plan.offsets), H, W, tile_size, int(normalize), float(eps),
-                         float(tail), _p(out), _p(den), _p(plan.status), _stream())
+                         float(tail), _p(out), _p(den), _p(plan.status), stream)
             plan.note_status()
             plan.generation += 1
             plan.moments_used = False
@@ -95,10 +96,11 @@ class _B200RenderRS(Function):
             if plan.moments_used:  # a second backward of the same forward
                 plan.bwd_ws.zero_()
             plan.moments_used = True
+            stream = _stream()
             _native.call("ss_render_backward_moments", _p(grad_out), None, _p(plan.records), n,
                          _p(den), _p(out), _p(plan.gids), plan.capacity, _p(plan.offsets), H, W,
                          ts, int(normalize), float(eps), float(tail), 0, _p(plan.bwd_ws),
-                         plan.bwd_ws_bytes, _p(plan.status), _stream())
+                         plan.bwd_ws_bytes, _p(plan.status), stream)
             flat = torch.empty(9 * n, device=dev, dtype=torch.float32)
             g_means, g_ls = flat[:2 * n].view(n, 2), flat[2 * n:4 * n].view(n, 2)
             g_rot, g_colors = flat[4 * n:5 * n], flat[5 * n:8 * n].view(n, 3)
@@ -107,7 +109,7 @@ class _B200RenderRS(Function):
                          plan.capacity, _p(plan.offsets), H, W, ts, 0, _p(plan.bwd_ws),
                          _p(log_scales), _p(rotations), _p(logits), float(dilation),
                          _p(g_means), _p(g_ls), _p(g_rot), _p(g_colors), _p(g_logits),
-                         _stream())
+                         stream)
         else:
             if plan is not None:  # the plan moved on to a later forward: rebuild this one's
                 rec, _, _ = project(means, log_scales, rotations, colors, logits, H, W, cutoff,

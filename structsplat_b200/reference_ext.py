@@ -31,22 +31,17 @@ the same image (every pixel sums its Gaussians in ascending id either way).
 """
 from __future__ import annotations
 
-import ctypes
-
 import torch
 
 from . import _native
+from .render import _stream
 
 _RENDER_TILES = (16, 32)
 _INTERNAL_TILE = 32
 
 
 def _p(t):
-    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() else None
-
-
-def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return t.data_ptr() if t is not None and t.numel() else None
 
 
 def _check(cond: bool, message: str) -> None:

@@ -13,7 +13,6 @@ None; CUDA tensors only — there is no CPU fallback.  Everything runs on the cu
 """
 from __future__ import annotations
 
-import ctypes
 import math
 from dataclasses import dataclass
 
@@ -33,11 +32,19 @@ ADDITIVE_MODES = ("b200_additive", "additive", "cuda_additive", "cuda_tiled_addi
 
 
 def _p(t):
-    return None if t is None else ctypes.c_void_p(t.data_ptr())
+    """Device address of a tensor as a plain int (ctypes passes it as ``void*``), None → NULL."""
+    return None if t is None else t.data_ptr()
 
 
 def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    """The current CUDA stream of the current device as a raw ``cudaStream_t`` address.
+
+    Read through torch's C getters: ``torch.cuda.current_stream()`` builds a Python Stream
+    object and re-resolves the device on every call, which costs several microseconds per
+    library call on the eager path."""
+    if not torch.cuda.is_initialized():
+        torch.cuda.init()
+    return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())
 
 
 def validate_eps(value: float) -> float:
@@ -135,15 +142,15 @@ class _CapacityCache:
             total = int(offsets[-1].item())
             cap = int(total * 1.25) + 1024
             host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
-            ent = self.entries[key] = {"cap": cap, "host": host, "event": None}
+            ent = self.entries[key] = {"cap": cap, "host": host, "event": None,
+                                       "recorder": torch.cuda.Event()}
         elif ent["event"] is not None and ent["event"].query():
             seen = int(ent["host"][0])
             if seen > ent["cap"]:
                 ent["cap"] = int(seen * 1.25) + 1024
         ent["host"].copy_(offsets[-1:], non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
-        ent["event"] = ev
+        ent["recorder"].record()
+        ent["event"] = ent["recorder"]
         return ent["cap"]
 
 
@@ -184,6 +191,7 @@ class EagerPlan:
         self.generation = 0
         self.moments_used = False
         self.host_status = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self.status_event = torch.cuda.Event()  # re-recorded by every call
         self.event = None
         self._size_list(1)
 
@@ -213,9 +221,8 @@ class EagerPlan:
 
     def note_status(self):
         self.host_status.copy_(self.status, non_blocking=True)
-        ev = torch.cuda.Event()
-        ev.record()
-        self.event = ev
+        self.status_event.record()
+        self.event = self.status_event
 
 
 class _EagerPlans:
@@ -326,20 +333,21 @@ class _B200Render(Function):
             # the fast path: the problem's buffers persist between calls (EagerPlan)
             plan = EAGER_PLANS.get(n, H, W, tile_size, cull, sigma_cutoff, means.device)
             plan.step_block.zero_()  # fast moments and the status word
+            stream = _stream()
             _native.call("ss_pack_splats", _p(means), _p(conics), _p(colors), _p(radii), _p(op),
-                         n, H, W, _p(plan.records), _stream())
+                         n, H, W, _p(plan.records), stream)
             _native.call("ss_tile_index_count", _p(plan.records), n, H, W, tile_size, int(cull),
                          float(sigma_cutoff), _p(plan.offsets), _p(plan.idx_ws),
-                         plan.idx_ws_bytes, _p(plan.status), _stream())
+                         plan.idx_ws_bytes, _p(plan.status), stream)
             plan.ensure_capacity()
             _native.call("ss_tile_index_fill", _p(plan.records), n, H, W, tile_size, int(cull),
                          float(sigma_cutoff), _p(plan.offsets), _p(plan.gids), plan.capacity,
-                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), _stream())
+                         _p(plan.idx_ws), plan.idx_ws_bytes, _p(plan.status), stream)
             out = torch.empty(H, W, 3, device=means.device, dtype=torch.float32)
             den = torch.empty(H, W, device=means.device, dtype=torch.float32)
             _native.call("ss_render_forward", _p(plan.records), n, _p(plan.gids), plan.capacity,
                          _p(plan.offsets), H, W, tile_size, int(normalize), float(eps),
-                         float(tail), _p(out), _p(den), _p(plan.status), _stream())
+                         float(tail), _p(out), _p(den), _p(plan.status), stream)
             plan.note_status()
             plan.generation += 1
             plan.moments_used = False
@@ -371,10 +379,11 @@ class _B200Render(Function):
             if plan.moments_used:  # a second backward of the same forward
                 plan.bwd_ws.zero_()
             plan.moments_used = True
+            stream = _stream()
             _native.call("ss_render_backward_moments", _p(grad_out), None, _p(plan.records), n,
                          _p(den), _p(out), _p(plan.gids), plan.capacity, _p(plan.offsets), H, W,
                          ts, int(normalize), float(eps), float(tail), 0, _p(plan.bwd_ws),
-                         plan.bwd_ws_bytes, _p(plan.status), _stream())
+                         plan.bwd_ws_bytes, _p(plan.status), stream)
             flat = torch.empty(9 * n, device=dev, dtype=torch.float32)
             g_means, g_conics = flat[:2 * n].view(n, 2), flat[2 * n:5 * n].view(n, 3)
             g_colors = flat[5 * n:8 * n].view(n, 3)
@@ -382,7 +391,7 @@ class _B200Render(Function):
             _native.call("ss_render_backward_finalize", _p(plan.records), n, _p(plan.gids),
                          plan.capacity, _p(plan.offsets), H, W, ts, int(has_op), 0,
                          _p(plan.bwd_ws), _p(g_means), _p(g_conics), _p(g_colors), _p(g_opac),
-                         _stream())
+                         stream)
         else:
             if plan is not None:  # the plan moved on to a later forward: rebuild this one's
                 rec = pack_records(means, conics, colors, radii, op, H, W)
