@@ -668,9 +668,10 @@ def run_batched(args, dev, workload):
         res["autotune"] = "off (--no-tune): 32-px tiles, default backward warps"
     res["loop_graph_steps"] = Kg
     # Fast mode sums the moments with float atomics, so two runs of the same fit drift apart by
-    # rounding over the steps; the deterministic mode's batched and per-image fits are bitwise
-    # the same iteration, so their PSNRs are equal (checked here over Kd steps, both timed).
-    Kd = min(K, 100)
+    # rounding over the steps; the deterministic mode's batched and per-image fits are the same
+    # iteration, so their PSNRs agree (checked here over the same K steps, both timed): the
+    # comparison at equal PSNR (within 0.01 dB) is this pair.
+    Kd = K
     dset = FitSettings(deterministic=True)
     fdet = fresh()
     dplan = FitPlan(batch, Batch.concat_fields(fdet), batch.concat_images(targets), dset)
@@ -689,7 +690,10 @@ def run_batched(args, dev, workload):
     t_det, t_det_loop, ddiff = max_over_ranks([t_det, t_det_loop, ddiff], device=dev)
     res["deterministic"] = {"steps": Kd, "batched_img_s": round(B_all * Kd / (t_det * 1e-3), 1),
                             "loop_eager_img_s": round(B_all * Kd / (t_det_loop * 1e-3), 1),
-                            "psnr_max_abs_diff_vs_loop": round(ddiff, 9)}
+                            "psnr_max_abs_diff_vs_loop": round(ddiff, 9),
+                            "psnr_within_0_01_db": bool(ddiff <= 0.01)}
+    res["deterministic"]["speedup_vs_loop_eager"] = round(
+        res["deterministic"]["batched_img_s"] / res["deterministic"]["loop_eager_img_s"], 3)
     # the fit step's work: the in-rectangle pairs of every image (forward + backward slots)
     pairs = sum(pair_count({"means": f.means, "log_scales": f.log_scales,
                             "rotations": f.rotations}, {"H": h, "W": w}, dev=dev)
