@@ -35,7 +35,7 @@ sys.path.insert(0, str(REPO))
 METRIC = "fwd+bwd ms/iter (1024², 100k Gaussians); batched fit img/s vs plain kernel"
 WORKLOAD = {"H": 1024, "W": 1024, "N": 100_000, "seed": 0, "mode": "normalized"}
 PAIR_SLOTS_FWD, PAIR_SLOTS_BWD = 14, 40   # FP32 issue slots per in-rectangle pair (reference)
-BACKWARD_DRAM_BYTES = 40_243_456 + 768  # one backward_kernel launch at this workload (ncu)
+BACKWARD_DRAM_BYTES = 40_252_928 + 768  # one backward_kernel launch at this workload (ncu)
 # one fused forward + backward tile pass launch at this workload (ncu; bench.py --fused 1)
 FUSED_DRAM_BYTES = 23_515_648 + 512
 SM_COUNT, FP32_LANES = 148, 128
