@@ -487,11 +487,37 @@ __global__ void __launch_bounds__(kThreads) tile_sort_kernel(const int32_t* __re
 
 // Long lists: one CTA per list, in shared memory up to kBigSortSmem ids, else in place.
 // Lists of up to kRadixSortMax ids sort with CUB's block radix sort over the bits the ids need
-// (key_bits: pad keys 2^bits - 1 sort last); longer ones with the shared-memory bitonic network
-// (the ids of a list are distinct, so both give the one ascending order).
+// (key_bits: pad keys 2^bits - 1 sort last), with 2, 3 or 4 keys per thread, the fewest that
+// hold the list (a radix sort's work grows with its keys, pads included); longer lists with the
+// shared-memory bitonic network (the ids of a list are distinct, so every path gives the one
+// ascending order).
 constexpr int kRadixItems = 4;
 constexpr int kRadixSortMax = 1024 * kRadixItems;
-using BigRadixSort = cub::BlockRadixSort<unsigned, 1024, kRadixItems>;
+template <int K>
+using BigRadixSortK = cub::BlockRadixSort<unsigned, 1024, K>;
+union BigRadixTemp {
+  typename BigRadixSortK<2>::TempStorage k2;
+  typename BigRadixSortK<3>::TempStorage k3;
+  typename BigRadixSortK<4>::TempStorage k4;
+};
+
+template <int K>
+__device__ __forceinline__ void radix_sort_list(int32_t* __restrict__ g, int len, unsigned pad,
+                                                int key_bits,
+                                                typename BigRadixSortK<K>::TempStorage& tmp) {
+  unsigned keys[K];
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const int e = threadIdx.x * K + i;
+    keys[i] = e < len ? (unsigned)g[e] : pad;
+  }
+  BigRadixSortK<K>(tmp).Sort(keys, 0, key_bits);
+#pragma unroll
+  for (int i = 0; i < K; ++i) {
+    const int e = threadIdx.x * K + i;
+    if (e < len) g[e] = (int32_t)keys[i];
+  }
+}
 
 __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __restrict__ offsets,
                                                              int32_t* __restrict__ gids,
@@ -501,7 +527,7 @@ __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __re
   pdl_wait();
   pdl_trigger();
   extern __shared__ int sbuf[];
-  __shared__ typename BigRadixSort::TempStorage radix_temp;
+  __shared__ BigRadixTemp radix_temp;
   int count = *big_count;
   const unsigned pad = key_bits >= 32 ? 0xffffffffu : (1u << key_bits) - 1u;
   for (int k = blockIdx.x; k < count; k += gridDim.x) {
@@ -509,19 +535,12 @@ __global__ void __launch_bounds__(1024) tile_sort_big_kernel(const int32_t* __re
     int64_t lo = offsets[t];
     int len = (int)(offsets[t + 1] - lo);
     auto sync = [] { __syncthreads(); };
-    if (len <= kRadixSortMax) {
-      unsigned keys[kRadixItems];
-#pragma unroll
-      for (int i = 0; i < kRadixItems; ++i) {
-        const int e = threadIdx.x * kRadixItems + i;
-        keys[i] = e < len ? (unsigned)gids[lo + e] : pad;
-      }
-      BigRadixSort(radix_temp).Sort(keys, 0, key_bits);
-#pragma unroll
-      for (int i = 0; i < kRadixItems; ++i) {
-        const int e = threadIdx.x * kRadixItems + i;
-        if (e < len) gids[lo + e] = (int32_t)keys[i];
-      }
+    if (len <= 2 * 1024) {  // lists here are longer than the warp sort's 1,024 ids
+      radix_sort_list<2>(gids + lo, len, pad, key_bits, radix_temp.k2);
+    } else if (len <= 3 * 1024) {
+      radix_sort_list<3>(gids + lo, len, pad, key_bits, radix_temp.k3);
+    } else if (len <= kRadixSortMax) {
+      radix_sort_list<4>(gids + lo, len, pad, key_bits, radix_temp.k4);
     } else if (len <= kBigSortSmem) {
       for (int e = threadIdx.x; e < len; e += blockDim.x) sbuf[e] = gids[lo + e];
       __syncthreads();
