@@ -185,34 +185,51 @@ __device__ __forceinline__ void blur_window(const float* src, Span sy, Span sx, 
   }
 }
 
-// The same blur for a compile-time radius R: each thread takes RO consecutive outputs along
-// the blur axis and holds the RO + 2R source values they need in registers (one load per
-// source value instead of one per tap); the taps are accumulated in the same order.
-template <bool ALONG_Y, int R, int RO>
-__device__ __forceinline__ void blur_window_sliding(const float* src, Span sy, Span sx, int sw,
-                                                    float* dst, Span oy, Span ox, int nx,
-                                                    const Taps& taps, int H, int W) {
+// The same blur for a compile-time radius R over NCH maps at once (map c at src + c * scs and
+// dst + c * dcs): each thread takes RO consecutive outputs along the blur axis of one map and
+// holds the RO + 2R source values they need in registers (one load per source value instead of
+// one per tap); the taps are accumulated in the same order.  A segment whose sources all lie in
+// the stored window (every interior tile's) loads them from one base address; one that reaches
+// the image edge reflects each index.  The maps share one item loop so that the threads' last
+// round is shared by the maps rather than repeated per map.
+template <bool ALONG_Y, int R, int RO, int NCH>
+__device__ __forceinline__ void blur_window_sliding(const float* src, int scs, Span sy, Span sx,
+                                                    int sw, float* dst, int dcs, Span oy,
+                                                    Span ox, int nx, const Taps& taps, int H,
+                                                    int W) {
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int nline = ALONG_Y ? ox.len() : oy.len();
   const int nalong = ALONG_Y ? oy.len() : ox.len();
   const int nseg = (nalong + RO - 1) / RO;
+  const int per_map = nline * nseg;
   const Span src_span = ALONG_Y ? sy : sx;
   const int n_axis = ALONG_Y ? H : W;
-  for (int item = tid; item < nline * nseg; item += kStThreads) {
-    const int line = ALONG_Y ? item % nline : item / nseg;
-    const int seg = ALONG_Y ? item / nline : item % nseg;
+  for (int item = tid; item < NCH * per_map; item += kStThreads) {
+    const int ch = NCH == 1 ? 0 : item / per_map;
+    const int it = NCH == 1 ? item : item - ch * per_map;
+    const int line = ALONG_Y ? it % nline : it / nseg;
+    const int seg = ALONG_Y ? it / nline : it % nseg;
     const int a0 = (ALONG_Y ? oy.lo : ox.lo) + seg * RO;
     const int a_end = (ALONG_Y ? oy.hi : ox.hi);
     const int other = (ALONG_Y ? ox.lo : oy.lo) + line;  // the column (ALONG_Y) or the row
+    const float* sc = src + ch * scs;
     float win[RO + 2 * R];
+    if (a0 - R >= src_span.lo && a0 + RO + R <= src_span.hi) {
+      const float* base = ALONG_Y ? sc + (a0 - R - sy.lo) * sw + (other - sx.lo)
+                                  : sc + (other - sy.lo) * sw + (a0 - R - sx.lo);
 #pragma unroll
-    for (int j = 0; j < RO + 2 * R; ++j) {
-      int c = a0 - R + j;
-      if (c < 0 || c >= n_axis) c = reflect(c, n_axis);
-      c = min(c, src_span.hi - 1);  // sources only the unstored outputs past a_end would use
-      win[j] = ALONG_Y ? src[(c - sy.lo) * sw + (other - sx.lo)]
-                       : src[(other - sy.lo) * sw + (c - sx.lo)];
+      for (int j = 0; j < RO + 2 * R; ++j) win[j] = base[ALONG_Y ? j * sw : j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < RO + 2 * R; ++j) {
+        int c = a0 - R + j;
+        if (c < 0 || c >= n_axis) c = reflect(c, n_axis);
+        c = min(c, src_span.hi - 1);  // sources only the unstored outputs past a_end would use
+        win[j] = ALONG_Y ? sc[(c - sy.lo) * sw + (other - sx.lo)]
+                         : sc[(other - sy.lo) * sw + (c - sx.lo)];
+      }
     }
+    float* dc = dst + ch * dcs;
 #pragma unroll
     for (int k = 0; k < RO; ++k) {
       if (a0 + k < a_end) {
@@ -220,25 +237,27 @@ __device__ __forceinline__ void blur_window_sliding(const float* src, Span sy, S
 #pragma unroll
         for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(taps.w[j], win[k + j]));
         const int y = ALONG_Y ? a0 + k : other, x = ALONG_Y ? other : a0 + k;
-        dst[(y - oy.lo) * nx + (x - ox.lo)] = acc;
+        dc[(y - oy.lo) * nx + (x - ox.lo)] = acc;
       }
     }
   }
 }
 
-// Blur dispatch: the register form for the workloads' radii (3: sigma 1; 6: rho 2; 9: rho 3).
-template <bool ALONG_Y>
-__device__ __forceinline__ void blur_any(const float* src, Span sy, Span sx, int sw, float* dst,
-                                         Span oy, Span ox, int nx, const Taps& taps, int H,
-                                         int W) {
+// Blur dispatch for NCH maps (src + c * scs -> dst + c * dcs): the register form for the
+// workloads' radii (3: sigma 1; 6: rho 2; 9: rho 3), else the per-tap form map by map.
+template <bool ALONG_Y, int NCH>
+__device__ __forceinline__ void blur_maps(const float* src, int scs, Span sy, Span sx, int sw,
+                                          float* dst, int dcs, Span oy, Span ox, int nx,
+                                          const Taps& taps, int H, int W) {
   if (taps.r == 3)
-    blur_window_sliding<ALONG_Y, 3, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+    blur_window_sliding<ALONG_Y, 3, 4, NCH>(src, scs, sy, sx, sw, dst, dcs, oy, ox, nx, taps, H, W);
   else if (taps.r == 6)
-    blur_window_sliding<ALONG_Y, 6, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+    blur_window_sliding<ALONG_Y, 6, 4, NCH>(src, scs, sy, sx, sw, dst, dcs, oy, ox, nx, taps, H, W);
   else if (taps.r == 9)
-    blur_window_sliding<ALONG_Y, 9, 4>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+    blur_window_sliding<ALONG_Y, 9, 4, NCH>(src, scs, sy, sx, sw, dst, dcs, oy, ox, nx, taps, H, W);
   else
-    blur_window<ALONG_Y>(src, sy, sx, sw, dst, oy, ox, nx, taps, H, W);
+    for (int c = 0; c < NCH; ++c)
+      blur_window<ALONG_Y>(src + c * scs, sy, sx, sw, dst + c * dcs, oy, ox, nx, taps, H, W);
 }
 
 template <int CH>
@@ -276,13 +295,9 @@ __global__ void __launch_bounds__(kStThreads)
   Span sgy = wy, sgx = wx;
   int gw = pw, gsz = wn;
   if (rg > 0) {
-#pragma unroll
-    for (int c = 0; c < CH; ++c)
-      blur_any<true>(S + c * wn, wy, wx, pw, B + c * bn, gy, wx, pw, tg, H, W);
+    blur_maps<true, CH>(S, wn, wy, wx, pw, B, bn, gy, wx, pw, tg, H, W);
     __syncthreads();
-#pragma unroll
-    for (int c = 0; c < CH; ++c)
-      blur_any<false>(B + c * bn, gy, wx, pw, S + c * gn, gy, gx, pg, tg, H, W);
+    blur_maps<false, CH>(B, bn, gy, wx, pw, S, gn, gy, gx, pg, tg, H, W);
     __syncthreads();
     sgy = gy;
     sgx = gx;
@@ -400,11 +415,9 @@ __global__ void __launch_bounds__(kStThreads)
   Span sy = wy, sx = wx;
   int tw = pw, tsz = wn;
   if (rt > 0) {
-    for (int c = 0; c < 3; ++c)
-      blur_any<true>(S + c * wn, wy, wx, pw, B + c * bn, oy, wx, pw, tt, H, W);
+    blur_maps<true, 3>(S, wn, wy, wx, pw, B, bn, oy, wx, pw, tt, H, W);
     __syncthreads();
-    for (int c = 0; c < 3; ++c)
-      blur_any<false>(B + c * bn, oy, wx, pw, S + c * on, oy, ox, po, tt, H, W);
+    blur_maps<false, 3>(B, bn, oy, wx, pw, S, on, oy, ox, po, tt, H, W);
     __syncthreads();
     sy = oy;
     sx = ox;
