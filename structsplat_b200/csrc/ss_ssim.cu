@@ -13,9 +13,10 @@
 //   a = dS/dmu_p = (2 mu_t (A2 - A1) - S 2 mu_p (B2 - B1)) / (B1 B2),
 //   b = dS/dE_pp = -S / B2,   c = dS/dE_pt = 2 A1 / (B1 B2),
 // because the zero-padded symmetric window is its own adjoint.  Four passes over the batch
-// (per pixel), or, on the tile grid of a render batch (tile sizes 16 and 32), two passes of one
-// CTA per (tile, channel) and a per-pixel fold: horizontal then vertical window of
-// (p, p^2, p t) and the maps; horizontal then vertical window of (a, b, c) and the gradient.
+// (per pixel), or, on the tile grid of a render batch (tile sizes 16 and 32), two tile passes
+// and a per-pixel fold: one CTA per tile for the horizontal then vertical window of
+// (p, p^2, p t) and the maps of all three channels; one CTA per (tile, channel) for the
+// horizontal then vertical window of (a, b, c) and the gradient.
 // The last step folds -w dSSIM/dp, with (1 - w) times the pixel loss's part already in
 // pixel_grad, through the normalisation into pixel_grad.
 #include <cmath>
@@ -308,62 +309,91 @@ __device__ __forceinline__ void window_run(const float* const (&in)[M], int stri
   }
 }
 
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// The maps of all three channels of a tile in one CTA: the tile and its halo of image and target
+// (RGB interleaved) are copied into shared memory once, as whole rows (a CTA per channel would
+// fetch the same interleaved rows three times), then each channel runs the horizontal window of
+// (p, p^2, p t), formed from the raw values as it goes, and the vertical window and the maps.
+template <int TS>
+struct Maps3Smem {
+  static constexpr int R = TS + 2 * kRadius;
+  static constexpr size_t kRaw = (size_t)6 * R * R;  // image then target, channel planes
+  static constexpr size_t kHs = (size_t)3 * R * TS;
+  static constexpr size_t kBytes = (kRaw + kHs) * sizeof(float);
+};
+
 template <int TS>
 __global__ void __launch_bounds__(kTileThreads)
-    ssim_maps_tile_kernel(const float* __restrict__ img, const float* __restrict__ tgt,
-                          const float* __restrict__ stats, Frames frames, int64_t P, Window win,
-                          float* __restrict__ abc, float* __restrict__ ssim) {
+    ssim_maps_tile3_kernel(const float* __restrict__ img, const float* __restrict__ tgt,
+                           const float* __restrict__ stats, Frames frames, int64_t P, Window win,
+                           float* __restrict__ abc, float* __restrict__ ssim) {
   pdl_wait();
   pdl_trigger();
   constexpr int R = TS + 2 * kRadius;
-  constexpr int kGroups = TS / kRun;  // runs per line
-  __shared__ float src[3][R * R];     // p, p^2, p t over the tile and its halo
-  __shared__ float hs[3][R * TS];     // horizontal window, every halo row
+  constexpr int kGroups = TS / kRun;
+  extern __shared__ float m3_smem[];
+  float* raw = m3_smem;                       // [6][R * R]: image c, then target c
+  float* hs = m3_smem + Maps3Smem<TS>::kRaw;  // [3][R * TS]
   __shared__ float red[kTileThreads / 32];
   const Frame fr = frame_of_tile(frames, blockIdx.x, 0);
   const int local = blockIdx.x - fr.first_tile;
   const int tx0 = (local % fr.tiles_x) * TS, ty0 = (local / fr.tiles_x) * TS;
   const int H = fr.H, W = fr.W;
-  const int c = blockIdx.y;  // one channel per CTA: a single load phase each
+  for (int i = threadIdx.x; i < R * 3 * R; i += kTileThreads) {
+    const int row = i / (3 * R), f = i - row * (3 * R);
+    const int xi = f / 3, ch = f - 3 * xi;
+    const int x = tx0 - kRadius + xi, y = ty0 - kRadius + row;
+    float* di = raw + ch * (R * R) + row * R + xi;
+    float* dt = di + 3 * (R * R);
+    if (x >= 0 && x < W && y >= 0 && y < H) {
+      const int64_t q = 3 * (fr.pixel_base + (int64_t)y * W + x) + ch;
+      cp_async4(di, img + q);
+      cp_async4(dt, tgt + q);
+    } else {
+      *di = 0.f;
+      *dt = 0.f;
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
   float ssum = 0.f;
-  {
-    // the tile and its halo: a fixed trip count, unrolled, so that every load of a thread is
-    // in flight before the first is used
-    constexpr int kIters = (R * R + kTileThreads - 1) / kTileThreads;
-    float v[kIters], t[kIters];
-#pragma unroll
-    for (int k = 0; k < kIters; ++k) {
-      const int i = threadIdx.x + k * kTileThreads;
-      const int x = tx0 - kRadius + i % R, y = ty0 - kRadius + i / R;
-      const bool in = i < R * R && x >= 0 && x < W && y >= 0 && y < H;
-      const int64_t q = fr.pixel_base + (int64_t)y * W + x;
-      v[k] = in ? img[3 * q + c] : 0.f;
-      t[k] = in ? tgt[3 * q + c] : 0.f;
-    }
-#pragma unroll
-    for (int k = 0; k < kIters; ++k) {
-      const int i = threadIdx.x + k * kTileThreads;
-      if (i < R * R) {
-        src[0][i] = v[k];
-        src[1][i] = v[k] * v[k];
-        src[2][i] = v[k] * t[k];
-      }
-    }
-    __syncthreads();
+  for (int c = 0; c < 3; ++c) {
+    const float* rp = raw + c * (R * R);
+    const float* rt = raw + (3 + c) * (R * R);
     for (int w = threadIdx.x; w < R * kGroups; w += kTileThreads) {
       const int r = w / kGroups, x0 = (w % kGroups) * kRun;
-      const float* const in[3] = {&src[0][r * R + x0], &src[1][r * R + x0], &src[2][r * R + x0]};
-      float out[3][kRun];
-      window_run<3>(in, 1, win, out);
+      float v[2 * kRadius + kRun], pp[2 * kRadius + kRun], pt[2 * kRadius + kRun];
 #pragma unroll
-      for (int m = 0; m < 3; ++m)
+      for (int i = 0; i < 2 * kRadius + kRun; ++i) {
+        const float a = rp[r * R + x0 + i], t = rt[r * R + x0 + i];
+        v[i] = a;
+        pp[i] = a * a;
+        pt[i] = a * t;
+      }
 #pragma unroll
-        for (int o = 0; o < kRun; ++o) hs[m][r * TS + x0 + o] = out[m][o];
+      for (int o = 0; o < kRun; ++o) {
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+        for (int k = 0; k <= 2 * kRadius; ++k) {
+          a0 = fmaf(win.g[k], v[o + k], a0);
+          a1 = fmaf(win.g[k], pp[o + k], a1);
+          a2 = fmaf(win.g[k], pt[o + k], a2);
+        }
+        hs[0 * R * TS + r * TS + x0 + o] = a0;
+        hs[1 * R * TS + r * TS + x0 + o] = a1;
+        hs[2 * R * TS + r * TS + x0 + o] = a2;
+      }
     }
     __syncthreads();
     for (int w = threadIdx.x; w < TS * kGroups; w += kTileThreads) {
       const int x = w % TS, y0 = (w / TS) * kRun;
-      const float* const in[3] = {&hs[0][y0 * TS + x], &hs[1][y0 * TS + x], &hs[2][y0 * TS + x]};
+      const float* const in[3] = {&hs[0 * R * TS + y0 * TS + x], &hs[1 * R * TS + y0 * TS + x],
+                                  &hs[2 * R * TS + y0 * TS + x]};
       float out[3][kRun];
       window_run<3>(in, TS, win, out);
 #pragma unroll
@@ -384,6 +414,7 @@ __global__ void __launch_bounds__(kTileThreads)
         abc[(int64_t)(3 * c + 2) * P + p] = 2.0f * A1 / D;
       }
     }
+    __syncthreads();  // hs is rewritten by the next channel
   }
   if (!ssim) return;
 #pragma unroll
@@ -581,17 +612,19 @@ int ss_fit_ssim(const ss_batch* batch, const float* image, const float* den, con
   const int ts = batch->tile_size;
   if ((ts == 16 || ts == 32) && batch->tiles > 0 && batch->tiles <= (int64_t)INT32_MAX &&
       frames_of_batch(batch, 0, &f) == SS_OK) {  // the tile grid of a render batch
-    const dim3 grid((unsigned)batch->tiles, 3);  // (tile, channel)
+    const dim3 grid((unsigned)batch->tiles, 3);  // the gradient: (tile, channel)
     float4* pg = reinterpret_cast<float4*>(pixel_grad);
     float* gbuf = h;  // 3P: each channel's -w dSSIM/dp
     if (ts == 32) {
-      launch("ssim maps", ssim_maps_tile_kernel<32>, grid, kTileThreads, 0, s, image, target,
-             stats, f, P, win, abc, ssim);
+      launch_smem("ssim maps", ssim_maps_tile3_kernel<32>, dim3((unsigned)batch->tiles, 1),
+                  kTileThreads, Maps3Smem<32>::kBytes, s, image, target, stats, f, P, win, abc,
+                  ssim);
       launch("ssim gradient", ssim_grad_tile_kernel<32>, grid, kTileThreads, 0, s, abc, image,
              target, f, P, win, ssim_weight, gbuf);
     } else {
-      launch("ssim maps", ssim_maps_tile_kernel<16>, grid, kTileThreads, 0, s, image, target,
-             stats, f, P, win, abc, ssim);
+      launch_smem("ssim maps", ssim_maps_tile3_kernel<16>, dim3((unsigned)batch->tiles, 1),
+                  kTileThreads, Maps3Smem<16>::kBytes, s, image, target, stats, f, P, win, abc,
+                  ssim);
       launch("ssim gradient", ssim_grad_tile_kernel<16>, grid, kTileThreads, 0, s, abc, image,
              target, f, P, win, ssim_weight, gbuf);
     }
