@@ -186,24 +186,26 @@ __device__ __forceinline__ void enumerate_pairs(const Splat* rec, int64_t n, int
 }
 
 // Exclusive scan of the T+1 counters into int64 and int32 offsets by one CTA of kThreads
-// threads, in rounds of 4 kThreads items; the counters are read from L2 (other CTAs' atomics).
+// threads, in rounds of kScanItems kThreads items (one round for up to 2,047 tiles); the counters
+// are read from L2 (other CTAs' atomics), every load of a round in flight before the scan.
+constexpr int kScanItems = 8;
 __device__ void block_scan_counts(const int* tile_count, int64_t items, long long* off64,
                                   int32_t* off32) {
   using Scan = cub::BlockScan<long long, kThreads>;
   __shared__ typename Scan::TempStorage tmp;
   long long carry = 0;
-  for (int64_t b0 = 0; b0 < items; b0 += 4 * kThreads) {
-    long long v[4];
+  for (int64_t b0 = 0; b0 < items; b0 += kScanItems * kThreads) {
+    long long v[kScanItems];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t idx = b0 + 4 * threadIdx.x + k;
+    for (int k = 0; k < kScanItems; ++k) {
+      const int64_t idx = b0 + kScanItems * threadIdx.x + k;
       v[k] = idx < items ? __ldcg(tile_count + idx * kCounterStride) : 0;
     }
     long long total;
     Scan(tmp).ExclusiveSum(v, v, total);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t idx = b0 + 4 * threadIdx.x + k;
+    for (int k = 0; k < kScanItems; ++k) {
+      const int64_t idx = b0 + kScanItems * threadIdx.x + k;
       if (idx < items) {
         const long long o = carry + v[k];
         off64[idx] = o;
@@ -607,7 +609,7 @@ int index_count(const Frames& frames, int ts, int64_t T, const void* records, in
     return check_launch("tile_index_count memset");
   const Splat* rec = static_cast<const Splat*>(records);
   float cutoff2 = sigma_cutoff * sigma_cutoff;
-  // the count kernel's last CTA scans up to kFusedScanMax counters (four rounds); larger sets
+  // the count kernel's last CTA scans up to kFusedScanMax counters (two rounds); larger sets
   // up to kSingleScanMax take the 1024-thread scan kernel, beyond that CUB's device scan
   const bool fused_scan = T + 1 <= kFusedScanMax;
   const bool single_scan = T + 1 <= kSingleScanMax;
