@@ -680,7 +680,7 @@ struct BwdSmem {
   static constexpr size_t kGidOff = kPixOff + (size_t)TS * TS * sizeof(float4);
   static constexpr size_t kOrderOff = kGidOff + (size_t)kStageMax * sizeof(int);
   static constexpr size_t kClassOff = kOrderOff + (size_t)kStageMax * sizeof(int);
-  static constexpr size_t kNextOff = kClassOff + 64 * sizeof(int);
+  static constexpr size_t kNextOff = kClassOff + 256 * sizeof(int);
   static constexpr size_t kQueueOff = kNextOff + 16;
   static constexpr size_t kBytes =
       kQueueOff + (FUSED ? (size_t)kWarps * kQueueLen * sizeof(uint32_t) : 0);
@@ -780,16 +780,16 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int member = lane >> 2, quad = lane & 3;
-  // Order of the staged entries [0, m) by a counting sort into 64 cost classes (loop passes
-  // descending, then rows in fours descending), so the eight Gaussians of a warp have nearly the
-  // same loop trip counts and the heaviest groups start first.  The order within a class comes
+  // Order of the staged entries [0, m) by a counting sort into 256 cost classes (loop passes
+  // descending, then rows descending), so the eight Gaussians of a warp have nearly the same
+  // loop trip counts and the heaviest groups start first.  The order within a class comes
   // from shared-memory atomics and varies from run to run; no result depends on it (every
   // entry's moments are computed by its own four lanes).
   bool tile_finite = false;  // set once the pixel inputs are in shared memory
   auto prepare = [&](float4(*st)[4], int m, int* ord) {
     constexpr int kPer = (kStageMax + NT - 1) / NT;  // entries per thread
     int code[kPer];
-    if (threadIdx.x < 64) class_count[threadIdx.x] = 0;
+    for (int i = threadIdx.x; i < 256; i += NT) class_count[i] = 0;
     if (threadIdx.x == 0) next_group = 0;
     __syncthreads();
 #pragma unroll
@@ -816,23 +816,30 @@ __global__ void __launch_bounds__(NT, (BackwardOccupancy<TS, NT>::kBlocks))
         const int w = min(r.z - tx0, TS) - max(r.x - tx0, 0);
         const int h = min(r.w - ty0, TS) - max(r.y - ty0, 0);
         const int passes = w > 0 && h > 0 ? min((w + 3) >> 2, 8) : 0;
-        const int hb = h > 0 ? min((h - 1) >> 2, 7) : 0;
-        const int cls = passes > 0 ? (8 - passes) * 8 + (7 - hb) : 63;
+        const int cls = passes > 0 ? (8 - passes) * 32 + (32 - min(h, 32)) : 255;
         code[i] = (cls << 16) | atomicAdd(&class_count[cls], 1);
       }
     }
     __syncthreads();
-    if (warp == 0) {  // exclusive scan of the 64 class counts
-      const int c0 = class_count[2 * lane], c1 = class_count[2 * lane + 1];
-      int x = c0 + c1;
+    if (warp == 0) {  // exclusive scan of the 256 class counts, eight per lane
+      int cc[8];
+      int x = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        cc[k] = class_count[8 * lane + k];
+        x += cc[k];
+      }
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o) x += y;
       }
-      const int excl = x - c0 - c1;
-      class_count[2 * lane] = excl;
-      class_count[2 * lane + 1] = excl + c0;
+      int run = x;
+#pragma unroll
+      for (int k = 7; k >= 0; --k) {
+        run -= cc[k];
+        class_count[8 * lane + k] = run;
+      }
     }
     __syncthreads();
 #pragma unroll
