@@ -44,8 +44,8 @@ class RenderPlan:
     device: torch.device = field(default_factory=lambda: torch.device("cuda"))
     # forward_backward in one tile pass (ss_render_forward_backward) instead of the forward and
     # backward tile kernels.  Off by default: at 1024x1024 with 100k Gaussians the fused pass
-    # takes 0.111 ms against 0.057 + 0.058 ms alone, but the two kernels already overlap under
-    # programmatic dependent launch, so the captured step is no faster.  A deterministic fused
+    # takes 0.103 ms against 0.051 + 0.057 ms alone, but the two kernels already overlap under
+    # programmatic dependent launch, so the captured step is no faster (0.1365 vs 0.1345 ms).  A deterministic fused
     # plan leaves capacity-truncated tiles unrendered (SS_STATUS_DETERMINISTIC_TRUNCATED).
     fused: bool = False
 
