@@ -36,15 +36,21 @@ def _p(t):
     return None if t is None else t.data_ptr()
 
 
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+_DEVICE = getattr(torch._C, "_cuda_getDevice", None)
+
+
 def _stream():
     """The current CUDA stream of the current device as a raw ``cudaStream_t`` address.
 
-    Read through torch's C getters: ``torch.cuda.current_stream()`` builds a Python Stream
-    object and re-resolves the device on every call, which costs several microseconds per
-    library call on the eager path."""
+    Read through torch's C getters where this torch has them: ``torch.cuda.current_stream()``
+    builds a Python Stream object and re-resolves the device on every call, which costs several
+    microseconds per library call on the eager path."""
+    if _RAW_STREAM is None or _DEVICE is None:
+        return torch.cuda.current_stream().cuda_stream
     if not torch.cuda.is_initialized():
         torch.cuda.init()
-    return torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice())
+    return _RAW_STREAM(_DEVICE())
 
 
 def validate_eps(value: float) -> float:
