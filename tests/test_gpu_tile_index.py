@@ -85,6 +85,21 @@ def test_scan_regimes_match_oracle(H, W):
     assert np.array_equal(gids, ref_g)
 
 
+@pytest.mark.parametrize("n", [1024, 1025, 2048, 2049, 3072, 3073, 4096, 4097, 16384, 16385])
+def test_single_tile_list_lengths(n):
+    """One 16x16 tile that every Gaussian covers: its list is exactly ids 0 .. n-1, whichever
+    sort a list of that length takes (the per-warp register sort up to 1,024 ids, the block
+    radix sort with 2, 3 or 4 keys per thread up to 2,048 / 3,072 / 4,096, the shared-memory
+    bitonic sort up to 16,384, the in-place one beyond), from the fill's arbitrary order."""
+    require_cuda()
+    rng = np.random.default_rng(n)
+    means = rng.uniform(0, 16, (n, 2)).astype(np.float32)
+    radii = rng.integers(1, 8, (n, 2))
+    gids, offsets = _index(means, radii, 16, 16, 16)
+    assert np.array_equal(offsets, [0, n])
+    assert np.array_equal(gids, np.arange(n))
+
+
 @pytest.mark.parametrize("n", [3000, 20000])
 def test_long_tile_lists_are_sorted(n):
     """Lists longer than the per-warp sort (1024) and the per-CTA shared-memory sort (16384)."""
