@@ -548,8 +548,9 @@ def batched_workload(images=BATCH_IMAGES, seed=BATCH_SEED, rank=0, world=1):
     sizes = [all_sizes[b] for b in mine]
     counts = [int(round(BATCH_DENSITY * h * w)) for h, w in sizes]
     jobs = [(h, w, seed * 1000 + 2 * b) for b, (h, w) in zip(mine, sizes)]
-    with ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
-                             mp_context=mp.get_context("spawn")) as pool:
+    # the ranks of a node build their shares at the same time: each takes its share of the cores
+    workers = max(1, min(16, (os.cpu_count() or 1) // max(world, 1)))
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as pool:
         targets = list(pool.map(_batch_target, jobs))
     fields = [make_field(h, w, n, seed=seed * 1000 + 2 * b + 1)
               for b, (h, w), n in zip(mine, sizes, counts)]
